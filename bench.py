@@ -1,0 +1,428 @@
+#!/usr/bin/env python
+"""Throughput benchmark: 2D type-1 + type-2 NUFFT, complex64, eps = 1e-6, 512 x 512 modes.
+
+Workload (one step = one type-1 and one type-2 transform of each point set):
+  (a) radial: 512 spokes x 1024 samples (M = 524,288), golden-angle spoke angles
+      theta_s = s * pi (sqrt(5) - 1) / 2 mod pi, 1024 evenly spaced radii in [-pi, pi);
+  (b) clustered: M = 4,000,000 points, x, y ~ N(0, 0.3^2) wrapped to [-pi, pi);
+  strengths c and modes f iid complex N(0, 1); seeded synthetic data.
+Metric: NU points per second, counting M once per transform (2 * (Ma + Mb) per step).
+
+`value` times the steps with inputs resident in HBM (CUDA events, L2 flushed
+between steps by writing a 256 MB buffer outside the timed events).  `e2e` times
+the same steps through the public API with pinned host buffers: host->device
+copies of x, y, c, f and device->host copies of the results are inside the
+timed region.  `--impl reference` times the CPU restatement of nufftax's
+pure-JAX path (oracle/) on all host cores on a bounded sample.
+Multi-GPU runs are independent replicas (weak scaling), timed as the max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+EPS = 1e-6
+N_MODES = (512, 512)
+METRIC = "type-1/2 NU points/s at eps 1e-6 (2D, 512^2 modes, complex64)"
+
+
+# ---------------------------------------------------------------------------
+# Workload
+# ---------------------------------------------------------------------------
+def radial_points(n_spokes=512, n_samples=1024):
+    ga = np.pi * (np.sqrt(5.0) - 1.0) / 2.0
+    theta = np.mod(np.arange(n_spokes) * ga, np.pi)
+    r = -np.pi + 2.0 * np.pi * np.arange(n_samples) / n_samples
+    x = (r[None, :] * np.cos(theta)[:, None]).ravel()
+    y = (r[None, :] * np.sin(theta)[:, None]).ravel()
+    return x.astype(np.float32), y.astype(np.float32)
+
+
+def clustered_points(M, rng, sigma=0.3):
+    xy = sigma * rng.standard_normal((2, M))
+    xy = np.mod(xy + np.pi, 2 * np.pi) - np.pi
+    return xy[0].astype(np.float32), xy[1].astype(np.float32)
+
+
+def workload(seed=1234, scale=1.0):
+    rng = np.random.default_rng(seed)
+    xa, ya = radial_points(max(1, int(512 * scale)), 1024)
+    Mb = max(1, int(4_000_000 * scale))
+    xb, yb = clustered_points(Mb, rng)
+    sets = []
+    for name, x, y in (("radial", xa, ya), ("clustered", xb, yb)):
+        M = x.size
+        c = (rng.standard_normal(M) + 1j * rng.standard_normal(M)).astype(np.complex64)
+        f = (rng.standard_normal((N_MODES[1], N_MODES[0])) + 1j * rng.standard_normal(
+            (N_MODES[1], N_MODES[0]))).astype(np.complex64)
+        sets.append({"name": name, "x": x, "y": y, "c": c, "f": f, "M": M})
+    return sets
+
+
+def points_per_step(sets):
+    return sum(2 * s["M"] for s in sets)
+
+
+# ---------------------------------------------------------------------------
+# Environment helpers
+# ---------------------------------------------------------------------------
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            d = json.loads(p.read_text())
+            return float(d["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200", "-i",
+                 str(self.index)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 7:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[0]))
+                mx.append(float(r[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, r[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+ALG_BYTES = {
+    # algorithmic bytes per launch (complex64, d = 2): coordinates + strengths once, grid once
+    "nfx_spread_sorted": lambda M, nf, nm: M * (4 * 2 + 8) + 8 * nf[0] * nf[1],
+    "nfx_interp_sorted": lambda M, nf, nm: M * (4 * 2 + 8) + 8 * nf[0] * nf[1],
+    "nfx_sort_points": lambda M, nf, nm: M * (4 * 2 + 4),
+    "nfx_deconv_shuffle": lambda M, nf, nm: 16 * nm[0] * nm[1],
+    "nfx_deconv_pad": lambda M, nf, nm: 8 * nm[0] * nm[1] + 8 * nf[0] * nf[1],
+}
+
+
+def run_gpu(args):
+    import torch
+
+    import nufftax_b200 as nb
+    from nufftax_b200 import profiling
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    sets = workload(seed=1234 + rank)
+    host = []
+    for s in sets:
+        h = {k: torch.from_numpy(s[k]).pin_memory() for k in ("x", "y", "c", "f")}
+        h["M"] = s["M"]
+        h["name"] = s["name"]
+        host.append(h)
+    devsets = [{k: (v.to(dev) if isinstance(v, torch.Tensor) else v) for k, v in h.items()} for h in host]
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    kp = nb.compute_kernel_params(EPS)
+    nf = tuple(nb.compute_grid_size(n, 2.0, kp.nspread) for n in N_MODES)
+
+    def step(ds):
+        nb.sort_cache.clear()
+        outs = []
+        for s in ds:
+            f1 = nb.nufft2d1(s["x"], s["y"], s["c"], N_MODES, eps=EPS)
+            c2 = nb.nufft2d2(s["x"], s["y"], s["f"], eps=EPS)
+            outs.append((f1, c2))
+        return outs
+
+    for _ in range(args.warmup):
+        step(devsets)
+    torch.cuda.synchronize()
+
+    # ---- timed region: device-resident inputs ---------------------------------
+    sampler = ClockSampler(local)
+    sampler.start()
+    stream = torch.cuda.current_stream(dev)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    with profiling.record() as rec:
+        for i in range(args.steps):
+            flush.fill_(float(i))
+            starts[i].record(stream)
+            step(devsets)
+            ends[i].record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    step_ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
+    total_ms = float(sum(step_ms))
+    per_call = rec.summary()
+    launches = sum(v["launches"] for v in per_call.values())
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    pts = points_per_step(sets) * args.steps * world
+    value = pts / (total_ms / 1e3)
+
+    # dominant kernel roofline (our kernels only)
+    peak, peak_kind = measured_peaks()
+    ours = {k: v for k, v in per_call.items() if k in ALG_BYTES}
+    dom = max(ours, key=lambda k: ours[k]["ms"])
+    # every step launches the dominant kernel once per point set
+    alg_total = args.steps * sum(ALG_BYTES[dom](s["M"], nf, N_MODES) for s in sets)
+    n_dom = ours[dom]["calls"]
+    alg_per_launch = alg_total / max(n_dom, 1)
+    avg_ms = ours[dom]["ms"] / max(n_dom, 1)
+    achieved = alg_total / (ours[dom]["ms"] / 1e3) / 1e9
+    breakdown = {k: {"calls": v["calls"], "ms_per_step": v["ms"] / args.steps} for k, v in per_call.items()}
+
+    # ---- e2e: public API with pinned host buffers -------------------------------
+    out_host = []
+    for h in host:
+        out_host.append((torch.empty((N_MODES[1], N_MODES[0]), dtype=torch.complex64).pin_memory(),
+                         torch.empty(h["M"], dtype=torch.complex64).pin_memory()))
+    h2d = sum(h[k].numel() * h[k].element_size() for h in host for k in ("x", "y", "c", "f"))
+    d2h = sum(a.numel() * a.element_size() + b.numel() * b.element_size() for a, b in out_host)
+
+    def e2e_step():
+        nb.sort_cache.clear()
+        for h, (fo, co) in zip(host, out_host):
+            x = h["x"].to(dev, non_blocking=True)
+            y = h["y"].to(dev, non_blocking=True)
+            c = h["c"].to(dev, non_blocking=True)
+            f = h["f"].to(dev, non_blocking=True)
+            f1 = nb.nufft2d1(x, y, c, N_MODES, eps=EPS)
+            c2 = nb.nufft2d2(x, y, f, eps=EPS)
+            fo.copy_(f1, non_blocking=True)
+            co.copy_(c2, non_blocking=True)
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    torch.cuda.synchronize()
+    e_ms = 0.0
+    for i in range(args.steps):
+        flush.fill_(float(i))
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        e2e_step()
+        b.record(stream)
+        torch.cuda.synchronize()
+        e_ms += a.elapsed_time(b)
+    if world > 1:
+        t = torch.tensor([e_ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e_ms = float(t.item())
+    e2e_value = pts / (e_ms / 1e3)
+
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "NU points/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "c64",
+        "data": "synthetic (seeded): radial 512x1024 golden-angle + 4M clustered N(0,0.3^2)",
+        "config": {"workload": "2D type-1 + type-2, 512x512 modes, nf 1024x1024, eps 1e-6, ns 8: radial "
+                               "M=524288 and clustered M=4000000 per step", "global_batch": points_per_step(sets) * world,
+                   "parallelism": f"replicas x{world}", "l2": "flushed between steps (256 MB write)"},
+        "e2e": {"value": e2e_value, "unit": "NU points/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                     "alg_bytes_per_launch": alg_per_launch, "avg_launch_ms": avg_ms},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+        "breakdown": breakdown,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_sample()
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# CPU legs: the oracle (restatement of nufftax's pure-JAX path)
+# ---------------------------------------------------------------------------
+def _oracle():
+    sys.path.insert(0, str(ROOT))
+    from oracle import nufft_oracle as O
+
+    return O
+
+
+def cpu_baseline_sample():
+    """Single-core oracle timing on a bounded sample (about 10-30 s of CPU work)."""
+    O = _oracle()
+    sets = workload(seed=99, scale=1.0)
+    sample = []
+    for s in sets:
+        m = 65536 if s["name"] == "radial" else 131072
+        sample.append({**s, "x": s["x"][:m], "y": s["y"][:m], "c": s["c"][:m], "M": m})
+    t0 = time.perf_counter()
+    for s in sample:
+        O.nufft_type1([s["x"], s["y"]], s["c"], N_MODES, eps=EPS)
+        O.nufft_type2([s["x"], s["y"]], s["f"], eps=EPS)
+    dt = time.perf_counter() - t0
+    return {"value": points_per_step(sample) / dt, "unit": "NU points/s", "cores": 1, "kind": "port",
+            "sample": f"radial first {sample[0]['M']} points + clustered first {sample[1]['M']} points, "
+                      f"one type 1 + one type 2 each, {dt:.1f} s"}
+
+
+def _spread_chunk(args):
+    O = _oracle()
+    x, y, c, nf, kp = args
+    return O.spread([O.premod(x), O.premod(y)], c, nf, kp)
+
+
+def _interp_chunk(args):
+    O = _oracle()
+    x, y, fw, kp = args
+    return O.interp([O.premod(x), O.premod(y)], fw, kp)
+
+
+def run_reference(args):
+    """Time the CPU restatement with every host core (process pool over point chunks)."""
+    import multiprocessing as mp
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    O = _oracle()
+    cores = os.cpu_count() or 1
+    sets = workload(seed=1234)
+    sample = []
+    for s in sets:
+        m = 131072 if s["name"] == "radial" else 524288
+        sample.append({**s, "x": s["x"][:m], "y": s["y"][:m], "c": s["c"][:m], "M": m})
+    kp = O.compute_kernel_params(EPS)
+    nf = [O.compute_grid_size(n, 2.0, kp.nspread) for n in N_MODES]
+    ph = [O.kernel_fourier_series(n, kp.nspread, kp.beta, kp.c) for n in nf]
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        def one_step():
+            for s in sample:
+                ch = np.array_split(np.arange(s["M"]), cores)
+                parts = pool.map(_spread_chunk, [(s["x"][i], s["y"][i], s["c"][i], nf, kp) for i in ch])
+                fw = np.sum(parts, axis=0)
+                O.deconvolve_shuffle(np.fft.ifftn(fw) * (nf[0] * nf[1]), ph, N_MODES)
+                fwh = O.deconvolve_pad(s["f"], ph, nf)
+                fw2 = np.fft.fftn(fwh)
+                pool.map(_interp_chunk, [(s["x"][i], s["y"][i], fw2, kp) for i in ch])
+
+        for _ in range(args.warmup):
+            one_step()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            one_step()
+        dt = time.perf_counter() - t0
+    pts = points_per_step(sample) * args.steps
+    value = pts / dt
+    line = {
+        "metric": METRIC, "value": value, "unit": "NU points/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c64", "data": "synthetic (seeded), bounded sample of the GPU workload",
+        "config": {"workload": "2D type-1 + type-2, 512x512 modes, nf 1024x1024, eps 1e-6, ns 8: radial "
+                               f"M={sample[0]['M']} and clustered M={sample[1]['M']} per step (sample)"},
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": "NU points/s", "cores": cores, "kind": "port",
+                         "sample": f"radial first {sample[0]['M']} + clustered first {sample[1]['M']} points"},
+        "e2e": {"value": value, "unit": "NU points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="nufftax_b200", choices=["nufftax_b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl != "reference":
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

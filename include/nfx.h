@@ -1,0 +1,160 @@
+/*
+ * nfx.h -- C ABI of the nufftax_b200 CUDA library (libnfx_b200.so, sm_100a).
+ *
+ * Plain C: device pointers, sizes and a CUDA stream passed as void*.  The caller
+ * owns every buffer (inputs, outputs and workspace); the library owns only its
+ * cuFFT plan cache.  Every entry point returns an nfx status code and never
+ * aborts; nfx_last_error() gives the message of the calling thread's last
+ * failure.  All work is enqueued on `stream` (NULL = legacy default stream) and
+ * no entry point synchronises the device.
+ *
+ * Array conventions (shared with nufftax, the reference):
+ *   coordinates   x, y, z: M reals (float or double per `precision`)
+ *   strengths     c: n_trans x M complex (interleaved re, im), transform-major
+ *   fine grid     fw: n_trans x nf3 x nf2 x nf1 complex, x fastest
+ *                 (nufftax/core/spread.py:466, 653)
+ *   modes         f: n_trans x n3 x n2 x n1 complex in CMCL order,
+ *                 k = -n/2 .. (n-1)/2 per axis (nufftax/core/deconvolve.py:27-73)
+ * Unused axes of 1D/2D problems have size 1 and NULL coordinate pointers.
+ */
+#ifndef NFX_H
+#define NFX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  NFX_OK = 0,
+  NFX_ERR_INVALID = 1,     /* bad argument (size, pointer, nspread, dim, ...) */
+  NFX_ERR_WORKSPACE = 2,   /* workspace smaller than the matching *_bytes query */
+  NFX_ERR_CUDA = 3,        /* a CUDA runtime call failed */
+  NFX_ERR_CUFFT = 4,       /* a cuFFT call failed */
+  NFX_ERR_UNSUPPORTED = 5  /* valid request outside what the kernels support */
+};
+
+enum { NFX_F32 = 0, NFX_F64 = 1 };
+
+/* Spreading/interpolation options: the grid, the ES kernel and the tiling.
+ * nspread/beta/kc are nufftax's KernelParams (nufftax/core/kernel.py:19-25,
+ * computed by compute_kernel_params, kernel.py:165-206).  tile[] = 0 and
+ * max_subproblem = 0 select the library defaults (nfx_default_tiles). */
+typedef struct nfx_opts {
+  int precision;       /* NFX_F32 (float/complex64) or NFX_F64 (double/complex128) */
+  int dim;             /* 1, 2 or 3 */
+  int nf[3];           /* fine grid size per axis (x, y, z); unused axes 1 */
+  int nspread;         /* kernel width, even, 2..16 */
+  double beta;         /* ES shape parameter */
+  double kc;           /* ES c = 4 / nspread^2 */
+  int prenorm;         /* 1: apply mod(x + pi, 2 pi) - pi before folding, as the
+                          transforms do (nufftax/transforms/nufft1.py:71); 0: fold
+                          only, as the core spread / interp functions do */
+  int tile[3];         /* bin edge per axis in cells; 0 = default */
+  int max_subproblem;  /* points per subproblem; 0 = default */
+} nfx_opts;
+
+/* Library identity and last error of the calling thread. */
+int nfx_version(void);
+const char* nfx_last_error(void);
+int nfx_num_sms(void);
+
+/* Fill tile[] / max_subproblem with the defaults the library would use. */
+int nfx_default_tiles(nfx_opts* opts);
+
+/* ---- bin sort --------------------------------------------------------------
+ * Bytes of workspace a sort of M points needs, and the sort itself: a stable
+ * counting sort of the points by the tile of their footprint's left cell.  The
+ * workspace then holds the permutation and the bin/subproblem tables that every
+ * *_sorted call below reads; it stays valid while the coordinates are unchanged.
+ * (No counterpart in the reference, which spreads unsorted points.) */
+int nfx_sort_workspace_bytes(const nfx_opts* opts, int64_t M, size_t* bytes);
+int nfx_sort_points(const nfx_opts* opts, const void* x, const void* y, const void* z, int64_t M, void* workspace,
+                    size_t workspace_bytes, void* stream);
+/* Copy the sort results out of a workspace (device pointers, any may be NULL):
+ * keys[M], perm[M] (int32) and bin_start[nbins + 1]. */
+int nfx_sort_results(const nfx_opts* opts, int64_t M, const void* workspace, size_t workspace_bytes, int* keys,
+                     int* perm, int* bin_start, int* nbins, void* stream);
+
+/* ---- spread / interp -------------------------------------------------------
+ * Replace nufftax/core/spread.py:717-758:
+ *   _spread_{1,2,3}d_dispatch(x[, y[, z]], c, nf1[, nf2[, nf3]], kernel_params) -> fw
+ *   _interp_{1,2,3}d_dispatch(x[, y[, z]], fw, kernel_params) -> c
+ * nfx_spread / nfx_interp sort first (workspace of nfx_sort_workspace_bytes);
+ * the *_sorted forms reuse a workspace already filled by nfx_sort_points.
+ * nfx_spread* overwrite fw (it is zeroed on the stream first). */
+int nfx_spread(const nfx_opts* opts, const void* x, const void* y, const void* z, int64_t M, const void* c,
+               int n_trans, void* fw, void* workspace, size_t workspace_bytes, void* stream);
+int nfx_interp(const nfx_opts* opts, const void* x, const void* y, const void* z, int64_t M, const void* fw,
+               int n_trans, void* c_out, void* workspace, size_t workspace_bytes, void* stream);
+int nfx_spread_sorted(const nfx_opts* opts, const void* x, const void* y, const void* z, int64_t M, const void* c,
+                      int n_trans, void* fw, const void* workspace, size_t workspace_bytes, void* stream);
+int nfx_interp_sorted(const nfx_opts* opts, const void* x, const void* y, const void* z, int64_t M, const void* fw,
+                      int n_trans, void* c_out, const void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---- adjoints (ES-derivative coordinate gradients) ---------------------------
+ * Replace the backward rules of the core custom_vjp's
+ * (nufftax/core/spread.py:766-1305; torch convention G = dL/dRe + i dL/dIm):
+ *   nfx_spread_grad_sorted: given the grid cotangent g (n_trans x grid) and the
+ *     forward strengths c, writes dc = interp(g) (if dc != NULL) and
+ *     d{x,y,z}[j] = sum_t Re(conj(c[t,j]) * sum_cells g * dphi/d{x,y,z})
+ *     (spread.py:820-858, 997-1032, 1168-1212), all in one pass over the tiles.
+ *   nfx_interp_grad_sorted: given the grid fw and the point cotangent g,
+ *     d{x,y,z}[j] = sum_t Re(conj(g[t,j]) * sum_cells fw * dphi/d{x,y,z})
+ *     (spread.py:911-944, 1080-1114, 1261-1305); the fw cotangent is
+ *     nfx_spread_sorted(g).
+ * Coordinate outputs are reals of the working precision; NULL skips an axis. */
+int nfx_spread_grad_sorted(const nfx_opts* opts, const void* x, const void* y, const void* z, int64_t M,
+                           const void* c, const void* g_grid, int n_trans, void* dc, void* dx, void* dy, void* dz,
+                           const void* workspace, size_t workspace_bytes, void* stream);
+int nfx_interp_grad_sorted(const nfx_opts* opts, const void* x, const void* y, const void* z, int64_t M,
+                           const void* fw, const void* g_pts, int n_trans, void* dx, void* dy, void* dz,
+                           const void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---- deconvolution / mode reordering ----------------------------------------
+ * fac1..fac3: per-axis factors (-1)^k / phihat(|k|) in CMCL order (device arrays
+ * of n_modes[d] reals; NULL for unused axes), nufftax/core/deconvolve.py:27-56.
+ * nfx_deconv_shuffle replaces deconvolve_shuffle_{1,2,3}d (deconvolve.py:81-111,
+ * 174-224, 312-366); nfx_deconv_pad replaces deconvolve_pad_{1,2,3}d
+ * (deconvolve.py:114-166, 227-304, 369-468) and writes every grid cell. */
+int nfx_deconv_shuffle(int precision, int dim, const int nf[3], const int n_modes[3], const void* fac1,
+                       const void* fac2, const void* fac3, const void* fw_hat, void* f_out, int n_trans,
+                       void* stream);
+int nfx_deconv_pad(int precision, int dim, const int nf[3], const int n_modes[3], const void* fac1, const void* fac2,
+                   const void* fac3, const void* f_in, void* fw_hat, int n_trans, void* stream);
+
+/* ---- FFT (cuFFT, cached plans) ----------------------------------------------
+ * In-place batched C2C over the last `dim` axes of n_trans grids.
+ * sign = +1: sum_n v[n] e^{+2 pi i k n / nf} (nufftax's ifftn(.) * prod(nf));
+ * sign = -1: e^{-...} (fftn).  nufftax/transforms/nufft1.py:81,154,232-235;
+ * nufft2.py:317,383,454-457. */
+int nfx_fft(int precision, int dim, const int nf[3], int n_trans, void* data, int sign, void* stream);
+int nfx_fft_cache_clear(void);
+
+/* ---- type 3 helpers (nufftax/transforms/nufft3.py:216-515) -------------------
+ * nfx_t3_prepare: from source coordinates (dim arrays of M) and target
+ *   frequencies (dim arrays of K) computes, on the device and without a host
+ *   round trip, the centres C, D, half-widths S and scales gamma, h per axis
+ *   (nufft3.py:268-281) into `params` (a device buffer of nfx_t3_params_bytes()),
+ *   then writes the rescaled folded sources xn_d = mod((x_d - C_d)/gamma_d + pi,
+ *   2 pi) - pi, the pre-phased strengths c' = c e^{i isign sum_d D_d x_d}
+ *   (n_trans x M), the rescaled folded targets sn_d = mod(h_d gamma_d (s_d - D_d)
+ *   + pi, 2 pi) - pi, and the per-target output factor
+ *   e^{i isign sum_d (s_d - D_d) C_d} / prod_d phihat(h_d gamma_d (s_d - D_d))
+ *   (nufft3.py:176-213, 390-394).  nf[d] is the type-3 grid per axis.
+ * nfx_t3_finish: out[t][k] *= factor[k]. */
+size_t nfx_t3_params_bytes(void);
+int nfx_t3_prepare(int precision, int dim, const int nf[3], int nspread, double beta, double kc, double upsampfac,
+                   int isign, const void* const* src, int64_t M, const void* c, int n_trans, const void* const* tgt,
+                   int64_t K, void* params, void* const* src_out, void* c_out, void* const* tgt_out, void* factor,
+                   void* scratch, size_t scratch_bytes, void* stream);
+size_t nfx_t3_scratch_bytes(int precision, int64_t M, int64_t K);
+int nfx_t3_finish(int precision, const void* factor, int64_t K, int n_trans, void* out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NFX_H */

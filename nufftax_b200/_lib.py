@@ -1,0 +1,128 @@
+"""ctypes binding of libnfx_b200.so (the C ABI declared in include/nfx.h).
+
+The library is required: importing the compute entry points without it raises,
+there is no CPU fallback.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import re
+import threading
+from ctypes import POINTER, c_double, c_int, c_int64, c_size_t, c_void_p
+from pathlib import Path
+
+LIB_PATH = Path(__file__).with_name("libnfx_b200.so")
+HEADER_PATH = Path(__file__).resolve().parent.parent / "include" / "nfx.h"
+
+NFX_OK = 0
+NFX_ERR_INVALID = 1
+NFX_ERR_WORKSPACE = 2
+NFX_ERR_CUDA = 3
+NFX_ERR_CUFFT = 4
+NFX_ERR_UNSUPPORTED = 5
+NFX_F32 = 0
+NFX_F64 = 1
+
+_STATUS = {
+    NFX_ERR_INVALID: ValueError,
+    NFX_ERR_WORKSPACE: ValueError,
+    NFX_ERR_UNSUPPORTED: NotImplementedError,
+}
+
+
+class NfxError(RuntimeError):
+    """A CUDA or cuFFT failure reported by libnfx_b200."""
+
+
+class NfxOpts(ctypes.Structure):
+    """Mirror of `nfx_opts` in include/nfx.h."""
+
+    _fields_ = [
+        ("precision", c_int),
+        ("dim", c_int),
+        ("nf", c_int * 3),
+        ("nspread", c_int),
+        ("beta", c_double),
+        ("kc", c_double),
+        ("prenorm", c_int),
+        ("tile", c_int * 3),
+        ("max_subproblem", c_int),
+    ]
+
+
+_vp = c_void_p
+_SIGNATURES = {
+    "nfx_version": ([], c_int),
+    "nfx_last_error": ([], ctypes.c_char_p),
+    "nfx_num_sms": ([], c_int),
+    "nfx_default_tiles": ([POINTER(NfxOpts)], c_int),
+    "nfx_sort_workspace_bytes": ([POINTER(NfxOpts), c_int64, POINTER(c_size_t)], c_int),
+    "nfx_sort_points": ([POINTER(NfxOpts), _vp, _vp, _vp, c_int64, _vp, c_size_t, _vp], c_int),
+    "nfx_sort_results": ([POINTER(NfxOpts), c_int64, _vp, c_size_t, _vp, _vp, _vp, POINTER(c_int), _vp], c_int),
+    "nfx_spread": ([POINTER(NfxOpts), _vp, _vp, _vp, c_int64, _vp, c_int, _vp, _vp, c_size_t, _vp], c_int),
+    "nfx_interp": ([POINTER(NfxOpts), _vp, _vp, _vp, c_int64, _vp, c_int, _vp, _vp, c_size_t, _vp], c_int),
+    "nfx_spread_sorted": ([POINTER(NfxOpts), _vp, _vp, _vp, c_int64, _vp, c_int, _vp, _vp, c_size_t, _vp], c_int),
+    "nfx_interp_sorted": ([POINTER(NfxOpts), _vp, _vp, _vp, c_int64, _vp, c_int, _vp, _vp, c_size_t, _vp], c_int),
+    "nfx_spread_grad_sorted": (
+        [POINTER(NfxOpts), _vp, _vp, _vp, c_int64, _vp, _vp, c_int, _vp, _vp, _vp, _vp, _vp, c_size_t, _vp], c_int),
+    "nfx_interp_grad_sorted": (
+        [POINTER(NfxOpts), _vp, _vp, _vp, c_int64, _vp, _vp, c_int, _vp, _vp, _vp, _vp, c_size_t, _vp], c_int),
+    "nfx_deconv_shuffle": ([c_int, c_int, POINTER(c_int), POINTER(c_int), _vp, _vp, _vp, _vp, _vp, c_int, _vp],
+                           c_int),
+    "nfx_deconv_pad": ([c_int, c_int, POINTER(c_int), POINTER(c_int), _vp, _vp, _vp, _vp, _vp, c_int, _vp], c_int),
+    "nfx_fft": ([c_int, c_int, POINTER(c_int), c_int, _vp, c_int, _vp], c_int),
+    "nfx_fft_cache_clear": ([], c_int),
+    "nfx_t3_params_bytes": ([], c_size_t),
+    "nfx_t3_scratch_bytes": ([c_int, c_int64, c_int64], c_size_t),
+    "nfx_t3_prepare": ([c_int, c_int, POINTER(c_int), c_int, c_double, c_double, c_double, c_int, POINTER(c_void_p),
+                        c_int64, _vp, c_int, POINTER(c_void_p), c_int64, _vp, POINTER(c_void_p), _vp,
+                        POINTER(c_void_p), _vp, _vp, c_size_t, _vp], c_int),
+    "nfx_t3_finish": ([c_int, _vp, c_int64, c_int, _vp, _vp], c_int),
+}
+
+_lock = threading.Lock()
+_lib: ctypes.CDLL | None = None
+
+
+def header_symbols() -> list[str]:
+    """Function names declared in include/nfx.h."""
+    text = HEADER_PATH.read_text()
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?[a-z_0-9]+\**\s+\**(nfx_[a-z0-9_]+)\s*\(", text, re.M)))
+
+
+def load() -> ctypes.CDLL:
+    """Load libnfx_b200.so once and attach argument types; raise if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not LIB_PATH.exists():
+            raise RuntimeError(
+                f"{LIB_PATH.name} is not built; run `python -m nufftax_b200._build` (nvcc, sm_100a). "
+                "nufftax_b200 has no CPU fallback.")
+        lib = ctypes.CDLL(str(LIB_PATH))
+        for name, (args, res) in _SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = lib
+        return lib
+
+
+def check(status: int, what: str) -> None:
+    """Raise the Python exception matching an nfx status code."""
+    if status == NFX_OK:
+        return
+    msg = load().nfx_last_error().decode(errors="replace")
+    exc = _STATUS.get(status, NfxError)
+    raise exc(f"{what} failed (nfx status {status}): {msg}")
+
+
+def int3(vals) -> ctypes.Array:
+    arr = (c_int * 3)(1, 1, 1)
+    for i, v in enumerate(vals):
+        arr[i] = int(v)
+    return arr

@@ -1,0 +1,583 @@
+// extern "C" entry points of libnfx_b200 (declared in include/nfx.h).
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
+
+#include "nfx.h"
+#include "nfx_spreadinterp.cuh"
+
+namespace nfx {
+
+// Per-dimension dispatchers, instantiated in nfx_si_{f32,f64}_{1,2,3}d.cu.
+template <typename T, int DIM>
+cudaError_t dispatch_spread(int ns, const PointArgs<T>& a, const void* c, void* fw, cudaStream_t st);
+template <typename T, int DIM>
+cudaError_t dispatch_interp(int ns, const PointArgs<T>& a, const void* fw, void* out, cudaStream_t st);
+template <typename T, int DIM>
+cudaError_t dispatch_grad(int ns, const PointArgs<T>& a, const void* G, const void* V, void* oi, void* dx, void* dy,
+                          void* dz, cudaStream_t st);
+
+#define NFX_EXTERN(T, D)                                                                                           \
+  extern template cudaError_t dispatch_spread<T, D>(int, const PointArgs<T>&, const void*, void*, cudaStream_t);   \
+  extern template cudaError_t dispatch_interp<T, D>(int, const PointArgs<T>&, const void*, void*, cudaStream_t);   \
+  extern template cudaError_t dispatch_grad<T, D>(int, const PointArgs<T>&, const void*, const void*, void*, void*, \
+                                                  void*, void*, cudaStream_t);
+NFX_EXTERN(float, 1)
+NFX_EXTERN(float, 2)
+NFX_EXTERN(float, 3)
+NFX_EXTERN(double, 1)
+NFX_EXTERN(double, 2)
+NFX_EXTERN(double, 3)
+#undef NFX_EXTERN
+
+static thread_local std::string g_last_error;
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+int num_sms() {
+  static std::mutex mu;
+  static std::map<int, int> cache;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = cache.find(dev);
+  if (it != cache.end()) return it->second;
+  int n = 0;
+  if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+  cache[dev] = n;
+  return n;
+}
+
+cudaError_t ensure_smem(const void* fn, size_t smem) {
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, size_t> done;
+  if (smem <= 48 * 1024) return cudaSuccess;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(mu);
+  auto k = std::make_pair(fn, dev);
+  if (done[k] >= smem) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess) done[k] = smem;
+  return e;
+}
+
+cudaError_t kernel_grid(const void* fn, int threads, size_t smem, int64_t max_work, int& grid) {
+  static std::mutex mu;
+  static std::map<std::tuple<const void*, int, size_t, int>, int> occ;
+  static std::map<std::pair<const void*, int>, size_t> smem_attr;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int per_sm = 0;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto key = std::make_tuple(fn, dev, smem, threads);
+    auto it = occ.find(key);
+    if (it != occ.end()) {
+      per_sm = it->second;
+    } else {
+      auto ak = std::make_pair(fn, dev);
+      if (smem > 48 * 1024 && smem_attr[ak] < smem) {
+        cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        smem_attr[ak] = smem;
+      }
+      cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem);
+      if (e != cudaSuccess) return e;
+      if (per_sm < 1) return cudaErrorInvalidConfiguration;
+      occ[key] = per_sm;
+    }
+  }
+  int64_t want = (int64_t)num_sms() * per_sm;
+  if (max_work < 1) max_work = 1;
+  grid = (int)std::min<int64_t>(want, max_work);
+  return cudaSuccess;
+}
+
+// ---------------------------------------------------------------------------
+// Options -> geometry and sort layout
+// ---------------------------------------------------------------------------
+constexpr int kMaxBins = 49152;
+constexpr size_t kSmemBudget = 200 * 1024;
+
+static size_t real_bytes(int precision) { return precision == NFX_F64 ? 8 : 4; }
+
+static int choose_pitch(int pad0, int ns) {
+  // Rows of one footprint are `ns` cells wide and a warp covers 32/ns rows;
+  // a pitch that is an odd multiple of ns (mod 32) puts those rows in disjoint
+  // bank ranges.
+  // Accept at most ~12% of extra row length for it.
+  if (ns == 2 || ns == 4 || ns == 8 || ns == 16) {
+    const int limit = pad0 + std::max(1, pad0 / 8);
+    for (int p = pad0; p <= limit; ++p)
+      if (p % ns == 0 && ((p / ns) % 2 == 1)) return p;
+  }
+  return pad0;
+}
+
+static void fill_geom(const nfx_opts* o, Geom& g) {
+  g.dim = o->dim;
+  for (int d = 0; d < 3; ++d) {
+    bool act = d < o->dim;
+    g.nf[d] = act ? o->nf[d] : 1;
+    g.tile[d] = act ? o->tile[d] : 1;
+    g.nb[d] = act ? (g.nf[d] + g.tile[d] - 1) / g.tile[d] : 1;
+    g.pad[d] = act ? g.tile[d] + o->nspread - 1 : 1;
+  }
+  g.pitch = choose_pitch(g.pad[0], o->nspread);
+  g.nbins = g.nb[0] * g.nb[1] * g.nb[2];
+  g.prenorm = o->prenorm;
+}
+
+static int validate_opts(const nfx_opts* o) {
+  if (o == nullptr) {
+    set_error("opts is NULL");
+    return NFX_ERR_INVALID;
+  }
+  if (o->precision != NFX_F32 && o->precision != NFX_F64) {
+    set_error("precision must be NFX_F32 or NFX_F64");
+    return NFX_ERR_INVALID;
+  }
+  if (o->dim < 1 || o->dim > 3) {
+    set_error("dim must be 1, 2 or 3");
+    return NFX_ERR_INVALID;
+  }
+  if (o->nspread < 2 || o->nspread > 16 || (o->nspread & 1)) {
+    set_error("nspread must be even and in [2, 16]");
+    return NFX_ERR_UNSUPPORTED;
+  }
+  for (int d = 0; d < o->dim; ++d) {
+    if (o->nf[d] < 1 || o->nf[d] > (1 << 28)) {
+      set_error("nf out of range");
+      return NFX_ERR_INVALID;
+    }
+    if (o->tile[d] < 0) {
+      set_error("tile must be >= 0");
+      return NFX_ERR_INVALID;
+    }
+  }
+  int64_t grid = 1;
+  for (int d = 0; d < o->dim; ++d) grid *= o->nf[d];
+  if (grid > ((int64_t)1 << 31) - 1) {
+    set_error("fine grid larger than 2^31 - 1 cells");
+    return NFX_ERR_UNSUPPORTED;
+  }
+  if (o->max_subproblem < 0) {
+    set_error("max_subproblem must be >= 0");
+    return NFX_ERR_INVALID;
+  }
+  return NFX_OK;
+}
+
+// Resolve tile[] = 0 / max_subproblem = 0 to defaults, keep the bin count and
+// the shared memory of every kernel within budget.
+static int resolve_opts(const nfx_opts* in, nfx_opts& o) {
+  int st = validate_opts(in);
+  if (st != NFX_OK) return st;
+  o = *in;
+  const int ns = o.nspread;
+  const size_t rb = real_bytes(o.precision);
+  int def[3];
+  if (o.dim == 1) {
+    def[0] = 512;
+  } else if (o.dim == 2) {
+    def[0] = def[1] = 32;
+  } else {
+    def[0] = 16;
+    def[1] = 16;
+    def[2] = 8;
+  }
+  bool user_tiles = true;
+  for (int d = 0; d < o.dim; ++d)
+    if (o.tile[d] == 0) {
+      user_tiles = false;
+      o.tile[d] = std::min(def[d], o.nf[d]);
+    }
+  for (int d = o.dim; d < 3; ++d) o.tile[d] = 1;
+  if (!user_tiles) {
+    // Shrink the largest tile edge while a kernel's shared memory is over
+    // budget; grow the edge of the axis with the most bins while there are too
+    // many bins for the sort (only if the result still fits).
+    for (int it = 0; it < 64; ++it) {
+      Geom g;
+      fill_geom(&o, g);
+      const bool smem_ok = spread_smem_bytes(rb, o.dim, ns, g) <= kSmemBudget && tile_smem_bytes(rb, g) <= kSmemBudget;
+      if (!smem_ok) {
+        int dmax = 0;
+        for (int d = 1; d < o.dim; ++d)
+          if (o.tile[d] > o.tile[dmax]) dmax = d;
+        if (o.tile[dmax] <= 2) break;
+        o.tile[dmax] = (o.tile[dmax] + 1) / 2;
+        continue;
+      }
+      if (g.nbins <= kMaxBins) break;
+      int dmax = 0;
+      for (int d = 1; d < o.dim; ++d)
+        if (g.nb[d] > g.nb[dmax]) dmax = d;
+      nfx_opts trial = o;
+      trial.tile[dmax] = std::min(o.tile[dmax] * 2, o.nf[dmax]);
+      Geom gt;
+      fill_geom(&trial, gt);
+      if (spread_smem_bytes(rb, o.dim, ns, gt) > kSmemBudget || tile_smem_bytes(rb, gt) > kSmemBudget) break;
+      o = trial;
+    }
+  }
+  if (o.max_subproblem == 0) o.max_subproblem = (o.dim == 3) ? 2048 : 1024;
+  Geom g;
+  fill_geom(&o, g);
+  if (g.nbins > kMaxBins) {
+    set_error("too many bins for the sort (raise tile)");
+    return NFX_ERR_UNSUPPORTED;
+  }
+  if (spread_smem_bytes(rb, o.dim, ns, g) > kSmemBudget || tile_smem_bytes(rb, g) > kSmemBudget) {
+    set_error("tile too large for shared memory (lower tile)");
+    return NFX_ERR_UNSUPPORTED;
+  }
+  return NFX_OK;
+}
+
+static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
+
+static void make_layout(const nfx_opts& o, const Geom& g, int64_t M, SortLayout& L) {
+  L.M = M;
+  L.nbins = g.nbins;
+  const int64_t target = std::max<int64_t>((int64_t)1 << 20, M / 4);
+  int64_t chunk = 1024;
+  while ((int64_t)g.nbins * ((M + chunk - 1) / chunk) > target && chunk < ((int64_t)1 << 30)) chunk *= 2;
+  L.chunk = (int)chunk;
+  L.nchunks = (int)std::max<int64_t>(1, (M + chunk - 1) / chunk);
+  L.sort_warps = (int)std::max<int64_t>(1, std::min<int64_t>(8, (96 * 1024) / ((int64_t)g.nbins * 4)));
+  L.sort_smem = (size_t)L.sort_warps * g.nbins * sizeof(int);
+  L.n_counts = (int64_t)g.nbins * L.nchunks;
+  L.scan_blocks = scan_blocks(L.n_counts);
+  L.maxsub = o.max_subproblem;
+  L.max_subs = g.nbins + (M + L.maxsub - 1) / L.maxsub;
+  size_t off = 0;
+  L.off_keys = off;
+  off += align256((size_t)M * 4);
+  L.off_perm = off;
+  off += align256((size_t)M * 4);
+  L.off_counts = off;
+  off += align256((size_t)L.n_counts * 4);
+  L.off_scan = off;
+  off += align256((size_t)L.scan_blocks * 4 + 4);
+  L.off_bin_start = off;
+  off += align256((size_t)(g.nbins + 1) * 4);
+  L.off_sub_bin = off;
+  off += align256((size_t)L.max_subs * 4);
+  L.off_sub_start = off;
+  off += align256((size_t)L.max_subs * 4);
+  L.off_nsub = off;
+  off += 256;
+  L.total = off;
+}
+
+static SortPtrs carve(const SortLayout& L, void* ws) {
+  char* b = (char*)ws;
+  SortPtrs P;
+  P.keys = (int*)(b + L.off_keys);
+  P.perm = (int*)(b + L.off_perm);
+  P.counts = (int*)(b + L.off_counts);
+  P.scan_tmp = (int*)(b + L.off_scan);
+  P.bin_start = (int*)(b + L.off_bin_start);
+  P.sub_bin = (int*)(b + L.off_sub_bin);
+  P.sub_start = (int*)(b + L.off_sub_start);
+  P.nsub = (int*)(b + L.off_nsub);
+  return P;
+}
+
+static SortView view(const SortLayout& L, const void* ws) {
+  SortPtrs P = carve(L, const_cast<void*>(ws));
+  SortView v;
+  v.perm = P.perm;
+  v.bin_start = P.bin_start;
+  v.sub_bin = P.sub_bin;
+  v.sub_start = P.sub_start;
+  v.nsub = P.nsub;
+  v.maxsub = L.maxsub;
+  v.max_subs = L.max_subs;
+  return v;
+}
+
+static int cuda_fail(cudaError_t e, const char* where) {
+  set_error(std::string(where) + ": " + cudaGetErrorString(e));
+  return NFX_ERR_CUDA;
+}
+
+struct Prepared {
+  nfx_opts o;
+  Geom g;
+  SortLayout L;
+};
+
+static int prepare(const nfx_opts* in, int64_t M, const void* x, const void* y, const void* z, const void* ws,
+                   size_t ws_bytes, Prepared& P) {
+  int st = resolve_opts(in, P.o);
+  if (st != NFX_OK) return st;
+  if (M < 0 || M > (int64_t)INT32_MAX - 1) {
+    set_error("M must be in [0, 2^31 - 2]");
+    return NFX_ERR_INVALID;
+  }
+  if (M > 0) {
+    const void* cs[3] = {x, y, z};
+    for (int d = 0; d < P.o.dim; ++d)
+      if (cs[d] == nullptr) {
+        set_error("coordinate pointer is NULL");
+        return NFX_ERR_INVALID;
+      }
+  }
+  fill_geom(&P.o, P.g);
+  make_layout(P.o, P.g, M, P.L);
+  if (ws == nullptr || ws_bytes < P.L.total) {
+    set_error("workspace too small: need " + std::to_string(P.L.total) + " bytes");
+    return NFX_ERR_WORKSPACE;
+  }
+  return NFX_OK;
+}
+
+template <typename T>
+static cudaError_t spread_dim(const Prepared& P, const void* x, const void* y, const void* z, int64_t M, const void* c,
+                              int n_trans, void* fw, const void* ws, cudaStream_t st) {
+  PointArgs<T> a = make_args<T>(P.g, P.o.beta, P.o.kc, x, y, z, M, n_trans, view(P.L, ws));
+  switch (P.o.dim) {
+    case 1:
+      return dispatch_spread<T, 1>(P.o.nspread, a, c, fw, st);
+    case 2:
+      return dispatch_spread<T, 2>(P.o.nspread, a, c, fw, st);
+    default:
+      return dispatch_spread<T, 3>(P.o.nspread, a, c, fw, st);
+  }
+}
+
+template <typename T>
+static cudaError_t interp_dim(const Prepared& P, const void* x, const void* y, const void* z, int64_t M,
+                              const void* fw, int n_trans, void* out, const void* ws, cudaStream_t st) {
+  PointArgs<T> a = make_args<T>(P.g, P.o.beta, P.o.kc, x, y, z, M, n_trans, view(P.L, ws));
+  switch (P.o.dim) {
+    case 1:
+      return dispatch_interp<T, 1>(P.o.nspread, a, fw, out, st);
+    case 2:
+      return dispatch_interp<T, 2>(P.o.nspread, a, fw, out, st);
+    default:
+      return dispatch_interp<T, 3>(P.o.nspread, a, fw, out, st);
+  }
+}
+
+template <typename T>
+static cudaError_t grad_dim(const Prepared& P, const void* x, const void* y, const void* z, int64_t M, const void* G,
+                            const void* V, int n_trans, void* oi, void* dx, void* dy, void* dz, const void* ws,
+                            cudaStream_t st) {
+  PointArgs<T> a = make_args<T>(P.g, P.o.beta, P.o.kc, x, y, z, M, n_trans, view(P.L, ws));
+  switch (P.o.dim) {
+    case 1:
+      return dispatch_grad<T, 1>(P.o.nspread, a, G, V, oi, dx, nullptr, nullptr, st);
+    case 2:
+      return dispatch_grad<T, 2>(P.o.nspread, a, G, V, oi, dx, dy, nullptr, st);
+    default:
+      return dispatch_grad<T, 3>(P.o.nspread, a, G, V, oi, dx, dy, dz, st);
+  }
+}
+
+static int64_t grid_cells(const Geom& g) { return (int64_t)g.nf[0] * g.nf[1] * g.nf[2]; }
+
+}  // namespace nfx
+
+using namespace nfx;
+
+extern "C" {
+
+int nfx_version(void) { return 10000; }
+const char* nfx_last_error(void) { return g_last_error.c_str(); }
+int nfx_num_sms(void) { return num_sms(); }
+
+int nfx_default_tiles(nfx_opts* opts) {
+  nfx_opts o;
+  int st = resolve_opts(opts, o);
+  if (st != NFX_OK) return st;
+  for (int d = 0; d < 3; ++d) opts->tile[d] = o.tile[d];
+  opts->max_subproblem = o.max_subproblem;
+  return NFX_OK;
+}
+
+int nfx_sort_workspace_bytes(const nfx_opts* opts, int64_t M, size_t* bytes) {
+  Prepared P;
+  int st = resolve_opts(opts, P.o);
+  if (st != NFX_OK) return st;
+  if (M < 0 || bytes == nullptr) {
+    set_error("M < 0 or bytes is NULL");
+    return NFX_ERR_INVALID;
+  }
+  fill_geom(&P.o, P.g);
+  make_layout(P.o, P.g, M, P.L);
+  *bytes = P.L.total;
+  return NFX_OK;
+}
+
+int nfx_sort_points(const nfx_opts* opts, const void* x, const void* y, const void* z, int64_t M, void* ws,
+                    size_t ws_bytes, void* stream) {
+  Prepared P;
+  int st = prepare(opts, M, x, y, z, ws, ws_bytes, P);
+  if (st != NFX_OK) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  SortPtrs ptr = carve(P.L, ws);
+  if (M == 0) {
+    cudaError_t e = cudaMemsetAsync(ptr.bin_start, 0, (size_t)(P.g.nbins + 1) * 4, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(ptr.nsub, 0, 4, s);
+    return e == cudaSuccess ? NFX_OK : cuda_fail(e, "nfx_sort_points");
+  }
+  cudaError_t e = P.o.precision == NFX_F32 ? launch_sort<float>(P.L, P.g, P.o.nspread, x, y, z, M, ptr, s)
+                                           : launch_sort<double>(P.L, P.g, P.o.nspread, x, y, z, M, ptr, s);
+  return e == cudaSuccess ? NFX_OK : cuda_fail(e, "nfx_sort_points");
+}
+
+int nfx_sort_results(const nfx_opts* opts, int64_t M, const void* ws, size_t ws_bytes, int* keys, int* perm,
+                     int* bin_start, int* nbins, void* stream) {
+  Prepared P;
+  int st = prepare(opts, M, (const void*)1, (const void*)1, (const void*)1, ws, ws_bytes, P);
+  if (st != NFX_OK) return st;
+  if (nbins) *nbins = P.g.nbins;
+  cudaStream_t s = (cudaStream_t)stream;
+  SortPtrs ptr = carve(P.L, const_cast<void*>(ws));
+  cudaError_t e = cudaSuccess;
+  if (keys && M > 0) e = cudaMemcpyAsync(keys, ptr.keys, (size_t)M * 4, cudaMemcpyDeviceToDevice, s);
+  if (e == cudaSuccess && perm && M > 0) e = cudaMemcpyAsync(perm, ptr.perm, (size_t)M * 4, cudaMemcpyDeviceToDevice, s);
+  if (e == cudaSuccess && bin_start)
+    e = cudaMemcpyAsync(bin_start, ptr.bin_start, (size_t)(P.g.nbins + 1) * 4, cudaMemcpyDeviceToDevice, s);
+  return e == cudaSuccess ? NFX_OK : cuda_fail(e, "nfx_sort_results");
+}
+
+int nfx_spread_sorted(const nfx_opts* opts, const void* x, const void* y, const void* z, int64_t M, const void* c,
+                      int n_trans, void* fw, const void* ws, size_t ws_bytes, void* stream) {
+  Prepared P;
+  int st = prepare(opts, M, x, y, z, ws, ws_bytes, P);
+  if (st != NFX_OK) return st;
+  if (n_trans < 1 || fw == nullptr || (M > 0 && c == nullptr)) {
+    set_error("n_trans < 1 or NULL c / fw");
+    return NFX_ERR_INVALID;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t cb = 2 * real_bytes(P.o.precision);
+  cudaError_t e = cudaMemsetAsync(fw, 0, (size_t)grid_cells(P.g) * n_trans * cb, s);
+  if (e != cudaSuccess) return cuda_fail(e, "nfx_spread_sorted memset");
+  if (M == 0) return NFX_OK;
+  e = P.o.precision == NFX_F32 ? spread_dim<float>(P, x, y, z, M, c, n_trans, fw, ws, s)
+                               : spread_dim<double>(P, x, y, z, M, c, n_trans, fw, ws, s);
+  return e == cudaSuccess ? NFX_OK : cuda_fail(e, "nfx_spread_sorted");
+}
+
+int nfx_interp_sorted(const nfx_opts* opts, const void* x, const void* y, const void* z, int64_t M, const void* fw,
+                      int n_trans, void* c_out, const void* ws, size_t ws_bytes, void* stream) {
+  Prepared P;
+  int st = prepare(opts, M, x, y, z, ws, ws_bytes, P);
+  if (st != NFX_OK) return st;
+  if (n_trans < 1 || fw == nullptr || (M > 0 && c_out == nullptr)) {
+    set_error("n_trans < 1 or NULL fw / c_out");
+    return NFX_ERR_INVALID;
+  }
+  if (M == 0) return NFX_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e = P.o.precision == NFX_F32 ? interp_dim<float>(P, x, y, z, M, fw, n_trans, c_out, ws, s)
+                                           : interp_dim<double>(P, x, y, z, M, fw, n_trans, c_out, ws, s);
+  return e == cudaSuccess ? NFX_OK : cuda_fail(e, "nfx_interp_sorted");
+}
+
+int nfx_spread(const nfx_opts* opts, const void* x, const void* y, const void* z, int64_t M, const void* c,
+               int n_trans, void* fw, void* ws, size_t ws_bytes, void* stream) {
+  int st = nfx_sort_points(opts, x, y, z, M, ws, ws_bytes, stream);
+  if (st != NFX_OK) return st;
+  return nfx_spread_sorted(opts, x, y, z, M, c, n_trans, fw, ws, ws_bytes, stream);
+}
+
+int nfx_interp(const nfx_opts* opts, const void* x, const void* y, const void* z, int64_t M, const void* fw,
+               int n_trans, void* c_out, void* ws, size_t ws_bytes, void* stream) {
+  int st = nfx_sort_points(opts, x, y, z, M, ws, ws_bytes, stream);
+  if (st != NFX_OK) return st;
+  return nfx_interp_sorted(opts, x, y, z, M, fw, n_trans, c_out, ws, ws_bytes, stream);
+}
+
+int nfx_spread_grad_sorted(const nfx_opts* opts, const void* x, const void* y, const void* z, int64_t M,
+                           const void* c, const void* g_grid, int n_trans, void* dc, void* dx, void* dy, void* dz,
+                           const void* ws, size_t ws_bytes, void* stream) {
+  Prepared P;
+  int st = prepare(opts, M, x, y, z, ws, ws_bytes, P);
+  if (st != NFX_OK) return st;
+  if (n_trans < 1 || g_grid == nullptr || (M > 0 && c == nullptr)) {
+    set_error("n_trans < 1 or NULL c / g_grid");
+    return NFX_ERR_INVALID;
+  }
+  if (M == 0) return NFX_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e = P.o.precision == NFX_F32
+                      ? grad_dim<float>(P, x, y, z, M, g_grid, c, n_trans, dc, dx, dy, dz, ws, s)
+                      : grad_dim<double>(P, x, y, z, M, g_grid, c, n_trans, dc, dx, dy, dz, ws, s);
+  return e == cudaSuccess ? NFX_OK : cuda_fail(e, "nfx_spread_grad_sorted");
+}
+
+int nfx_interp_grad_sorted(const nfx_opts* opts, const void* x, const void* y, const void* z, int64_t M,
+                           const void* fw, const void* g_pts, int n_trans, void* dx, void* dy, void* dz,
+                           const void* ws, size_t ws_bytes, void* stream) {
+  Prepared P;
+  int st = prepare(opts, M, x, y, z, ws, ws_bytes, P);
+  if (st != NFX_OK) return st;
+  if (n_trans < 1 || fw == nullptr || (M > 0 && g_pts == nullptr)) {
+    set_error("n_trans < 1 or NULL fw / g_pts");
+    return NFX_ERR_INVALID;
+  }
+  if (M == 0) return NFX_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e = P.o.precision == NFX_F32
+                      ? grad_dim<float>(P, x, y, z, M, fw, g_pts, n_trans, nullptr, dx, dy, dz, ws, s)
+                      : grad_dim<double>(P, x, y, z, M, fw, g_pts, n_trans, nullptr, dx, dy, dz, ws, s);
+  return e == cudaSuccess ? NFX_OK : cuda_fail(e, "nfx_interp_grad_sorted");
+}
+
+static int check_deconv(int precision, int dim, const int nf[3], const int nm[3], const void* fac1, const void* fac2,
+                        const void* fac3, int n_trans, int nf_full[3], int nm_full[3]) {
+  if ((precision != NFX_F32 && precision != NFX_F64) || dim < 1 || dim > 3 || nf == nullptr || nm == nullptr ||
+      fac1 == nullptr || (dim >= 2 && fac2 == nullptr) || (dim >= 3 && fac3 == nullptr) || n_trans < 1) {
+    set_error("invalid deconvolution arguments");
+    return NFX_ERR_INVALID;
+  }
+  for (int d = 0; d < 3; ++d) {
+    nf_full[d] = d < dim ? nf[d] : 1;
+    nm_full[d] = d < dim ? nm[d] : 1;
+    if (nf_full[d] < 1 || nm_full[d] < 0 || nm_full[d] > nf_full[d]) {
+      set_error("need 0 <= n_modes <= nf per axis");
+      return NFX_ERR_INVALID;
+    }
+  }
+  return NFX_OK;
+}
+
+int nfx_deconv_shuffle(int precision, int dim, const int nf[3], const int n_modes[3], const void* fac1,
+                       const void* fac2, const void* fac3, const void* fw_hat, void* f_out, int n_trans,
+                       void* stream) {
+  int nff[3], nmf[3];
+  int st = check_deconv(precision, dim, nf, n_modes, fac1, fac2, fac3, n_trans, nff, nmf);
+  if (st != NFX_OK) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e = precision == NFX_F32
+                      ? launch_deconv_shuffle<float>(dim, nff, nmf, (const float*)fac1, (const float*)fac2,
+                                                     (const float*)fac3, fw_hat, f_out, n_trans, s)
+                      : launch_deconv_shuffle<double>(dim, nff, nmf, (const double*)fac1, (const double*)fac2,
+                                                      (const double*)fac3, fw_hat, f_out, n_trans, s);
+  return e == cudaSuccess ? NFX_OK : cuda_fail(e, "nfx_deconv_shuffle");
+}
+
+int nfx_deconv_pad(int precision, int dim, const int nf[3], const int n_modes[3], const void* fac1, const void* fac2,
+                   const void* fac3, const void* f_in, void* fw_hat, int n_trans, void* stream) {
+  int nff[3], nmf[3];
+  int st = check_deconv(precision, dim, nf, n_modes, fac1, fac2, fac3, n_trans, nff, nmf);
+  if (st != NFX_OK) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e = precision == NFX_F32
+                      ? launch_deconv_pad<float>(dim, nff, nmf, (const float*)fac1, (const float*)fac2,
+                                                 (const float*)fac3, f_in, fw_hat, n_trans, s)
+                      : launch_deconv_pad<double>(dim, nff, nmf, (const double*)fac1, (const double*)fac2,
+                                                  (const double*)fac3, f_in, fw_hat, n_trans, s);
+  return e == cudaSuccess ? NFX_OK : cuda_fail(e, "nfx_deconv_pad");
+}
+
+}  // extern "C"

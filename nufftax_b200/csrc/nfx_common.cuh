@@ -1,0 +1,124 @@
+// Shared device helpers for the nufftax_b200 CUDA library (sm_100a).
+//
+// Coordinate folding is written with explicitly rounded intrinsics so that no
+// multiply-add is ever contracted: the integer cell and bin indices derived from
+// it are bit-identical to a CPU evaluation of the same float operations
+// (nufftax/core/spread.py:78-97 fold_rescale, nufftax/transforms/nufft1.py:71
+// jnp.mod(x + pi, 2 pi) - pi, nufftax/core/spread.py:214 i0 = ceil(xs - ns/2)).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace nfx {
+
+template <typename T> struct C2;
+template <> struct C2<float> { using type = float2; };
+template <> struct C2<double> { using type = double2; };
+template <typename T> using cplx_t = typename C2<T>::type;
+
+// ---- explicitly rounded arithmetic (no FMA contraction) -------------------
+__device__ __forceinline__ float rn_mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float rn_add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float rn_sub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double rn_mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double rn_add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double rn_sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float t_floor(float a) { return floorf(a); }
+__device__ __forceinline__ double t_floor(double a) { return floor(a); }
+__device__ __forceinline__ float t_fmod(float a, float b) { return fmodf(a, b); }
+__device__ __forceinline__ double t_fmod(double a, double b) { return fmod(a, b); }
+__device__ __forceinline__ int ceil_to_int(float a) { return __float2int_ru(a); }
+__device__ __forceinline__ int ceil_to_int(double a) { return __double2int_ru(a); }
+__device__ __forceinline__ float t_exp(float a) { return expf(a); }
+__device__ __forceinline__ double t_exp(double a) { return exp(a); }
+__device__ __forceinline__ float t_sqrt(float a) { return sqrtf(a); }
+__device__ __forceinline__ double t_sqrt(double a) { return sqrt(a); }
+
+// Constants rounded to the working type the way JAX weak typing rounds Python
+// floats: the double value first, then one conversion.
+constexpr double kPi = 3.141592653589793;
+constexpr double kTwoPi = 2.0 * 3.141592653589793;
+constexpr double kInvTwoPi = 1.0 / (2.0 * 3.141592653589793);
+
+// jnp.mod(x + pi, 2 pi) - pi: lax.rem (exact fmod) plus the sign fix of
+// jnp.remainder (add the divisor when the remainder is negative and non-zero).
+template <typename T>
+__device__ __forceinline__ T premod(T x) {
+  const T pi = (T)kPi;
+  const T two_pi = (T)kTwoPi;
+  T a = rn_add(x, pi);
+  T r = t_fmod(a, two_pi);
+  if (r != (T)0 && r < (T)0) r = rn_add(r, two_pi);
+  return rn_sub(r, pi);
+}
+
+// fold_rescale: ((x * (1/2pi) + 0.5) - floor(.)) * nf, one rounding per op.
+template <typename T>
+__device__ __forceinline__ T fold_rescale(T x, int nf) {
+  T t = rn_mul(x, (T)kInvTwoPi);
+  t = rn_add(t, (T)0.5);
+  t = rn_sub(t, t_floor(t));
+  return rn_mul(t, (T)nf);
+}
+
+template <typename T>
+__device__ __forceinline__ T scaled_coord(T x, int nf, int prenorm) {
+  return fold_rescale(prenorm ? premod(x) : x, nf);
+}
+
+// Left cell of the footprint: i0 = ceil(xs - ns/2).
+template <typename T, int NS>
+__device__ __forceinline__ int left_cell(T xs) {
+  return ceil_to_int(rn_sub(xs, (T)(NS / 2)));
+}
+
+// Periodic wrap of any int into [0, n).
+__device__ __forceinline__ int wrap_index(int i, int n) {
+  int r = i % n;
+  return r < 0 ? r + n : r;
+}
+
+// ES kernel value phi(z) = exp(beta (sqrt(1 - c z^2) - 1)), zero where the
+// argument is negative (nufftax/core/kernel.py:79-111; arg = 1 - (c z) z).
+template <typename T>
+__device__ __forceinline__ T es_weight(T z, T beta, T kc) {
+  T arg = (T)1 - (kc * z) * z;
+  T w = t_exp(beta * (t_sqrt(arg > (T)0 ? arg : (T)0) - (T)1));
+  return arg >= (T)0 ? w : (T)0;
+}
+
+// phi and dphi/dz (nufftax/core/kernel.py:114-162; dphi masked where arg <= 1e-14).
+template <typename T>
+__device__ __forceinline__ void es_weight_deriv(T z, T beta, T kc, T& phi, T& dphi) {
+  const T tiny = (T)1e-14;
+  T arg = (T)1 - (kc * z) * z;
+  T sq = t_sqrt(arg > tiny ? arg : tiny);
+  T w = t_exp(beta * (sq - (T)1));
+  phi = arg >= (T)0 ? w : (T)0;
+  T d = -beta * kc * z / sq * phi;
+  dphi = arg > tiny ? d : (T)0;
+}
+
+// Vectorised global reduction of a complex64 value (one 8-byte red).
+__device__ __forceinline__ void red_add(float2* addr, float2 v) {
+  asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(addr), "f"(v.x), "f"(v.y) : "memory");
+}
+__device__ __forceinline__ void red_add(double2* addr, double2 v) {
+  atomicAdd(&addr->x, v.x);
+  atomicAdd(&addr->y, v.y);
+}
+
+// Grid geometry shared by the sort, spread and interp kernels (plain values).
+struct Geom {
+  int dim;
+  int nf[3];     // fine grid per axis (x, y, z); unused axes are 1
+  int tile[3];   // bin edge in cells per axis; unused axes are 1
+  int nb[3];     // bins per axis
+  int pad[3];    // padded tile extent (tile + ns - 1) per axis; 1 for unused
+  int pitch;     // shared-memory row pitch along x (>= pad[0])
+  int nbins;
+  int prenorm;
+};
+
+}  // namespace nfx

@@ -1,0 +1,120 @@
+// Fused deconvolution + mode reordering around the FFT.
+//
+// Type 1 (nufftax/core/deconvolve.py:81-111, 174-224, 312-366): one pass reads
+//   the FFT output at k mod nf for every kept mode k in CMCL order
+//   (k = -N/2 .. (N-1)/2 per axis) and multiplies by the per-axis factors
+//   fac_d[k] = (-1)^k / phihat_d(|k|) (deconvolve.py:27-56), outer product in the
+//   reference's order (fac3 * fac2) * fac1.  Output is written coalesced along x.
+// Type 2 (deconvolve.py:114-166, 227-304, 369-468): one pass writes every
+//   cell of the fine grid: the deconvolved mode where the cell is a kept mode,
+//   zero elsewhere (no separate memset of the grid).
+#include "nfx_internal.h"
+
+namespace nfx {
+
+template <typename T>
+__global__ void k_deconv_shuffle(int nf1, int nf2, int nf3, int n1, int n2, int n3, const T* __restrict__ f1,
+                                 const T* __restrict__ f2, const T* __restrict__ f3,
+                                 const cplx_t<T>* __restrict__ in, cplx_t<T>* __restrict__ out, int n_trans) {
+  using CT = cplx_t<T>;
+  const int64_t per = (int64_t)n1 * n2 * n3;
+  const int64_t total = per * n_trans;
+  const int64_t grid = (int64_t)nf1 * nf2 * nf3;
+  const int k1min = -(n1 / 2), k2min = -(n2 / 2), k3min = -(n3 / 2);
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t t = i / per;
+    int64_t r = i - t * per;
+    const int p1 = (int)(r % n1);
+    r /= n1;
+    const int p2 = (int)(r % n2);
+    const int p3 = (int)(r / n2);
+    int i1 = p1 + k1min;
+    int i2 = p2 + k2min;
+    int i3 = p3 + k3min;
+    if (i1 < 0) i1 += nf1;
+    if (i2 < 0) i2 += nf2;
+    if (i3 < 0) i3 += nf3;
+    const CT v = in[t * grid + ((int64_t)i3 * nf2 + i2) * nf1 + i1];
+    T fac = f1[p1];
+    if (f2 != nullptr) fac = (f3 != nullptr ? f3[p3] * f2[p2] : f2[p2]) * f1[p1];
+    CT o;
+    o.x = v.x * fac;
+    o.y = v.y * fac;
+    out[i] = o;
+  }
+}
+
+template <typename T>
+__global__ void k_deconv_pad(int nf1, int nf2, int nf3, int n1, int n2, int n3, const T* __restrict__ f1,
+                             const T* __restrict__ f2, const T* __restrict__ f3, const cplx_t<T>* __restrict__ in,
+                             cplx_t<T>* __restrict__ out, int n_trans) {
+  using CT = cplx_t<T>;
+  const int64_t grid = (int64_t)nf1 * nf2 * nf3;
+  const int64_t total = grid * n_trans;
+  const int64_t per = (int64_t)n1 * n2 * n3;
+  const int k1max = (n1 - 1) / 2, k2max = (n2 - 1) / 2, k3max = (n3 - 1) / 2;
+  const int k1min = -(n1 / 2), k2min = -(n2 / 2), k3min = -(n3 / 2);
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t t = i / grid;
+    int64_t r = i - t * grid;
+    const int c1 = (int)(r % nf1);
+    r /= nf1;
+    const int c2 = (int)(r % nf2);
+    const int c3 = (int)(r / nf2);
+    // mode of this cell per axis, or none
+    const int k1 = c1 <= k1max ? c1 : (c1 >= nf1 + k1min ? c1 - nf1 : INT32_MIN);
+    const int k2 = c2 <= k2max ? c2 : (c2 >= nf2 + k2min ? c2 - nf2 : INT32_MIN);
+    const int k3 = c3 <= k3max ? c3 : (c3 >= nf3 + k3min ? c3 - nf3 : INT32_MIN);
+    CT o;
+    o.x = (T)0;
+    o.y = (T)0;
+    if (k1 != INT32_MIN && k2 != INT32_MIN && k3 != INT32_MIN) {
+      const int p1 = k1 - k1min, p2 = k2 - k2min, p3 = k3 - k3min;
+      const CT v = in[t * per + ((int64_t)p3 * n2 + p2) * n1 + p1];
+      T fac = f1[p1];
+      if (f2 != nullptr) fac = (f3 != nullptr ? f3[p3] * f2[p2] : f2[p2]) * f1[p1];
+      o.x = v.x * fac;
+      o.y = v.y * fac;
+    }
+    out[i] = o;
+  }
+}
+
+static unsigned elementwise_grid(int64_t n) {
+  int64_t want = (n + 255) / 256;
+  int64_t cap = (int64_t)num_sms() * 16;
+  return (unsigned)(want < cap ? (want > 0 ? want : 1) : cap);
+}
+
+template <typename T>
+cudaError_t launch_deconv_shuffle(int dim, const int nf[3], const int nm[3], const T* f1, const T* f2, const T* f3,
+                                  const void* fw_hat, void* out, int n_trans, cudaStream_t st) {
+  const int64_t total = (int64_t)nm[0] * nm[1] * nm[2] * n_trans;
+  if (total == 0) return cudaSuccess;
+  k_deconv_shuffle<T><<<elementwise_grid(total), 256, 0, st>>>(
+      nf[0], nf[1], nf[2], nm[0], nm[1], nm[2], f1, dim >= 2 ? f2 : nullptr, dim >= 3 ? f3 : nullptr,
+      (const cplx_t<T>*)fw_hat, (cplx_t<T>*)out, n_trans);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_deconv_pad(int dim, const int nf[3], const int nm[3], const T* f1, const T* f2, const T* f3,
+                              const void* f_in, void* fw_hat, int n_trans, cudaStream_t st) {
+  const int64_t total = (int64_t)nf[0] * nf[1] * nf[2] * n_trans;
+  if (total == 0) return cudaSuccess;
+  k_deconv_pad<T><<<elementwise_grid(total), 256, 0, st>>>(nf[0], nf[1], nf[2], nm[0], nm[1], nm[2], f1,
+                                                           dim >= 2 ? f2 : nullptr, dim >= 3 ? f3 : nullptr,
+                                                           (const cplx_t<T>*)f_in, (cplx_t<T>*)fw_hat, n_trans);
+  return cudaGetLastError();
+}
+
+template cudaError_t launch_deconv_shuffle<float>(int, const int*, const int*, const float*, const float*,
+                                                  const float*, const void*, void*, int, cudaStream_t);
+template cudaError_t launch_deconv_shuffle<double>(int, const int*, const int*, const double*, const double*,
+                                                   const double*, const void*, void*, int, cudaStream_t);
+template cudaError_t launch_deconv_pad<float>(int, const int*, const int*, const float*, const float*, const float*,
+                                              const void*, void*, int, cudaStream_t);
+template cudaError_t launch_deconv_pad<double>(int, const int*, const int*, const double*, const double*,
+                                               const double*, const void*, void*, int, cudaStream_t);
+
+}  // namespace nfx

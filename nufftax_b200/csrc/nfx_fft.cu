@@ -1,0 +1,86 @@
+// cuFFT glue: a mutex-guarded cache of batched in-place C2C/Z2Z plans keyed by
+// (device, precision, dims, batch).  Replaces the jnp.fft calls of
+// nufftax/transforms/nufft1.py:81,154,232-235 and nufft2.py:317,383,454-457:
+// sign = +1 is the unnormalised inverse transform (nufftax's ifftn(.) * prod(nf)),
+// sign = -1 the forward transform.
+#include <cufft.h>
+
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
+
+#include "nfx.h"
+#include "nfx_internal.h"
+
+namespace nfx {
+
+namespace {
+using PlanKey = std::tuple<int, int, int, int, int, int, int>;  // dev, prec, dim, nf1, nf2, nf3, batch
+std::mutex g_plan_mu;
+std::map<PlanKey, cufftHandle>& plans() {
+  static std::map<PlanKey, cufftHandle> m;
+  return m;
+}
+
+int cufft_fail(cufftResult r, const char* where) {
+  set_error(std::string(where) + ": cuFFT error " + std::to_string((int)r));
+  return NFX_ERR_CUFFT;
+}
+}  // namespace
+
+}  // namespace nfx
+
+using namespace nfx;
+
+extern "C" {
+
+int nfx_fft(int precision, int dim, const int nf[3], int n_trans, void* data, int sign, void* stream) {
+  if ((precision != NFX_F32 && precision != NFX_F64) || dim < 1 || dim > 3 || nf == nullptr || n_trans < 1 ||
+      data == nullptr || (sign != 1 && sign != -1)) {
+    set_error("invalid nfx_fft arguments");
+    return NFX_ERR_INVALID;
+  }
+  int n[3];
+  long long dist = 1;
+  for (int d = 0; d < dim; ++d) {
+    if (nf[d] < 1) {
+      set_error("nf < 1");
+      return NFX_ERR_INVALID;
+    }
+    n[d] = nf[dim - 1 - d];  // slowest axis first for cuFFT
+    dist *= nf[d];
+  }
+  int dev = 0;
+  cudaGetDevice(&dev);
+  PlanKey key(dev, precision, dim, nf[0], dim > 1 ? nf[1] : 1, dim > 2 ? nf[2] : 1, n_trans);
+  std::lock_guard<std::mutex> lk(g_plan_mu);
+  cufftHandle plan;
+  auto it = plans().find(key);
+  if (it == plans().end()) {
+    cufftResult r = cufftPlanMany(&plan, dim, n, nullptr, 1, (int)dist, nullptr, 1, (int)dist,
+                                  precision == NFX_F32 ? CUFFT_C2C : CUFFT_Z2Z, n_trans);
+    if (r != CUFFT_SUCCESS) return cufft_fail(r, "cufftPlanMany");
+    plans()[key] = plan;
+  } else {
+    plan = it->second;
+  }
+  cufftResult r = cufftSetStream(plan, (cudaStream_t)stream);
+  if (r != CUFFT_SUCCESS) return cufft_fail(r, "cufftSetStream");
+  const int dir = sign > 0 ? CUFFT_INVERSE : CUFFT_FORWARD;
+  if (precision == NFX_F32)
+    r = cufftExecC2C(plan, (cufftComplex*)data, (cufftComplex*)data, dir);
+  else
+    r = cufftExecZ2Z(plan, (cufftDoubleComplex*)data, (cufftDoubleComplex*)data, dir);
+  if (r != CUFFT_SUCCESS) return cufft_fail(r, "cufftExec");
+  return NFX_OK;
+}
+
+int nfx_fft_cache_clear(void) {
+  std::lock_guard<std::mutex> lk(g_plan_mu);
+  for (auto& kv : plans()) cufftDestroy(kv.second);
+  plans().clear();
+  return NFX_OK;
+}
+
+}  // extern "C"

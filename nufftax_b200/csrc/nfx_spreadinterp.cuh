@@ -1,0 +1,508 @@
+// Tile spreading, interpolation and ES-derivative gradient kernels.
+//
+// Work unit: a subproblem = up to `maxsub` consecutive sorted points of one bin.
+// All of a bin's footprints lie in its padded tile (tile + ns - 1 cells per
+// axis, periodic wrap applied only when the tile is read from / flushed to the
+// fine grid), so each CTA works entirely in shared memory:
+//
+//  * spread (nufftax/core/spread.py:285-339, 435-494, 596-658; Pallas twin
+//    nufftax/core/pallas_spread.py:337-613): points are staged 32 at a time per
+//    warp (each lane folds one point and evaluates its d*ns ES weights once);
+//    the warp then walks the 32 footprints cell by cell, lane l taking cells
+//    l, l+32, ... of the same point, so every shared-memory atomic of one
+//    instruction hits a distinct address (no same-address serialisation even for
+//    heavily clustered points).  The finished tile is flushed with one vectorised
+//    `red.global.add.v2.f32` per non-zero cell, coalesced along x.
+//  * interp (nufftax/core/spread.py:342-381, 497-540, 661-709): the padded tile
+//    is staged into shared memory with coalesced loads, then each thread
+//    evaluates one point as a separable sum (x innermost); no atomics.
+//  * grad (nufftax/core/spread.py:820-1305): the same staged tile, with the ES
+//    derivative weights (dphi/dx = -phi'(z) nf / 2pi) for each axis, giving the
+//    interpolated value and all coordinate gradients in one pass.
+#pragma once
+
+#include "nfx_internal.h"
+
+namespace nfx {
+
+template <int NS, int DIM>
+struct Pow {
+  static constexpr int value = NS * Pow<NS, DIM - 1>::value;
+};
+template <int NS>
+struct Pow<NS, 0> {
+  static constexpr int value = 1;
+};
+
+template <typename T>
+struct PointArgs {
+  const T* x;
+  const T* y;
+  const T* z;
+  int64_t M;
+  int n_trans;
+  int64_t grid_stride;  // complex elements per transform of the fine grid
+  Geom g;
+  T beta, kc;
+  SortView s;
+};
+
+__device__ __forceinline__ void bin_origin(const Geom& g, int b, int& o0, int& o1, int& o2) {
+  int bx = b % g.nb[0];
+  int r = b / g.nb[0];
+  int by = r % g.nb[1];
+  int bz = r / g.nb[1];
+  o0 = bx * g.tile[0];
+  o1 = by * g.tile[1];
+  o2 = bz * g.tile[2];
+}
+
+__device__ __forceinline__ int wrap_up(int i, int n) {
+  while (i >= n) i -= n;
+  return i;
+}
+
+template <typename T>
+__device__ __forceinline__ T coord(const PointArgs<T>& a, int d, int p) {
+  return d == 0 ? a.x[p] : (d == 1 ? a.y[p] : a.z[p]);
+}
+
+// ---------------------------------------------------------------------------
+// Spread
+// ---------------------------------------------------------------------------
+template <typename T, int DIM, int NS, int NW>
+__global__ void __launch_bounds__(NW * 32) k_spread(PointArgs<T> a, const cplx_t<T>* __restrict__ c,
+                                                    cplx_t<T>* __restrict__ fw) {
+  using CT = cplx_t<T>;
+  constexpr int CELLS = Pow<NS, DIM>::value;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const Geom& g = a.g;
+  const int tile_cells = g.pad[2] * g.pad[1] * g.pitch;
+  T* s_re = reinterpret_cast<T*>(smem_raw);
+  T* s_im = s_re + tile_cells;
+  T* s_w = s_im + tile_cells;                  // NW*32*DIM*NS
+  T* s_c = s_w + NW * 32 * DIM * NS;           // NW*32*2
+  int* s_off = reinterpret_cast<int*>(s_c + NW * 32 * 2);  // NW*32
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const int row = g.pitch;
+  const int plane = g.pitch * g.pad[1];
+  const int nsub = *a.s.nsub;
+  const int used = g.pad[0] * g.pad[1] * g.pad[2];
+
+  for (int sidx = blockIdx.x; sidx < nsub; sidx += gridDim.x) {
+    const int b = a.s.sub_bin[sidx];
+    const int k0 = a.s.sub_start[sidx];
+    const int k1 = min(k0 + a.s.maxsub, a.s.bin_start[b + 1]);
+    int o[3];
+    bin_origin(g, b, o[0], o[1], o[2]);
+    for (int t = 0; t < a.n_trans; ++t) {
+      for (int i = threadIdx.x; i < 2 * tile_cells; i += blockDim.x) s_re[i] = (T)0;
+      __syncthreads();
+      for (int kb = k0 + warp * 32; kb < k1; kb += NW * 32) {
+        const int k = kb + lane;
+        const int slot = warp * 32 + lane;
+        if (k < k1) {
+          const int p = a.s.perm[k];
+          int off = 0;
+          bool inside = true;
+#pragma unroll
+          for (int d = 0; d < DIM; ++d) {
+            const T xs = scaled_coord(coord(a, d, p), g.nf[d], g.prenorm);
+            const int i0 = left_cell<T, NS>(xs);
+            const int l = wrap_index(i0, g.nf[d]) - o[d];
+            // A point outside its bin's tile can only come from coordinates
+            // changed after the sort; it is dropped instead of indexing out of
+            // the tile.
+            inside = inside && (unsigned)l < (unsigned)g.tile[d];
+            off += l * (d == 0 ? 1 : (d == 1 ? row : plane));
+            T* w = s_w + (slot * DIM + d) * NS;
+#pragma unroll
+            for (int q = 0; q < NS; ++q) w[q] = es_weight(rn_sub((T)(i0 + q), xs), a.beta, a.kc);
+          }
+          const CT cv = c[(int64_t)t * a.M + p];
+          s_off[slot] = inside ? off : 0;
+          s_c[2 * slot] = inside ? cv.x : (T)0;
+          s_c[2 * slot + 1] = inside ? cv.y : (T)0;
+        }
+        __syncwarp();
+        const int cnt = min(32, k1 - kb);
+        const int items = cnt * CELLS;
+        for (int it = lane; it < items; it += 32) {
+          const int j = it / CELLS;
+          const int q = it - j * CELLS;
+          const int kx = q % NS;
+          const int ky = (q / NS) % NS;
+          const int kz = q / (NS * NS);
+          const int sj = warp * 32 + j;
+          const T* wj = s_w + sj * DIM * NS;
+          T w;
+          if (DIM == 1)
+            w = wj[kx];
+          else if (DIM == 2)
+            w = wj[NS + ky] * wj[kx];
+          else
+            w = (wj[2 * NS + kz] * wj[NS + ky]) * wj[kx];
+          const int addr = s_off[sj] + kz * plane + ky * row + kx;
+          atomicAdd(&s_re[addr], s_c[2 * sj] * w);
+          atomicAdd(&s_im[addr], s_c[2 * sj + 1] * w);
+        }
+        __syncwarp();
+      }
+      __syncthreads();
+      CT* out = fw + (int64_t)t * a.grid_stride;
+      for (int i = threadIdx.x; i < used; i += blockDim.x) {
+        const int lx = i % g.pad[0];
+        const int r = i / g.pad[0];
+        const int ly = r % g.pad[1];
+        const int lz = r / g.pad[1];
+        const int si = lz * plane + ly * row + lx;
+        const T vr = s_re[si], vi = s_im[si];
+        if (vr != (T)0 || vi != (T)0) {
+          const int gx = wrap_up(o[0] + lx, g.nf[0]);
+          const int gy = wrap_up(o[1] + ly, g.nf[1]);
+          const int gz = wrap_up(o[2] + lz, g.nf[2]);
+          CT v;
+          v.x = vr;
+          v.y = vi;
+          red_add(out + ((int64_t)gz * g.nf[1] + gy) * g.nf[0] + gx, v);
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Stage a padded tile of one transform's grid into shared memory (interleaved).
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void stage_tile(const Geom& g, const int o[3], const cplx_t<T>* __restrict__ grid,
+                                           cplx_t<T>* s_tile) {
+  const int row = g.pitch;
+  const int plane = g.pitch * g.pad[1];
+  const int nrows = g.pad[1] * g.pad[2];
+  // one warp per row, lanes along x: coalesced
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int r = warp; r < nrows; r += nw) {
+    const int ly = r % g.pad[1];
+    const int lz = r / g.pad[1];
+    const int gy = wrap_up(o[1] + ly, g.nf[1]);
+    const int gz = wrap_up(o[2] + lz, g.nf[2]);
+    const cplx_t<T>* src = grid + ((int64_t)gz * g.nf[1] + gy) * g.nf[0];
+    cplx_t<T>* dst = s_tile + lz * plane + ly * row;
+    for (int lx = lane; lx < g.pad[0]; lx += 32) dst[lx] = src[wrap_up(o[0] + lx, g.nf[0])];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Interp
+// ---------------------------------------------------------------------------
+template <typename T, int DIM, int NS, int NW>
+__global__ void __launch_bounds__(NW * 32) k_interp(PointArgs<T> a, const cplx_t<T>* __restrict__ fw,
+                                                    cplx_t<T>* __restrict__ cout) {
+  using CT = cplx_t<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  CT* s_tile = reinterpret_cast<CT*>(smem_raw);
+  const Geom& g = a.g;
+  const int row = g.pitch;
+  const int plane = g.pitch * g.pad[1];
+  const int nsub = *a.s.nsub;
+  for (int sidx = blockIdx.x; sidx < nsub; sidx += gridDim.x) {
+    const int b = a.s.sub_bin[sidx];
+    const int k0 = a.s.sub_start[sidx];
+    const int k1 = min(k0 + a.s.maxsub, a.s.bin_start[b + 1]);
+    int o[3];
+    bin_origin(g, b, o[0], o[1], o[2]);
+    for (int t = 0; t < a.n_trans; ++t) {
+      __syncthreads();
+      stage_tile<T>(g, o, fw + (int64_t)t * a.grid_stride, s_tile);
+      __syncthreads();
+      for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
+        const int p = a.s.perm[k];
+        T w[DIM][NS];
+        int off = 0;
+        bool inside = true;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+          const T xs = scaled_coord(coord(a, d, p), g.nf[d], g.prenorm);
+          const int i0 = left_cell<T, NS>(xs);
+          const int l = wrap_index(i0, g.nf[d]) - o[d];
+          inside = inside && (unsigned)l < (unsigned)g.tile[d];
+          off += l * (d == 0 ? 1 : (d == 1 ? row : plane));
+#pragma unroll
+          for (int q = 0; q < NS; ++q) w[d][q] = es_weight(rn_sub((T)(i0 + q), xs), a.beta, a.kc);
+        }
+        if (!inside) {  // stale sort: see k_spread
+          CT zero;
+          zero.x = zero.y = (T)0;
+          cout[(int64_t)t * a.M + p] = zero;
+          continue;
+        }
+        T ar = 0, ai = 0;
+        const CT* base = s_tile + off;
+#pragma unroll 1
+        for (int kz = 0; kz < (DIM == 3 ? NS : 1); ++kz) {
+          T zr = 0, zi = 0;
+#pragma unroll
+          for (int ky = 0; ky < (DIM >= 2 ? NS : 1); ++ky) {
+            const CT* rp = base + kz * plane + ky * row;
+            T xr = 0, xi = 0;
+#pragma unroll
+            for (int kx = 0; kx < NS; ++kx) {
+              const CT v = rp[kx];
+              xr += v.x * w[0][kx];
+              xi += v.y * w[0][kx];
+            }
+            if (DIM >= 2) {
+              zr += xr * w[DIM >= 2 ? 1 : 0][ky];
+              zi += xi * w[DIM >= 2 ? 1 : 0][ky];
+            } else {
+              zr += xr;
+              zi += xi;
+            }
+          }
+          if (DIM == 3) {
+            ar += zr * w[DIM - 1][kz];
+            ai += zi * w[DIM - 1][kz];
+          } else {
+            ar += zr;
+            ai += zi;
+          }
+        }
+        CT r;
+        r.x = ar;
+        r.y = ai;
+        cout[(int64_t)t * a.M + p] = r;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Gradient pass (see launch_grad in nfx_internal.h)
+// ---------------------------------------------------------------------------
+template <typename T, int DIM, int NS, int NW>
+__global__ void __launch_bounds__(NW * 32) k_grad(PointArgs<T> a, const cplx_t<T>* __restrict__ G,
+                                                  const cplx_t<T>* __restrict__ V, cplx_t<T>* __restrict__ out_interp,
+                                                  T* __restrict__ dx, T* __restrict__ dy, T* __restrict__ dz) {
+  using CT = cplx_t<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  CT* s_tile = reinterpret_cast<CT*>(smem_raw);
+  const Geom& g = a.g;
+  const int row = g.pitch;
+  const int plane = g.pitch * g.pad[1];
+  const int nsub = *a.s.nsub;
+  T* douts[3] = {dx, dy, dz};
+  for (int sidx = blockIdx.x; sidx < nsub; sidx += gridDim.x) {
+    const int b = a.s.sub_bin[sidx];
+    const int k0 = a.s.sub_start[sidx];
+    const int k1 = min(k0 + a.s.maxsub, a.s.bin_start[b + 1]);
+    int o[3];
+    bin_origin(g, b, o[0], o[1], o[2]);
+    for (int t = 0; t < a.n_trans; ++t) {
+      __syncthreads();
+      stage_tile<T>(g, o, G + (int64_t)t * a.grid_stride, s_tile);
+      __syncthreads();
+      for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
+        const int p = a.s.perm[k];
+        T w[DIM][NS], dw[DIM][NS];
+        int off = 0;
+        bool inside = true;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+          const T xs = scaled_coord(coord(a, d, p), g.nf[d], g.prenorm);
+          const int i0 = left_cell<T, NS>(xs);
+          const int l = wrap_index(i0, g.nf[d]) - o[d];
+          inside = inside && (unsigned)l < (unsigned)g.tile[d];
+          off += l * (d == 0 ? 1 : (d == 1 ? row : plane));
+          const T scale = -(T)((double)g.nf[d] / (2.0 * kPi));
+#pragma unroll
+          for (int q = 0; q < NS; ++q) {
+            T ph, dph;
+            es_weight_deriv(rn_sub((T)(i0 + q), xs), a.beta, a.kc, ph, dph);
+            w[d][q] = ph;
+            dw[d][q] = dph * scale;
+          }
+        }
+        // S[0] = sum G w ; S[1+d] = sum G (w with axis d differentiated)
+        T sr[1 + DIM], si[1 + DIM];
+#pragma unroll
+        for (int i = 0; i <= DIM; ++i) sr[i] = si[i] = (T)0;
+        const CT* base = s_tile + (inside ? off : 0);
+#pragma unroll 1
+        for (int kz = 0; kz < (inside && DIM == 3 ? NS : (inside ? 1 : 0)); ++kz) {
+          // per-z accumulators: [0] plain, [1] d/dx, [2] d/dy
+          T zr0 = 0, zi0 = 0, zr1 = 0, zi1 = 0, zr2 = 0, zi2 = 0;
+#pragma unroll
+          for (int ky = 0; ky < (DIM >= 2 ? NS : 1); ++ky) {
+            const CT* rp = base + kz * plane + ky * row;
+            T xr = 0, xi = 0, xr1 = 0, xi1 = 0;
+#pragma unroll
+            for (int kx = 0; kx < NS; ++kx) {
+              const CT v = rp[kx];
+              xr += v.x * w[0][kx];
+              xi += v.y * w[0][kx];
+              xr1 += v.x * dw[0][kx];
+              xi1 += v.y * dw[0][kx];
+            }
+            if (DIM >= 2) {
+              const T wy = w[DIM >= 2 ? 1 : 0][ky], dwy = dw[DIM >= 2 ? 1 : 0][ky];
+              zr0 += xr * wy;
+              zi0 += xi * wy;
+              zr1 += xr1 * wy;
+              zi1 += xi1 * wy;
+              zr2 += xr * dwy;
+              zi2 += xi * dwy;
+            } else {
+              zr0 += xr;
+              zi0 += xi;
+              zr1 += xr1;
+              zi1 += xi1;
+            }
+          }
+          if (DIM == 3) {
+            const T wz = w[DIM - 1][kz], dwz = dw[DIM - 1][kz];
+            sr[0] += zr0 * wz;
+            si[0] += zi0 * wz;
+            sr[1] += zr1 * wz;
+            si[1] += zi1 * wz;
+            sr[2] += zr2 * wz;
+            si[2] += zi2 * wz;
+            sr[DIM] += zr0 * dwz;
+            si[DIM] += zi0 * dwz;
+          } else {
+            sr[0] += zr0;
+            si[0] += zi0;
+            sr[1] += zr1;
+            si[1] += zi1;
+            if (DIM == 2) {
+              sr[DIM] += zr2;
+              si[DIM] += zi2;
+            }
+          }
+        }
+        if (out_interp != nullptr) {
+          CT r;
+          r.x = sr[0];
+          r.y = si[0];
+          out_interp[(int64_t)t * a.M + p] = r;
+        }
+        const CT vv = V[(int64_t)t * a.M + p];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+          if (douts[d] != nullptr) {
+            // Re(conj(v) * s) = v.x s.x + v.y s.y ; accumulate over transforms
+            const T val = vv.x * sr[1 + d] + vv.y * si[1 + d];
+            if (t == 0)
+              douts[d][p] = val;
+            else
+              douts[d][p] += val;
+          }
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host-side launch helpers (per instantiation)
+// ---------------------------------------------------------------------------
+template <typename T, int DIM, int NS>
+struct Launch {
+  static constexpr int NW = warps_per_cta(sizeof(T), DIM, NS);
+  static size_t tile_smem(const Geom& g) { return (size_t)g.pad[2] * g.pad[1] * g.pitch * sizeof(cplx_t<T>); }
+
+  template <typename K>
+  static cudaError_t prep(K kernel, size_t smem, int& grid, int64_t max_subs) {
+    return kernel_grid(reinterpret_cast<const void*>(kernel), NW * 32, smem, max_subs, grid);
+  }
+
+  static cudaError_t spread(const PointArgs<T>& a, const cplx_t<T>* c, cplx_t<T>* fw, cudaStream_t st) {
+    size_t smem = spread_smem_bytes(sizeof(T), DIM, NS, a.g);
+    int grid = 0;
+    cudaError_t e = prep(k_spread<T, DIM, NS, NW>, smem, grid, a.s.max_subs);
+    if (e != cudaSuccess) return e;
+    k_spread<T, DIM, NS, NW><<<grid, NW * 32, smem, st>>>(a, c, fw);
+    return cudaGetLastError();
+  }
+  static cudaError_t interp(const PointArgs<T>& a, const cplx_t<T>* fw, cplx_t<T>* out, cudaStream_t st) {
+    size_t smem = tile_smem(a.g);
+    int grid = 0;
+    cudaError_t e = prep(k_interp<T, DIM, NS, NW>, smem, grid, a.s.max_subs);
+    if (e != cudaSuccess) return e;
+    k_interp<T, DIM, NS, NW><<<grid, NW * 32, smem, st>>>(a, fw, out);
+    return cudaGetLastError();
+  }
+  static cudaError_t grad(const PointArgs<T>& a, const cplx_t<T>* G, const cplx_t<T>* V, cplx_t<T>* oi, T* dx, T* dy,
+                          T* dz, cudaStream_t st) {
+    size_t smem = tile_smem(a.g);
+    int grid = 0;
+    cudaError_t e = prep(k_grad<T, DIM, NS, NW>, smem, grid, a.s.max_subs);
+    if (e != cudaSuccess) return e;
+    k_grad<T, DIM, NS, NW><<<grid, NW * 32, smem, st>>>(a, G, V, oi, dx, dy, dz);
+    return cudaGetLastError();
+  }
+};
+
+template <typename T, int DIM>
+cudaError_t dispatch_spread(int ns, const PointArgs<T>& a, const void* c, void* fw, cudaStream_t st) {
+  using CT = cplx_t<T>;
+  switch (ns) {
+#define NFX_CASE(N) \
+  case N:           \
+    return Launch<T, DIM, N>::spread(a, (const CT*)c, (CT*)fw, st);
+    NFX_CASE(2) NFX_CASE(4) NFX_CASE(6) NFX_CASE(8) NFX_CASE(10) NFX_CASE(12) NFX_CASE(14) NFX_CASE(16)
+#undef NFX_CASE
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+template <typename T, int DIM>
+cudaError_t dispatch_interp(int ns, const PointArgs<T>& a, const void* fw, void* out, cudaStream_t st) {
+  using CT = cplx_t<T>;
+  switch (ns) {
+#define NFX_CASE(N) \
+  case N:           \
+    return Launch<T, DIM, N>::interp(a, (const CT*)fw, (CT*)out, st);
+    NFX_CASE(2) NFX_CASE(4) NFX_CASE(6) NFX_CASE(8) NFX_CASE(10) NFX_CASE(12) NFX_CASE(14) NFX_CASE(16)
+#undef NFX_CASE
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+template <typename T, int DIM>
+cudaError_t dispatch_grad(int ns, const PointArgs<T>& a, const void* G, const void* V, void* oi, void* dx, void* dy,
+                          void* dz, cudaStream_t st) {
+  using CT = cplx_t<T>;
+  switch (ns) {
+#define NFX_CASE(N)                                                                                             \
+  case N:                                                                                                       \
+    return Launch<T, DIM, N>::grad(a, (const CT*)G, (const CT*)V, (CT*)oi, (T*)dx, (T*)dy, (T*)dz, st);
+    NFX_CASE(2) NFX_CASE(4) NFX_CASE(6) NFX_CASE(8) NFX_CASE(10) NFX_CASE(12) NFX_CASE(14) NFX_CASE(16)
+#undef NFX_CASE
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+template <typename T>
+PointArgs<T> make_args(const Geom& g, double beta, double kc, const void* x, const void* y, const void* z, int64_t M,
+                       int n_trans, const SortView& s) {
+  PointArgs<T> a;
+  a.x = (const T*)x;
+  a.y = (const T*)y;
+  a.z = (const T*)z;
+  a.M = M;
+  a.n_trans = n_trans;
+  a.grid_stride = (int64_t)g.nf[0] * g.nf[1] * g.nf[2];
+  a.g = g;
+  a.beta = (T)beta;
+  a.kc = (T)kc;
+  a.s = s;
+  return a;
+}
+
+}  // namespace nfx

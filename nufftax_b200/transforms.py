@@ -1,0 +1,370 @@
+"""Public NUFFT transforms nufft{1,2,3}d{1,2,3} (nufftax/transforms/autodiff.py:38-148).
+
+Signatures, defaults, batching (leading n_trans axis), output layouts and the
+`upsampfac` (forward, backward) tuple follow nufftax.  Inputs may be CUDA
+tensors (results stay on the device), CPU tensors or numpy arrays (copied to the
+current CUDA device and back).  Every numerical step runs in libnfx_b200:
+
+  type 1 (nufftax/transforms/nufft1.py:21-243): bin sort -> spread -> cuFFT ->
+         deconvolve + CMCL reorder + crop;
+  type 2 (nufftax/transforms/nufft2.py:21-227): deconvolve + zero-pad -> cuFFT ->
+         bin sort -> interp;
+  type 3 (nufftax/transforms/nufft3.py:216-515): on-device centring/scaling and
+         pre-phase -> spread -> inner type 2 -> phihat(s') and phase correction.
+
+Autograd (torch convention G = dL/dRe + i dL/dIm) replaces the JAX primitives'
+JVP/transpose rules (nufftax/transforms/primitives.py):
+  type 1: dc = type-2 adjoint pipeline of G; dx from the ES-derivative adjoint
+          kernel on the same grid (one fused pass for dc, dx, dy, dz);
+  type 2: df = type-1 adjoint pipeline of G; dx from the ES-derivative
+          interpolation of the forward fine grid;
+  type 3: dc, dx, ds through type-3 transforms of weighted cotangents
+          (primitives.py:534-659).
+"""
+
+from __future__ import annotations
+
+from ctypes import c_void_p
+from typing import Sequence
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._plan import (PointSort, complex_dtype, deconv_pad, deconv_shuffle, fft_inplace, precision_of, ptr,
+                    real_dtype, sort_cache, stream_of)
+from .grid import compute_grid_size
+from .kernel import compute_kernel_params
+
+
+def _split_upsampfac(upsampfac) -> tuple[float, float]:
+    """Scalar -> (uf, uf); (forward, backward) pair kept (autodiff.py:21-30)."""
+    if isinstance(upsampfac, (tuple, list)):
+        return float(upsampfac[0]), float(upsampfac[1])
+    return float(upsampfac), float(upsampfac)
+
+
+class _Boundary:
+    """Moves host inputs to the device and results back to the caller's kind."""
+
+    def __init__(self, *arrays):
+        self.kind = "cuda"
+        self.device = None
+        for a in arrays:
+            if isinstance(a, torch.Tensor) and a.is_cuda:
+                self.device = a.device
+                break
+        if self.device is None:
+            if not torch.cuda.is_available():
+                raise RuntimeError("nufftax_b200 needs a CUDA device (there is no CPU fallback)")
+            self.device = torch.device("cuda", torch.cuda.current_device())
+        for a in arrays:
+            if isinstance(a, np.ndarray):
+                self.kind = "numpy"
+                break
+            if isinstance(a, torch.Tensor) and not a.is_cuda:
+                self.kind = "cpu"
+
+    def to_dev(self, a, dtype=None) -> torch.Tensor:
+        if isinstance(a, np.ndarray):
+            a = torch.from_numpy(np.ascontiguousarray(a))
+        elif not isinstance(a, torch.Tensor):
+            a = torch.as_tensor(a)
+        if a.device != self.device:
+            a = a.to(self.device, non_blocking=True)
+        if dtype is not None and a.dtype != dtype:
+            a = a.to(dtype)
+        return a
+
+    def back(self, t: torch.Tensor):
+        if self.kind == "cuda":
+            return t
+        t = t.detach().cpu() if self.kind == "numpy" else t.cpu()
+        return t.numpy() if self.kind == "numpy" else t
+
+
+def _precision_for(source) -> int:
+    dt = source.dtype
+    if isinstance(dt, np.dtype) or not isinstance(dt, torch.dtype):
+        dt = torch.from_numpy(np.zeros(1, dtype=np.asarray(source).dtype)).dtype
+    if dt in (torch.complex64, torch.float32, torch.float16, torch.bfloat16):
+        return _lib.NFX_F32
+    if dt in (torch.complex128, torch.float64):
+        return _lib.NFX_F64
+    raise TypeError(f"unsupported dtype {dt}")
+
+
+def _fft_sign_type1(isign: int) -> int:
+    # nufft1.py:81 -- isign > 0: ifft * nf (e^{+}); else fft (e^{-})
+    return 1 if isign > 0 else -1
+
+
+def _fft_sign_type2(isign: int) -> int:
+    # nufft2.py:81 -- isign < 0: fft (e^{-}); else ifft * nf (e^{+})
+    return -1 if isign < 0 else 1
+
+
+# ---------------------------------------------------------------------------
+# Type 1
+# ---------------------------------------------------------------------------
+class _Type1(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, c2, n_modes, eps, isign, uf, uf_t, *coords):
+        dim = len(coords)
+        kp = compute_kernel_params(eps, uf)
+        nf = tuple(compute_grid_size(n, uf, kp.nspread) for n in n_modes)
+        ps = sort_cache.get(list(coords), nf, kp, prenorm=True)
+        fw = ps.spread(c2)
+        fft_inplace(fw, dim, _fft_sign_type1(isign))
+        f = deconv_shuffle(fw, n_modes, kp)
+        ctx.meta = (n_modes, eps, isign, uf, uf_t)
+        ctx.save_for_backward(c2, *coords)
+        return f
+
+    @staticmethod
+    def backward(ctx, G):
+        c2, *coords = ctx.saved_tensors
+        n_modes, eps, isign, uf, uf_t = ctx.meta
+        dim = len(coords)
+        need_c = ctx.needs_input_grad[0]
+        need_x = list(ctx.needs_input_grad[6:])
+        kp = compute_kernel_params(eps, uf_t)
+        nf = tuple(compute_grid_size(n, uf_t, kp.nspread) for n in n_modes)
+        H = deconv_pad(G.contiguous(), nf, kp)
+        fft_inplace(H, dim, -_fft_sign_type1(isign))
+        ps = sort_cache.get(list(coords), nf, kp, prenorm=True)
+        dc, dxs = None, [None] * dim
+        if any(need_x):
+            dc, dxs = ps.spread_grad(c2, H, need_c, need_x)
+        elif need_c:
+            dc = ps.interp(H)
+        return (dc, None, None, None, None, None, *dxs)
+
+
+def _type1(coords, c, n_modes: Sequence[int], eps, isign, upsampfac):
+    bd = _Boundary(c, *coords)
+    precision = _precision_for(c)
+    cd = bd.to_dev(c, complex_dtype(precision))
+    xs = [bd.to_dev(x, real_dtype(precision)).contiguous() for x in coords]
+    M = xs[0].shape[0]
+    batched = cd.ndim == 2
+    c2 = (cd if batched else cd.unsqueeze(0)).contiguous()
+    if c2.shape[-1] != M:
+        raise ValueError("c must have M entries along its last axis")
+    uf, uf_t = _split_upsampfac(upsampfac)
+    f = _Type1.apply(c2, tuple(int(n) for n in n_modes), float(eps), int(isign), uf, uf_t, *xs)
+    return bd.back(f if batched else f[0])
+
+
+def nufft1d1(x, c, n_modes: int, eps: float = 1e-6, isign: int = 1, upsampfac=2.0):
+    """f[k] = sum_j c[j] exp(i isign k x[j]), k = -N/2..(N-1)/2 -> (n_trans?, N)."""
+    return _type1([x], c, (int(n_modes),), eps, isign, upsampfac)
+
+
+def nufft2d1(x, y, c, n_modes, eps: float = 1e-6, isign: int = 1, upsampfac=2.0):
+    """2D type 1 -> (n_trans?, N2, N1)."""
+    n = (int(n_modes), int(n_modes)) if np.isscalar(n_modes) else tuple(int(v) for v in n_modes)
+    return _type1([x, y], c, n, eps, isign, upsampfac)
+
+
+def nufft3d1(x, y, z, c, n_modes, eps: float = 1e-6, isign: int = 1, upsampfac=2.0):
+    """3D type 1 -> (n_trans?, N3, N2, N1)."""
+    n = (int(n_modes),) * 3 if np.isscalar(n_modes) else tuple(int(v) for v in n_modes)
+    return _type1([x, y, z], c, n, eps, isign, upsampfac)
+
+
+# ---------------------------------------------------------------------------
+# Type 2
+# ---------------------------------------------------------------------------
+class _Type2(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, f2, eps, isign, uf, uf_t, *coords):
+        dim = len(coords)
+        n_modes = tuple(int(v) for v in reversed(f2.shape[1:]))
+        kp = compute_kernel_params(eps, uf)
+        nf = tuple(compute_grid_size(n, uf, kp.nspread) for n in n_modes)
+        fw = deconv_pad(f2, nf, kp)
+        fft_inplace(fw, dim, _fft_sign_type2(isign))
+        ps = sort_cache.get(list(coords), nf, kp, prenorm=True)
+        c = ps.interp(fw)
+        ctx.meta = (n_modes, eps, isign, uf, uf_t)
+        ctx.ps = ps
+        need_x = any(ctx.needs_input_grad[5:])
+        ctx.save_for_backward(*coords, fw if need_x else None)
+        return c
+
+    @staticmethod
+    def backward(ctx, G):
+        *coords, fw = ctx.saved_tensors
+        n_modes, eps, isign, uf, uf_t = ctx.meta
+        dim = len(coords)
+        need_f = ctx.needs_input_grad[0]
+        need_x = list(ctx.needs_input_grad[5:])
+        G = G.contiguous()
+        df = None
+        if need_f:
+            kp = compute_kernel_params(eps, uf_t)
+            nf = tuple(compute_grid_size(n, uf_t, kp.nspread) for n in n_modes)
+            ps_t = sort_cache.get(list(coords), nf, kp, prenorm=True)
+            gw = ps_t.spread(G)
+            fft_inplace(gw, dim, -_fft_sign_type2(isign))
+            df = deconv_shuffle(gw, n_modes, kp)
+        dxs = ctx.ps.interp_grad(fw, G, need_x) if any(need_x) else [None] * dim
+        return (df, None, None, None, None, *dxs)
+
+
+def _type2(coords, f, eps, isign, upsampfac):
+    dim = len(coords)
+    bd = _Boundary(f, *coords)
+    precision = _precision_for(f)
+    fd = bd.to_dev(f, complex_dtype(precision))
+    xs = [bd.to_dev(x, real_dtype(precision)).contiguous() for x in coords]
+    batched = fd.ndim == dim + 1
+    f2 = (fd if batched else fd.unsqueeze(0)).contiguous()
+    uf, uf_t = _split_upsampfac(upsampfac)
+    c = _Type2.apply(f2, float(eps), int(isign), uf, uf_t, *xs)
+    return bd.back(c if batched else c[0])
+
+
+def nufft1d2(x, f, eps: float = 1e-6, isign: int = -1, upsampfac=2.0):
+    """c[j] = sum_k f[k] exp(i isign k x[j]) -> (n_trans?, M)."""
+    return _type2([x], f, eps, isign, upsampfac)
+
+
+def nufft2d2(x, y, f, eps: float = 1e-6, isign: int = -1, upsampfac=2.0):
+    """2D type 2; f is (n_trans?, N2, N1)."""
+    return _type2([x, y], f, eps, isign, upsampfac)
+
+
+def nufft3d2(x, y, z, f, eps: float = 1e-6, isign: int = -1, upsampfac=2.0):
+    """3D type 2; f is (n_trans?, N3, N2, N1)."""
+    return _type2([x, y, z], f, eps, isign, upsampfac)
+
+
+# ---------------------------------------------------------------------------
+# Type 3
+# ---------------------------------------------------------------------------
+def _type3_forward(src: list[torch.Tensor], c2: torch.Tensor, tgt: list[torch.Tensor], nf: tuple[int, ...],
+                   eps: float, isign: int, uf: float) -> torch.Tensor:
+    dim = len(src)
+    dev = c2.device
+    precision = precision_of(c2.dtype)
+    rdt = real_dtype(precision)
+    M = src[0].shape[0]
+    K = tgt[0].shape[0]
+    nt = c2.shape[0]
+    kp = compute_kernel_params(eps, uf)
+    lib = _lib.load()
+    if M == 0 or K == 0:
+        return torch.zeros((nt, K), dtype=c2.dtype, device=dev)
+    params = torch.empty(int(lib.nfx_t3_params_bytes()), dtype=torch.uint8, device=dev)
+    sbytes = int(lib.nfx_t3_scratch_bytes(precision, M, K))
+    scratch = torch.empty(sbytes, dtype=torch.uint8, device=dev)
+    src_out = [torch.empty(M, dtype=rdt, device=dev) for _ in range(dim)]
+    tgt_out = [torch.empty(K, dtype=rdt, device=dev) for _ in range(dim)]
+    c_out = torch.empty_like(c2)
+    factor = torch.empty(K, dtype=c2.dtype, device=dev)
+    arr = c_void_p * 3
+
+    def parr(ts):
+        return arr(*([t.data_ptr() for t in ts] + [None] * (3 - len(ts))))
+
+    with torch.cuda.device(dev):
+        _lib.check(lib.nfx_t3_prepare(precision, dim, _lib.int3(nf), kp.nspread, kp.beta, kp.c, uf, int(isign),
+                                      parr(src), M, ptr(c2), nt, parr(tgt), K, ptr(params), parr(src_out),
+                                      ptr(c_out), parr(tgt_out), ptr(factor), ptr(scratch), sbytes,
+                                      c_void_p(stream_of(dev))), "nfx_t3_prepare")
+    # spread at the rescaled sources (fold only, like nufft3.py:283/378/483)
+    ps = PointSort(src_out, nf, kp, prenorm=False)
+    fw = ps.spread(c_out)
+    # inner type 2 on the fine grid treated as modes (nufft3.py:381-387)
+    nf_in = tuple(compute_grid_size(n, uf, kp.nspread) for n in nf)
+    fw2 = deconv_pad(fw, nf_in, kp)
+    fft_inplace(fw2, dim, _fft_sign_type2(isign))
+    ps2 = PointSort(tgt_out, nf_in, kp, prenorm=True)
+    out = ps2.interp(fw2)
+    with torch.cuda.device(dev):
+        _lib.check(lib.nfx_t3_finish(precision, ptr(factor), K, nt, ptr(out), c_void_p(stream_of(dev))),
+                   "nfx_t3_finish")
+    return out
+
+
+class _Type3(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, c2, nf, eps, isign, uf, dim, *pts):
+        src, tgt = list(pts[:dim]), list(pts[dim:])
+        ctx.meta = (nf, eps, isign, uf, dim)
+        ctx.save_for_backward(c2, *pts)
+        return _type3_forward(src, c2, tgt, nf, eps, isign, uf)
+
+    @staticmethod
+    def backward(ctx, G):
+        c2, *pts = ctx.saved_tensors
+        nf, eps, isign, uf, dim = ctx.meta
+        src, tgt = pts[:dim], pts[dim:]
+        G = G.contiguous()
+        need_c = ctx.needs_input_grad[0]
+        need = ctx.needs_input_grad[6:]
+        dc = None
+        if need_c:
+            # conjugate transpose: type 3 from targets to sources with -isign
+            dc = _type3_forward(list(tgt), G, list(src), nf, eps, -isign, uf)
+        grads = []
+        for d in range(dim):
+            if need[d]:
+                w = (-1j * isign) * tgt[d].to(G.dtype)[None, :] * G
+                T = _type3_forward(list(tgt), w.contiguous(), list(src), nf, eps, -isign, uf)
+                grads.append((c2.conj() * T).real.sum(0))
+            else:
+                grads.append(None)
+        for d in range(dim):
+            if need[dim + d]:
+                F = _type3_forward(list(src), (src[d].to(c2.dtype)[None, :] * c2).contiguous(), list(tgt), nf, eps,
+                                   isign, uf)
+                grads.append((G.conj() * (1j * isign) * F).real.sum(0))
+            else:
+                grads.append(None)
+        return (dc, None, None, None, None, None, *grads)
+
+
+def _type3(src, c, tgt, n_modes, eps, isign, upsampfac):
+    dim = len(src)
+    bd = _Boundary(c, *src, *tgt)
+    precision = _precision_for(c)
+    cd = bd.to_dev(c, complex_dtype(precision))
+    xs = [bd.to_dev(a, real_dtype(precision)).contiguous() for a in src]
+    ss = [bd.to_dev(a, real_dtype(precision)).contiguous() for a in tgt]
+    batched = cd.ndim == 2
+    c2 = (cd if batched else cd.unsqueeze(0)).contiguous()
+    nf = (int(n_modes),) if dim == 1 and np.isscalar(n_modes) else tuple(int(v) for v in n_modes)
+    if len(nf) != dim:
+        raise ValueError(f"n_modes must have {dim} entries")
+    f = _Type3.apply(c2, nf, float(eps), int(isign), float(upsampfac), dim, *xs, *ss)
+    return bd.back(f if batched else f[0])
+
+
+def nufft1d3(x, c, s, n_modes: int, eps: float = 1e-6, isign: int = 1, upsampfac: float = 2.0):
+    """f[k] = sum_j c[j] exp(i isign s[k] x[j]); n_modes from compute_type3_grid_size."""
+    return _type3([x], c, [s], n_modes, eps, isign, upsampfac)
+
+
+def nufft2d3(x, y, c, s, t, n_modes, eps: float = 1e-6, isign: int = 1, upsampfac: float = 2.0):
+    """2D type 3; n_modes = (nf1, nf2) from compute_type3_grid_sizes_2d."""
+    return _type3([x, y], c, [s, t], n_modes, eps, isign, upsampfac)
+
+
+def nufft3d3(x, y, z, c, s, t, u, n_modes, eps: float = 1e-6, isign: int = 1, upsampfac: float = 2.0):
+    """3D type 3; n_modes = (nf1, nf2, nf3) from compute_type3_grid_sizes_3d."""
+    return _type3([x, y, z], c, [s, t, u], n_modes, eps, isign, upsampfac)
+
+
+# Aliases kept by nufftax for backward compatibility (autodiff.py:153-161).
+nufft1d1_jvp = nufft1d1
+nufft1d2_jvp = nufft1d2
+nufft2d1_jvp = nufft2d1
+nufft2d2_jvp = nufft2d2
+nufft3d1_jvp = nufft3d1
+nufft3d2_jvp = nufft3d2
+nufft1d3_jvp = nufft1d3
+nufft2d3_jvp = nufft2d3
+nufft3d3_jvp = nufft3d3

@@ -1,0 +1,125 @@
+"""CPU: the C-ABI library loads and exports include/nfx.h; host-side logic.
+
+No compute call is made here (there is no GPU): only option resolution,
+workspace sizing and argument validation, which return before touching CUDA.
+"""
+
+import ctypes
+from ctypes import byref, c_size_t
+
+import numpy as np
+import pytest
+
+import nufftax_b200 as nb
+from nufftax_b200 import _lib
+from nufftax_b200.kernel import deconv_factors
+from oracle import nufft_oracle as O
+
+
+def test_library_exports_every_header_symbol():
+    lib = _lib.load()
+    names = _lib.header_symbols()
+    assert len(names) >= 20
+    for n in names:
+        assert hasattr(lib, n), n
+    assert lib.nfx_version() >= 10000
+
+
+def test_signatures_cover_header():
+    assert set(_lib.header_symbols()) == set(_lib._SIGNATURES)
+
+
+def _opts(dim=2, nf=(1024, 1024), ns=8, precision=0):
+    o = _lib.NfxOpts()
+    o.precision = precision
+    o.dim = dim
+    o.nf = _lib.int3(nf)
+    o.nspread = ns
+    o.beta = 18.6
+    o.kc = 4.0 / max(ns, 1) ** 2
+    return o
+
+
+def test_default_tiles_and_workspace():
+    lib = _lib.load()
+    o = _opts()
+    assert lib.nfx_default_tiles(byref(o)) == 0
+    assert list(o.tile)[:2] == [32, 32] and o.max_subproblem > 0
+    b = c_size_t(0)
+    assert lib.nfx_sort_workspace_bytes(byref(o), 4_000_000, byref(b)) == 0
+    assert 8 * 4_000_000 < b.value < 64 * 4_000_000
+    o3 = _opts(3, (256, 256, 256))
+    assert lib.nfx_default_tiles(byref(o3)) == 0
+    assert all(t > 0 for t in o3.tile)
+
+
+@pytest.mark.parametrize("ns,code", [(3, _lib.NFX_ERR_UNSUPPORTED), (18, _lib.NFX_ERR_UNSUPPORTED),
+                                     (0, _lib.NFX_ERR_UNSUPPORTED)])
+def test_invalid_nspread_rejected(ns, code):
+    lib = _lib.load()
+    o = _opts(ns=ns)
+    assert lib.nfx_default_tiles(byref(o)) == code
+    assert b"nspread" in lib.nfx_last_error()
+
+
+def test_invalid_arguments_rejected_without_gpu():
+    lib = _lib.load()
+    o = _opts()
+    o.dim = 4
+    assert lib.nfx_default_tiles(byref(o)) == _lib.NFX_ERR_INVALID
+    o = _opts()
+    # workspace too small is reported before any device work
+    assert lib.nfx_sort_points(byref(o), ctypes.c_void_p(8), ctypes.c_void_p(8), None, 10, ctypes.c_void_p(8), 4,
+                               None) == _lib.NFX_ERR_WORKSPACE
+    # missing coordinate pointer
+    assert lib.nfx_spread(byref(o), ctypes.c_void_p(8), None, None, 10, ctypes.c_void_p(8), 1, ctypes.c_void_p(8),
+                          ctypes.c_void_p(8), 1 << 30, None) == _lib.NFX_ERR_INVALID
+    # FFT with a bad sign / deconvolution with more modes than grid
+    assert lib.nfx_fft(0, 2, _lib.int3((8, 8)), 1, ctypes.c_void_p(8), 0, None) == _lib.NFX_ERR_INVALID
+    assert lib.nfx_deconv_pad(0, 1, _lib.int3((8,)), _lib.int3((9,)), ctypes.c_void_p(8), None, None,
+                              ctypes.c_void_p(8), ctypes.c_void_p(8), 1, None) == _lib.NFX_ERR_INVALID
+    with pytest.raises(ValueError):
+        _lib.check(_lib.NFX_ERR_INVALID, "probe")
+
+
+@pytest.mark.parametrize("eps", [1e-2, 1e-3, 1e-5, 1e-6, 1e-9, 1e-12, 1e-15])
+@pytest.mark.parametrize("uf", [2.0, 1.25])
+def test_kernel_params_match_oracle(eps, uf):
+    a = nb.compute_kernel_params(eps, uf)
+    b = O.compute_kernel_params(eps, uf)
+    assert tuple(a) == tuple(b)
+
+
+def test_grid_helpers_match_oracle():
+    for n in [1, 7, 64, 128, 384, 512, 1000, 8192]:
+        for uf in (2.0, 1.25):
+            assert nb.compute_grid_size(n, uf, 8) == O.compute_grid_size(n, uf, 8)
+    assert nb.compute_type3_grid_size(np.pi, 300.0, eps=1e-6) == 1250
+    x = np.linspace(-np.pi, np.pi, 11)
+    s = np.linspace(-300, 300, 7)
+    assert nb.compute_type3_grid_size(x, s) == 1250
+    assert nb.compute_type3_grid_sizes_2d(np.pi, np.pi, 300, 300) == (1250, 1250)
+    assert nb.compute_type3_grid_sizes_3d(1.0, 2.0, 3.0, 10, 20, 30) == tuple(
+        O.type3_grid_size(e, s, 1e-6) for e, s in ((1.0, 10), (2.0, 20), (3.0, 30)))
+
+
+@pytest.mark.parametrize("nf,n", [(256, 128), (1024, 512), (20, 7), (16, 16)])
+def test_deconv_factors_match_oracle(nf, n):
+    kp = nb.compute_kernel_params(1e-6)
+    ph = O.kernel_fourier_series(nf, kp.nspread, kp.beta, kp.c)
+    assert np.allclose(deconv_factors(nf, n, kp), O.deconv_factors_1d(ph, n), rtol=1e-14)
+
+
+def test_upsampfac_split():
+    from nufftax_b200.transforms import _split_upsampfac
+
+    assert _split_upsampfac(2.0) == (2.0, 2.0)
+    assert _split_upsampfac((2.0, 1.25)) == (2.0, 1.25)
+
+
+def test_product_does_not_import_oracle():
+    import pathlib
+
+    pkg = pathlib.Path(nb.__file__).parent
+    for f in pkg.rglob("*.py"):
+        assert "oracle" not in f.read_text().replace("oracle is", ""), f
