@@ -199,13 +199,19 @@ def run_gpu(args):
             outs.append((f1, c2))
         return outs
 
-    for _ in range(args.warmup):
-        step(devsets)
-    torch.cuda.synchronize()
-
-    # ---- timed region: device-resident inputs ---------------------------------
+    # The clock sampler (200 ms period) runs from the warm-up through the timed
+    # region; warm-up continues past W steps until it has lasted 1 s so that the
+    # samples reflect the clocks under this load.
     sampler = ClockSampler(local)
     sampler.start()
+    t_w = time.perf_counter()
+    n_w = 0
+    while n_w < args.warmup or time.perf_counter() - t_w < 1.0:
+        step(devsets)
+        torch.cuda.synchronize()
+        n_w += 1
+
+    # ---- timed region: device-resident inputs ---------------------------------
     stream = torch.cuda.current_stream(dev)
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
@@ -219,7 +225,6 @@ def run_gpu(args):
             step(devsets)
             ends[i].record(stream)
     torch.cuda.synchronize()
-    clocks = sampler.stop()
     step_ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
     total_ms = float(sum(step_ms))
     per_call = rec.summary()
@@ -276,6 +281,7 @@ def run_gpu(args):
         b.record(stream)
         torch.cuda.synchronize()
         e_ms += a.elapsed_time(b)
+    clocks = sampler.stop()
     if world > 1:
         t = torch.tensor([e_ms], device=dev)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
@@ -411,7 +417,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="nufftax_b200", choices=["nufftax_b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -5,7 +5,10 @@ Tolerances (written per test):
   * transforms: relative l2 <= 2 eps against the oracle's restatement of
     nufftax's pure-JAX path (complex64 for eps >= 1e-6, complex128 below), and
     the error against the FP64 direct sum on a subsample is asserted < 10 eps
-    (the bar nufftax's own tests use against an exact transform);
+    (the bar nufftax's own tests use against an exact transform) plus, for
+    complex64, 2 N 2^-24: the reference folds coordinates in float32, so a
+    point's grid position carries a relative rounding of 2^-24, i.e. a phase
+    error up to about N 2^-24 at the highest of N modes;
   * spread / interp components: relative l2 <= 2e-6 (complex64) or 1e-12
     (complex128) against the oracle's float64 accumulation.
 """
@@ -169,6 +172,11 @@ def test_adjoint_identity_gpu():
 # ---------------------------------------------------------------------------
 # Transforms
 # ---------------------------------------------------------------------------
+def direct_tol(eps, prec, n_modes):
+    """Bound against the exact sum: 10 eps, plus the float32 fold limit for complex64."""
+    return 10 * eps + (2 * max(n_modes) * 2.0**-24 if prec == "c64" else 0.0)
+
+
 def _sub_modes(rng, n_modes, K=256):
     ks = O.flat_mode_list(n_modes)
     if ks.shape[0] <= K:
@@ -197,7 +205,7 @@ def test_type1_parity(dim, n_modes, M, eps, prec, isign):
     assert rel_l2(f, ref) <= 2 * eps
     idx, ks = _sub_modes(rng, n_modes)
     direct = O.direct_type1(X, c, n_modes, isign=isign, flat_modes=ks)
-    assert rel_l2(f.ravel()[idx], direct) < 10 * eps
+    assert rel_l2(f.ravel()[idx], direct) < direct_tol(eps, prec, n_modes)
 
 
 @pytest.mark.parametrize("dim,n_modes,M", T12)
@@ -216,7 +224,7 @@ def test_type2_parity(dim, n_modes, M, eps, prec, isign):
     rows = rng.choice(M, min(M, 256), replace=False)
     vals, flat = O.modes_as_flat(f, dim)
     direct = O.direct_type2(X, vals, flat, isign=isign, rows=rows)
-    assert rel_l2(c[rows], direct) < 10 * eps
+    assert rel_l2(c[rows], direct) < direct_tol(eps, prec, n_modes)
 
 
 @pytest.mark.parametrize("name", ["t1_1d", "t1_2d", "t1_3d"])
