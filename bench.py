@@ -414,6 +414,25 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_case(args):
+    """One point set, `reps` rounds of sort + type 1 + type 2, no timing: for ncu captures."""
+    import torch
+
+    import nufftax_b200 as nb
+
+    dev = torch.device("cuda", 0)
+    sets = [s for s in workload(seed=1234, scale=args.scale) if s["name"] == args.case]
+    s = sets[0]
+    x, y = torch.from_numpy(s["x"]).to(dev), torch.from_numpy(s["y"]).to(dev)
+    c, f = torch.from_numpy(s["c"]).to(dev), torch.from_numpy(s["f"]).to(dev)
+    for _ in range(args.reps):
+        nb.sort_cache.clear()
+        nb.nufft2d1(x, y, c, N_MODES, eps=EPS)
+        nb.nufft2d2(x, y, f, eps=EPS)
+    torch.cuda.synchronize()
+    print(json.dumps({"case": args.case, "M": s["M"], "reps": args.reps}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -421,7 +440,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="nufftax_b200", choices=["nufftax_b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--case", choices=["radial", "clustered"], help="profile one point set only (no timing)")
+    ap.add_argument("--reps", type=int, default=2)
+    ap.add_argument("--scale", type=float, default=1.0)
     args = ap.parse_args()
+    if args.case:
+        run_case(args)
+        return
     if args.warmup < 3 and args.impl != "reference":
         args.warmup = 3
     if args.impl == "reference":
