@@ -94,6 +94,19 @@ int nfx_spread_sorted(const nfx_opts* opts, const void* x, const void* y, const 
 int nfx_interp_sorted(const nfx_opts* opts, const void* x, const void* y, const void* z, int64_t M, const void* fw,
                       int n_trans, void* c_out, const void* workspace, size_t workspace_bytes, void* stream);
 
+/* ---- spreading without any allocation ---------------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory or pass a workspace (code inside another framework's operator that
+ * only receives its operand and result buffers, or code under a fixed memory
+ * budget): same result as nfx_spread, with the sort scratch in a fixed array
+ * of nfx_noalloc_scratch_bytes() (64 MiB) that the library holds on every GPU
+ * that loads it.  Requests needing more scratch fail with NFX_ERR_UNSUPPORTED.
+ * The first call on a device looks up the array's address (make it before any
+ * stream capture); calls that overlap on the GPU race on the shared array. */
+size_t nfx_noalloc_scratch_bytes(void);
+int nfx_spread_noalloc(const nfx_opts* opts, const void* x, const void* y, const void* z, int64_t M, const void* c,
+                       int n_trans, void* fw, void* stream);
+
 /* ---- adjoints (ES-derivative coordinate gradients) ---------------------------
  * Replace the backward rules of the core custom_vjp's
  * (nufftax/core/spread.py:766-1305; torch convention G = dL/dRe + i dL/dIm):

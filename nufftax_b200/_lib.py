@@ -62,6 +62,8 @@ _SIGNATURES = {
     "nfx_sort_results": ([POINTER(NfxOpts), c_int64, _vp, c_size_t, _vp, _vp, _vp, POINTER(c_int), _vp], c_int),
     "nfx_spread": ([POINTER(NfxOpts), _vp, _vp, _vp, c_int64, _vp, c_int, _vp, _vp, c_size_t, _vp], c_int),
     "nfx_interp": ([POINTER(NfxOpts), _vp, _vp, _vp, c_int64, _vp, c_int, _vp, _vp, c_size_t, _vp], c_int),
+    "nfx_noalloc_scratch_bytes": ([], c_size_t),
+    "nfx_spread_noalloc": ([POINTER(NfxOpts), _vp, _vp, _vp, c_int64, _vp, c_int, _vp, _vp], c_int),
     "nfx_spread_sorted": ([POINTER(NfxOpts), _vp, _vp, _vp, c_int64, _vp, c_int, _vp, _vp, c_size_t, _vp], c_int),
     "nfx_interp_sorted": ([POINTER(NfxOpts), _vp, _vp, _vp, c_int64, _vp, c_int, _vp, _vp, c_size_t, _vp], c_int),
     "nfx_spread_grad_sorted": (
