@@ -433,6 +433,86 @@ def run_case(args):
     print(json.dumps({"case": args.case, "M": s["M"], "reps": args.reps}))
 
 
+def batched_workload(seed=77, P=64):
+    """64 problems: M log-uniform in [1e4, 2e6], modes per axis from {128, 256, 384, 512},
+    even problems uniform, odd problems clustered N(0, 0.3^2)."""
+    rng = np.random.default_rng(seed)
+    probs = []
+    for p in range(P):
+        M = int(np.exp(rng.uniform(np.log(1e4), np.log(2e6))))
+        if p % 2:
+            x, y = clustered_points(M, rng)
+        else:
+            x, y = rng.uniform(-np.pi, np.pi, (2, M)).astype(np.float32)
+        nm = (int(rng.choice([128, 256, 384, 512])), int(rng.choice([128, 256, 384, 512])))
+        c = (rng.standard_normal(M) + 1j * rng.standard_normal(M)).astype(np.complex64)
+        f = (rng.standard_normal((nm[1], nm[0])) + 1j * rng.standard_normal((nm[1], nm[0]))).astype(np.complex64)
+        probs.append({"x": x, "y": y, "c": c, "f": f, "M": M, "n_modes": nm})
+    return probs
+
+
+def run_batched(args):
+    """Batched plan (one persistent launch per pass, CUDA graph) vs the per-problem plain path."""
+    import torch
+
+    import nufftax_b200 as nb
+    from nufftax_b200.autotune import tune
+    from nufftax_b200.batch import BatchPlan
+
+    dev = torch.device("cuda", 0)
+    eps = 1e-5
+    probs = batched_workload()
+    d = [{k: (torch.from_numpy(v).to(dev) if isinstance(v, np.ndarray) else v) for k, v in q.items()} for q in probs]
+    pts = sum(2 * q["M"] for q in probs)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def plain_step():
+        nb.sort_cache.clear()
+        for q in d:
+            nb.nufft2d1(q["x"], q["y"], q["c"], q["n_modes"], eps=eps)
+            nb.nufft2d2(q["x"], q["y"], q["f"], eps=eps)
+
+    def timed(fn, steps, warm):
+        for _ in range(warm):
+            fn()
+        torch.cuda.synchronize()
+        tot = 0.0
+        for i in range(steps):
+            flush.fill_(float(i))
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            torch.cuda.synchronize()
+            tot += a.elapsed_time(b)
+        return tot / steps
+
+    plain_ms = timed(plain_step, args.steps, args.warmup)
+    kp = nb.compute_kernel_params(eps)
+    tiles, maxsubs = [], []
+    if args.autotune:
+        for q in d:
+            nf = tuple(nb.compute_grid_size(n, 2.0, kp.nspread) for n in q["n_modes"])
+            t, m = tune([q["x"], q["y"]], nf, kp)
+            tiles.append(t)
+            maxsubs.append(m)
+    plan = BatchPlan([[q["x"], q["y"]] for q in d], [q["n_modes"] for q in d], eps=eps,
+                     tiles=tiles or None, max_subproblem=maxsubs or None, graph=True)
+    for p, q in enumerate(d):
+        plan.c_in[p].copy_(q["c"])
+        plan.f_in[p].copy_(q["f"])
+    batch_ms = timed(lambda: plan.run(), args.steps, args.warmup)
+    line = {"metric": "batched 2D type-1 + type-2 NU points/s (64 problems, eps 1e-5, complex64)",
+            "value": pts / (batch_ms / 1e3), "unit": "NU points/s", "plain_value": pts / (plain_ms / 1e3),
+            "speedup_vs_plain": plain_ms / batch_ms, "ms_per_step": batch_ms, "plain_ms_per_step": plain_ms,
+            "points_per_step": pts, "steps": args.steps, "warmup": args.warmup, "autotune": bool(args.autotune),
+            "config": {"workload": "64 problems, M log-uniform [1e4, 2e6], modes per axis from {128,256,384,512}, "
+                                   "half uniform / half clustered N(0,0.3^2), sort included every step",
+                       "l2": "flushed between steps"}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -443,7 +523,12 @@ def main():
     ap.add_argument("--case", choices=["radial", "clustered"], help="profile one point set only (no timing)")
     ap.add_argument("--reps", type=int, default=2)
     ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--config", choices=["default", "batched"], default="default")
+    ap.add_argument("--autotune", action="store_true")
     args = ap.parse_args()
+    if args.config == "batched":
+        run_batched(args)
+        return
     if args.case:
         run_case(args)
         return

@@ -146,6 +146,52 @@ int nfx_deconv_pad(int precision, int dim, const int nf[3], const int n_modes[3]
 int nfx_fft(int precision, int dim, const int nf[3], int n_trans, void* data, int sign, void* stream);
 int nfx_fft_cache_clear(void);
 
+/* ---- batching: many problems in one launch --------------------------------
+ * No counterpart in the reference (nufftax vmaps one problem's strengths).
+ * Each problem has its own points, fine grid, tiling and sort workspace; the
+ * kernel (nspread, beta, kc), precision, dim and prenorm come from `common`.
+ * nfx_batch_sort sorts every problem; nfx_batch_upload writes a device table
+ * for one direction (spread: src = strengths, dst = fine grid, which the caller
+ * zeroes; interp: src = fine grid, dst = values); nfx_batch_launch runs ONE
+ * persistent launch over the (problem, bin tile) work queue of all problems.
+ * The table stays valid while the problems' buffers do, so the launches can be
+ * captured in a CUDA graph and replayed.  nfx_batch_deconv_* do the same for
+ * the deconvolution passes (pad = 0: shuffle/crop after a type-1 FFT; pad = 1:
+ * zero-pad before a type-2 FFT); nf / n_modes are 3 ints per problem and fac 3
+ * pointers per problem. */
+typedef struct nfx_batch_problem {
+  int64_t M;
+  const void* x;
+  const void* y;
+  const void* z;
+  int nf[3];
+  int tile[3];         /* 0 = default */
+  int max_subproblem;  /* 0 = default */
+  void* workspace;     /* sort workspace of nfx_sort_workspace_bytes for this problem */
+  size_t workspace_bytes;
+  const void* src;
+  void* dst;
+} nfx_batch_problem;
+
+typedef struct nfx_batch_info {
+  size_t table_bytes;  /* device table size for nfx_batch_upload */
+  size_t smem_bytes;   /* shared memory of the batched launch */
+  int64_t max_subs;    /* bound on the work-queue length */
+} nfx_batch_info;
+
+int nfx_batch_info_get(const nfx_opts* common, int spread, const nfx_batch_problem* probs, int nprob,
+                       nfx_batch_info* info);
+int nfx_batch_upload(const nfx_opts* common, int spread, const nfx_batch_problem* probs, int nprob, void* dev_table,
+                     size_t table_bytes, void* stream);
+int nfx_batch_sort(const nfx_opts* common, const nfx_batch_problem* probs, int nprob, void* stream);
+int nfx_batch_launch(const nfx_opts* common, int spread, const void* dev_table, int nprob, const nfx_batch_info* info,
+                     void* stream);
+size_t nfx_batch_deconv_table_bytes(int precision, int nprob);
+int nfx_batch_deconv_upload(int precision, int dim, int pad, const int* nf, const int* n_modes,
+                            const void* const* fac, const void* const* src, void* const* dst, int nprob,
+                            void* dev_table, size_t table_bytes, int64_t* total, void* stream);
+int nfx_batch_deconv(int precision, int pad, const void* dev_table, int nprob, int64_t total, void* stream);
+
 /* ---- type 3 helpers (nufftax/transforms/nufft3.py:216-515) -------------------
  * nfx_t3_prepare: from source coordinates (dim arrays of M) and target
  *   frequencies (dim arrays of K) computes, on the device and without a host

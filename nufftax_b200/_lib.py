@@ -51,6 +51,30 @@ class NfxOpts(ctypes.Structure):
     ]
 
 
+class NfxBatchProblem(ctypes.Structure):
+    """Mirror of `nfx_batch_problem` in include/nfx.h."""
+
+    _fields_ = [
+        ("M", c_int64),
+        ("x", c_void_p),
+        ("y", c_void_p),
+        ("z", c_void_p),
+        ("nf", c_int * 3),
+        ("tile", c_int * 3),
+        ("max_subproblem", c_int),
+        ("workspace", c_void_p),
+        ("workspace_bytes", c_size_t),
+        ("src", c_void_p),
+        ("dst", c_void_p),
+    ]
+
+
+class NfxBatchInfo(ctypes.Structure):
+    """Mirror of `nfx_batch_info` in include/nfx.h."""
+
+    _fields_ = [("table_bytes", c_size_t), ("smem_bytes", c_size_t), ("max_subs", c_int64)]
+
+
 _vp = c_void_p
 _SIGNATURES = {
     "nfx_version": ([], c_int),
@@ -75,6 +99,15 @@ _SIGNATURES = {
     "nfx_deconv_pad": ([c_int, c_int, POINTER(c_int), POINTER(c_int), _vp, _vp, _vp, _vp, _vp, c_int, _vp], c_int),
     "nfx_fft": ([c_int, c_int, POINTER(c_int), c_int, _vp, c_int, _vp], c_int),
     "nfx_fft_cache_clear": ([], c_int),
+    "nfx_batch_info_get": ([POINTER(NfxOpts), c_int, POINTER(NfxBatchProblem), c_int, POINTER(NfxBatchInfo)], c_int),
+    "nfx_batch_upload": ([POINTER(NfxOpts), c_int, POINTER(NfxBatchProblem), c_int, _vp, c_size_t, _vp], c_int),
+    "nfx_batch_sort": ([POINTER(NfxOpts), POINTER(NfxBatchProblem), c_int, _vp], c_int),
+    "nfx_batch_launch": ([POINTER(NfxOpts), c_int, _vp, c_int, POINTER(NfxBatchInfo), _vp], c_int),
+    "nfx_batch_deconv_table_bytes": ([c_int, c_int], c_size_t),
+    "nfx_batch_deconv_upload": ([c_int, c_int, c_int, POINTER(c_int), POINTER(c_int), POINTER(c_void_p),
+                                 POINTER(c_void_p), POINTER(c_void_p), c_int, _vp, c_size_t, POINTER(c_int64), _vp],
+                                c_int),
+    "nfx_batch_deconv": ([c_int, c_int, _vp, c_int, c_int64, _vp], c_int),
     "nfx_t3_params_bytes": ([], c_size_t),
     "nfx_t3_scratch_bytes": ([c_int, c_int64, c_int64], c_size_t),
     "nfx_t3_prepare": ([c_int, c_int, POINTER(c_int), c_int, c_double, c_double, c_double, c_int, POINTER(c_void_p),

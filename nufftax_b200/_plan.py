@@ -95,7 +95,7 @@ class PointSort:
         _lib.check(lib.nfx_sort_workspace_bytes(byref(self.opts), self.M, byref(nbytes)), "nfx_sort_workspace_bytes")
         self.ws_bytes = int(nbytes.value)
         self.ws = torch.empty(max(self.ws_bytes, 1), dtype=torch.uint8, device=self.device)
-        with torch.cuda.device(self.device), span("nfx_sort_points", self.device, 6 if self.M > 0 else 0):
+        with torch.cuda.device(self.device), span("nfx_sort_points", self.device, 11 if self.M > 0 else 0):
             _lib.check(lib.nfx_sort_points(byref(self.opts), *self._xyz(), self.M, ptr(self.ws), self.ws_bytes,
                                            c_void_p(stream_of(self.device))), "nfx_sort_points")
 

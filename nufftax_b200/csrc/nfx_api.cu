@@ -5,6 +5,7 @@
 #include <mutex>
 #include <string>
 #include <tuple>
+#include <vector>
 
 #include "nfx.h"
 #include "nfx_spreadinterp.cuh"
@@ -20,11 +21,17 @@ template <typename T, int DIM>
 cudaError_t dispatch_grad(int ns, const PointArgs<T>& a, const void* G, const void* V, void* oi, void* dx, void* dy,
                           void* dz, cudaStream_t st);
 
+template <typename T, int DIM>
+cudaError_t dispatch_batch(int ns, bool spread, const void* items, int n, const int* prefix, int64_t max_subs,
+                           size_t smem, cudaStream_t st);
+
 #define NFX_EXTERN(T, D)                                                                                           \
   extern template cudaError_t dispatch_spread<T, D>(int, const PointArgs<T>&, const void*, void*, cudaStream_t);   \
   extern template cudaError_t dispatch_interp<T, D>(int, const PointArgs<T>&, const void*, void*, cudaStream_t);   \
   extern template cudaError_t dispatch_grad<T, D>(int, const PointArgs<T>&, const void*, const void*, void*, void*, \
-                                                  void*, void*, cudaStream_t);
+                                                  void*, void*, cudaStream_t);                                     \
+  extern template cudaError_t dispatch_batch<T, D>(int, bool, const void*, int, const int*, int64_t, size_t,       \
+                                                   cudaStream_t);
 NFX_EXTERN(float, 1)
 NFX_EXTERN(float, 2)
 NFX_EXTERN(float, 3)
@@ -203,7 +210,8 @@ static int resolve_opts(const nfx_opts* in, nfx_opts& o) {
     for (int it = 0; it < 64; ++it) {
       Geom g;
       fill_geom(&o, g);
-      const bool smem_ok = spread_smem_bytes(rb, o.dim, ns, g) <= kSmemBudget && tile_smem_bytes(rb, g) <= kSmemBudget;
+      const bool smem_ok = spread_smem_bytes(rb, o.dim, ns, g) <= kSmemBudget &&
+                           interp_smem_bytes(rb, o.dim, ns, g) <= kSmemBudget;
       if (!smem_ok) {
         int dmax = 0;
         for (int d = 1; d < o.dim; ++d)
@@ -220,7 +228,8 @@ static int resolve_opts(const nfx_opts* in, nfx_opts& o) {
       trial.tile[dmax] = std::min(o.tile[dmax] * 2, o.nf[dmax]);
       Geom gt;
       fill_geom(&trial, gt);
-      if (spread_smem_bytes(rb, o.dim, ns, gt) > kSmemBudget || tile_smem_bytes(rb, gt) > kSmemBudget) break;
+      if (spread_smem_bytes(rb, o.dim, ns, gt) > kSmemBudget || interp_smem_bytes(rb, o.dim, ns, gt) > kSmemBudget)
+        break;
       o = trial;
     }
   }
@@ -231,7 +240,11 @@ static int resolve_opts(const nfx_opts* in, nfx_opts& o) {
     set_error("too many bins for the sort (raise tile)");
     return NFX_ERR_UNSUPPORTED;
   }
-  if (spread_smem_bytes(rb, o.dim, ns, g) > kSmemBudget || tile_smem_bytes(rb, g) > kSmemBudget) {
+  if (g.tile[0] * g.tile[1] * g.tile[2] > kMaxBins) {
+    set_error("too many cells per tile for the sort (lower tile)");
+    return NFX_ERR_UNSUPPORTED;
+  }
+  if (spread_smem_bytes(rb, o.dim, ns, g) > kSmemBudget || interp_smem_bytes(rb, o.dim, ns, g) > kSmemBudget) {
     set_error("tile too large for shared memory (lower tile)");
     return NFX_ERR_UNSUPPORTED;
   }
@@ -243,34 +256,39 @@ static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
 static void make_layout(const nfx_opts& o, const Geom& g, int64_t M, SortLayout& L) {
   L.M = M;
   L.nbins = g.nbins;
+  L.ncell = g.tile[0] * g.tile[1] * g.tile[2];
+  const int64_t nk = std::max<int64_t>(g.nbins, L.ncell);
   const int64_t target = std::max<int64_t>((int64_t)1 << 20, M / 4);
   int64_t chunk = 1024;
-  while ((int64_t)g.nbins * ((M + chunk - 1) / chunk) > target && chunk < ((int64_t)1 << 30)) chunk *= 2;
+  while (nk * ((M + chunk - 1) / chunk) > target && chunk < ((int64_t)1 << 30)) chunk *= 2;
   L.chunk = (int)chunk;
   L.nchunks = (int)std::max<int64_t>(1, (M + chunk - 1) / chunk);
-  L.sort_warps = (int)std::max<int64_t>(1, std::min<int64_t>(8, (96 * 1024) / ((int64_t)g.nbins * 4)));
+  // warps of the scatter passes: each needs a key-histogram row in shared memory
+  L.sort_warps = (int)std::max<int64_t>(1, std::min<int64_t>(8, (int64_t)kSmemBudget / ((int64_t)g.nbins * 4)));
   L.sort_smem = (size_t)L.sort_warps * g.nbins * sizeof(int);
-  L.n_counts = (int64_t)g.nbins * L.nchunks;
+  L.sort_warps_cell = (int)std::max<int64_t>(1, std::min<int64_t>(8, (int64_t)kSmemBudget / ((int64_t)L.ncell * 4)));
+  L.sort_smem_cell = (size_t)L.sort_warps_cell * L.ncell * sizeof(int);
+  L.n_counts = nk * L.nchunks;
   L.scan_blocks = scan_blocks(L.n_counts);
   L.maxsub = o.max_subproblem;
   L.max_subs = g.nbins + (M + L.maxsub - 1) / L.maxsub;
   size_t off = 0;
-  L.off_keys = off;
-  off += align256((size_t)M * 4);
-  L.off_perm = off;
-  off += align256((size_t)M * 4);
-  L.off_counts = off;
-  off += align256((size_t)L.n_counts * 4);
-  L.off_scan = off;
-  off += align256((size_t)L.scan_blocks * 4 + 4);
-  L.off_bin_start = off;
-  off += align256((size_t)(g.nbins + 1) * 4);
-  L.off_sub_bin = off;
-  off += align256((size_t)L.max_subs * 4);
-  L.off_sub_start = off;
-  off += align256((size_t)L.max_subs * 4);
-  L.off_nsub = off;
-  off += 256;
+  auto take = [&](size_t bytes) {
+    size_t at = off;
+    off += align256(bytes);
+    return at;
+  };
+  L.off_keys = take((size_t)M * 4);
+  L.off_keys_cell = take((size_t)M * 4);
+  L.off_keys_by_cell = take((size_t)M * 4);
+  L.off_perm_cell = take((size_t)M * 4);
+  L.off_perm = take((size_t)M * 4);
+  L.off_counts = take((size_t)L.n_counts * 4);
+  L.off_scan = take((size_t)L.scan_blocks * 4 + 4);
+  L.off_bin_start = take((size_t)(g.nbins + 1) * 4);
+  L.off_sub_bin = take((size_t)L.max_subs * 4);
+  L.off_sub_start = take((size_t)L.max_subs * 4);
+  L.off_nsub = take(4);
   L.total = off;
 }
 
@@ -278,6 +296,9 @@ static SortPtrs carve(const SortLayout& L, void* ws) {
   char* b = (char*)ws;
   SortPtrs P;
   P.keys = (int*)(b + L.off_keys);
+  P.keys_cell = (int*)(b + L.off_keys_cell);
+  P.keys_by_cell = (int*)(b + L.off_keys_by_cell);
+  P.perm_cell = (int*)(b + L.off_perm_cell);
   P.perm = (int*)(b + L.off_perm);
   P.counts = (int*)(b + L.off_counts);
   P.scan_tmp = (int*)(b + L.off_scan);
@@ -381,6 +402,35 @@ static cudaError_t grad_dim(const Prepared& P, const void* x, const void* y, con
 }
 
 static int64_t grid_cells(const Geom& g) { return (int64_t)g.nf[0] * g.nf[1] * g.nf[2]; }
+
+template <typename T>
+__global__ void k_batch_prefix(const BatchItem<T>* __restrict__ items, int n, int* __restrict__ prefix) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  int run = 0;
+  for (int p = 0; p < n; ++p) {
+    prefix[p] = run;
+    run += *items[p].a.s.nsub;
+  }
+  prefix[n] = run;
+}
+
+// Per-problem options from the shared ones (kernel, precision, dim) and the
+// problem's own grid / tiling.
+static int batch_problem_opts(const nfx_opts* common, const nfx_batch_problem& pb, Prepared& P) {
+  nfx_opts o = *common;
+  for (int d = 0; d < 3; ++d) {
+    o.nf[d] = pb.nf[d];
+    o.tile[d] = pb.tile[d];
+  }
+  o.max_subproblem = pb.max_subproblem;
+  return prepare(&o, pb.M, pb.x, pb.y, pb.z, pb.workspace, pb.workspace_bytes, P);
+}
+
+static size_t batch_item_bytes(int precision) {
+  return precision == NFX_F32 ? sizeof(BatchItem<float>) : sizeof(BatchItem<double>);
+}
+
+static size_t batch_prefix_offset(int precision, int n) { return align256(batch_item_bytes(precision) * n); }
 
 }  // namespace nfx
 
@@ -578,6 +628,178 @@ int nfx_deconv_pad(int precision, int dim, const int nf[3], const int n_modes[3]
                       : launch_deconv_pad<double>(dim, nff, nmf, (const double*)fac1, (const double*)fac2,
                                                   (const double*)fac3, f_in, fw_hat, n_trans, s);
   return e == cudaSuccess ? NFX_OK : cuda_fail(e, "nfx_deconv_pad");
+}
+
+
+// ---- batched spread / interp / deconvolution --------------------------------
+
+int nfx_batch_info_get(const nfx_opts* common, int spread, const nfx_batch_problem* probs, int nprob,
+                       nfx_batch_info* info) {
+  if (common == nullptr || probs == nullptr || nprob < 1 || info == nullptr) {
+    set_error("nfx_batch_info_get: invalid arguments");
+    return NFX_ERR_INVALID;
+  }
+  size_t smem = 0;
+  int64_t subs = 0;
+  for (int p = 0; p < nprob; ++p) {
+    Prepared P;
+    nfx_opts o = *common;
+    for (int d = 0; d < 3; ++d) {
+      o.nf[d] = probs[p].nf[d];
+      o.tile[d] = probs[p].tile[d];
+    }
+    o.max_subproblem = probs[p].max_subproblem;
+    int st = resolve_opts(&o, P.o);
+    if (st != NFX_OK) return st;
+    fill_geom(&P.o, P.g);
+    make_layout(P.o, P.g, probs[p].M, P.L);
+    const size_t rb = real_bytes(P.o.precision);
+    const size_t sm = spread ? spread_smem_bytes(rb, P.o.dim, P.o.nspread, P.g) : tile_smem_bytes(rb, P.g);
+    smem = sm > smem ? sm : smem;
+    subs += P.L.max_subs;
+  }
+  info->table_bytes = batch_prefix_offset(common->precision, nprob) + align256((size_t)(nprob + 1) * 4);
+  info->smem_bytes = smem;
+  info->max_subs = subs;
+  return NFX_OK;
+}
+
+int nfx_batch_upload(const nfx_opts* common, int spread, const nfx_batch_problem* probs, int nprob, void* dev_table,
+                     size_t table_bytes, void* stream) {
+  nfx_batch_info info;
+  int st = nfx_batch_info_get(common, spread, probs, nprob, &info);
+  if (st != NFX_OK) return st;
+  if (dev_table == nullptr || table_bytes < info.table_bytes) {
+    set_error("nfx_batch_upload: table too small");
+    return NFX_ERR_WORKSPACE;
+  }
+  std::vector<unsigned char> host(batch_item_bytes(common->precision) * nprob);
+  for (int p = 0; p < nprob; ++p) {
+    Prepared P;
+    st = batch_problem_opts(common, probs[p], P);
+    if (st != NFX_OK) return st;
+    if (probs[p].src == nullptr || probs[p].dst == nullptr) {
+      set_error("nfx_batch_upload: NULL src / dst");
+      return NFX_ERR_INVALID;
+    }
+    if (common->precision == NFX_F32) {
+      BatchItem<float>* it = (BatchItem<float>*)host.data() + p;
+      it->a = make_args<float>(P.g, P.o.beta, P.o.kc, probs[p].x, probs[p].y, probs[p].z, probs[p].M, 1,
+                               view(P.L, probs[p].workspace));
+      it->src = probs[p].src;
+      it->dst = probs[p].dst;
+    } else {
+      BatchItem<double>* it = (BatchItem<double>*)host.data() + p;
+      it->a = make_args<double>(P.g, P.o.beta, P.o.kc, probs[p].x, probs[p].y, probs[p].z, probs[p].M, 1,
+                                view(P.L, probs[p].workspace));
+      it->src = probs[p].src;
+      it->dst = probs[p].dst;
+    }
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e = cudaMemcpyAsync(dev_table, host.data(), host.size(), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  return e == cudaSuccess ? NFX_OK : cuda_fail(e, "nfx_batch_upload");
+}
+
+int nfx_batch_sort(const nfx_opts* common, const nfx_batch_problem* probs, int nprob, void* stream) {
+  if (common == nullptr || probs == nullptr || nprob < 1) {
+    set_error("nfx_batch_sort: invalid arguments");
+    return NFX_ERR_INVALID;
+  }
+  for (int p = 0; p < nprob; ++p) {
+    nfx_opts o = *common;
+    for (int d = 0; d < 3; ++d) {
+      o.nf[d] = probs[p].nf[d];
+      o.tile[d] = probs[p].tile[d];
+    }
+    o.max_subproblem = probs[p].max_subproblem;
+    int st = nfx_sort_points(&o, probs[p].x, probs[p].y, probs[p].z, probs[p].M, probs[p].workspace,
+                             probs[p].workspace_bytes, stream);
+    if (st != NFX_OK) return st;
+  }
+  return NFX_OK;
+}
+
+int nfx_batch_launch(const nfx_opts* common, int spread, const void* dev_table, int nprob, const nfx_batch_info* info,
+                     void* stream) {
+  if (common == nullptr || dev_table == nullptr || nprob < 1 || info == nullptr) {
+    set_error("nfx_batch_launch: invalid arguments");
+    return NFX_ERR_INVALID;
+  }
+  nfx_opts o;
+  nfx_opts probe = *common;
+  probe.nf[0] = probe.nf[1] = probe.nf[2] = 64;
+  probe.tile[0] = probe.tile[1] = probe.tile[2] = 0;
+  int st = resolve_opts(&probe, o);
+  if (st != NFX_OK) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  int* prefix = (int*)((char*)dev_table + batch_prefix_offset(common->precision, nprob));
+  cudaError_t e;
+  if (common->precision == NFX_F32)
+    k_batch_prefix<float><<<1, 32, 0, s>>>((const BatchItem<float>*)dev_table, nprob, prefix);
+  else
+    k_batch_prefix<double><<<1, 32, 0, s>>>((const BatchItem<double>*)dev_table, nprob, prefix);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "nfx_batch_launch prefix");
+  const bool sp = spread != 0;
+  const int ns = common->nspread;
+  if (common->precision == NFX_F32) {
+    e = common->dim == 1   ? dispatch_batch<float, 1>(ns, sp, dev_table, nprob, prefix, info->max_subs, info->smem_bytes, s)
+        : common->dim == 2 ? dispatch_batch<float, 2>(ns, sp, dev_table, nprob, prefix, info->max_subs, info->smem_bytes, s)
+                           : dispatch_batch<float, 3>(ns, sp, dev_table, nprob, prefix, info->max_subs, info->smem_bytes, s);
+  } else {
+    e = common->dim == 1   ? dispatch_batch<double, 1>(ns, sp, dev_table, nprob, prefix, info->max_subs, info->smem_bytes, s)
+        : common->dim == 2 ? dispatch_batch<double, 2>(ns, sp, dev_table, nprob, prefix, info->max_subs, info->smem_bytes, s)
+                           : dispatch_batch<double, 3>(ns, sp, dev_table, nprob, prefix, info->max_subs, info->smem_bytes, s);
+  }
+  return e == cudaSuccess ? NFX_OK : cuda_fail(e, "nfx_batch_launch");
+}
+
+size_t nfx_batch_deconv_table_bytes(int precision, int nprob) {
+  return align256(deconv_item_bytes(precision == NFX_F64 ? 1 : 0) * (size_t)(nprob > 0 ? nprob : 1));
+}
+
+int nfx_batch_deconv_upload(int precision, int dim, int pad, const int* nf, const int* n_modes,
+                            const void* const* fac, const void* const* src, void* const* dst, int nprob,
+                            void* dev_table, size_t table_bytes, int64_t* total, void* stream) {
+  if ((precision != NFX_F32 && precision != NFX_F64) || dim < 1 || dim > 3 || nf == nullptr || n_modes == nullptr ||
+      fac == nullptr || src == nullptr || dst == nullptr || nprob < 1 || dev_table == nullptr || total == nullptr) {
+    set_error("nfx_batch_deconv_upload: invalid arguments");
+    return NFX_ERR_INVALID;
+  }
+  if (table_bytes < nfx_batch_deconv_table_bytes(precision, nprob)) {
+    set_error("nfx_batch_deconv_upload: table too small");
+    return NFX_ERR_WORKSPACE;
+  }
+  for (int p = 0; p < nprob; ++p) {
+    int a[3], b[3];
+    int st = check_deconv(precision, dim, nf + 3 * p, n_modes + 3 * p, fac[3 * p], fac[3 * p + 1], fac[3 * p + 2], 1,
+                          a, b);
+    if (st != NFX_OK) return st;
+    if (src[p] == nullptr || dst[p] == nullptr) {
+      set_error("nfx_batch_deconv_upload: NULL src / dst");
+      return NFX_ERR_INVALID;
+    }
+  }
+  std::vector<unsigned char> host(deconv_item_bytes(precision == NFX_F64 ? 1 : 0) * nprob);
+  *total = fill_deconv_items(precision == NFX_F64 ? 1 : 0, dim, pad != 0, nf, n_modes, fac, src, dst, nprob,
+                             host.data());
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e = cudaMemcpyAsync(dev_table, host.data(), host.size(), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  return e == cudaSuccess ? NFX_OK : cuda_fail(e, "nfx_batch_deconv_upload");
+}
+
+int nfx_batch_deconv(int precision, int pad, const void* dev_table, int nprob, int64_t total, void* stream) {
+  if ((precision != NFX_F32 && precision != NFX_F64) || dev_table == nullptr || nprob < 1 || total < 0) {
+    set_error("nfx_batch_deconv: invalid arguments");
+    return NFX_ERR_INVALID;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e = precision == NFX_F32 ? launch_deconv_batch<float>(pad != 0, dev_table, nprob, total, s)
+                                       : launch_deconv_batch<double>(pad != 0, dev_table, nprob, total, s);
+  return e == cudaSuccess ? NFX_OK : cuda_fail(e, "nfx_batch_deconv");
 }
 
 }  // extern "C"

@@ -8,6 +8,8 @@
 // Type 2 (deconvolve.py:114-166, 227-304, 369-468): one pass writes every
 //   cell of the fine grid: the deconvolved mode where the cell is a kept mode,
 //   zero elsewhere (no separate memset of the grid).
+#include <type_traits>
+
 #include "nfx_internal.h"
 
 namespace nfx {
@@ -80,6 +82,87 @@ __global__ void k_deconv_pad(int nf1, int nf2, int nf3, int n1, int n2, int n3, 
   }
 }
 
+// Batched forms: one launch over many problems of different grids.  `items`
+// is a device table sorted by `start` (first global element of each problem).
+template <typename T>
+struct DeconvItem {
+  int nf[3];
+  int nm[3];
+  const T* fac[3];
+  const void* src;
+  void* dst;
+  int64_t start;
+};
+
+template <typename T>
+__device__ __forceinline__ int deconv_find(const DeconvItem<T>* __restrict__ items, int n, int64_t i) {
+  int lo = 0, hi = n;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (items[mid].start <= i)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+template <typename T>
+__global__ void k_deconv_shuffle_batch(const DeconvItem<T>* __restrict__ items, int n, int64_t total) {
+  using CT = cplx_t<T>;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const DeconvItem<T>& it = items[deconv_find(items, n, i)];
+    int64_t r = i - it.start;
+    const int n1 = it.nm[0], n2 = it.nm[1];
+    const int p1 = (int)(r % n1);
+    r /= n1;
+    const int p2 = (int)(r % n2);
+    const int p3 = (int)(r / n2);
+    int i1 = p1 - n1 / 2, i2 = p2 - n2 / 2, i3 = p3 - it.nm[2] / 2;
+    if (i1 < 0) i1 += it.nf[0];
+    if (i2 < 0) i2 += it.nf[1];
+    if (i3 < 0) i3 += it.nf[2];
+    const CT v = ((const CT*)it.src)[((int64_t)i3 * it.nf[1] + i2) * it.nf[0] + i1];
+    T fac = it.fac[0][p1];
+    if (it.fac[1] != nullptr) fac = (it.fac[2] != nullptr ? it.fac[2][p3] * it.fac[1][p2] : it.fac[1][p2]) * it.fac[0][p1];
+    CT o;
+    o.x = v.x * fac;
+    o.y = v.y * fac;
+    ((CT*)it.dst)[i - it.start] = o;
+  }
+}
+
+template <typename T>
+__global__ void k_deconv_pad_batch(const DeconvItem<T>* __restrict__ items, int n, int64_t total) {
+  using CT = cplx_t<T>;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const DeconvItem<T>& it = items[deconv_find(items, n, i)];
+    int64_t r = i - it.start;
+    const int nf1 = it.nf[0], nf2 = it.nf[1], nf3 = it.nf[2];
+    const int c1 = (int)(r % nf1);
+    r /= nf1;
+    const int c2 = (int)(r % nf2);
+    const int c3 = (int)(r / nf2);
+    const int n1 = it.nm[0], n2 = it.nm[1], n3 = it.nm[2];
+    const int k1 = c1 <= (n1 - 1) / 2 ? c1 : (c1 >= nf1 - n1 / 2 ? c1 - nf1 : INT32_MIN);
+    const int k2 = c2 <= (n2 - 1) / 2 ? c2 : (c2 >= nf2 - n2 / 2 ? c2 - nf2 : INT32_MIN);
+    const int k3 = c3 <= (n3 - 1) / 2 ? c3 : (c3 >= nf3 - n3 / 2 ? c3 - nf3 : INT32_MIN);
+    CT o;
+    o.x = (T)0;
+    o.y = (T)0;
+    if (k1 != INT32_MIN && k2 != INT32_MIN && k3 != INT32_MIN) {
+      const int p1 = k1 + n1 / 2, p2 = k2 + n2 / 2, p3 = k3 + n3 / 2;
+      const CT v = ((const CT*)it.src)[((int64_t)p3 * n2 + p2) * n1 + p1];
+      T fac = it.fac[0][p1];
+      if (it.fac[1] != nullptr)
+        fac = (it.fac[2] != nullptr ? it.fac[2][p3] * it.fac[1][p2] : it.fac[1][p2]) * it.fac[0][p1];
+      o.x = v.x * fac;
+      o.y = v.y * fac;
+    }
+    ((CT*)it.dst)[i - it.start] = o;
+  }
+}
+
 static unsigned elementwise_grid(int64_t n) {
   int64_t want = (n + 255) / 256;
   int64_t cap = (int64_t)num_sms() * 16;
@@ -108,6 +191,48 @@ cudaError_t launch_deconv_pad(int dim, const int nf[3], const int nm[3], const T
   return cudaGetLastError();
 }
 
+template <typename T>
+cudaError_t launch_deconv_batch(bool pad, const void* items, int n, int64_t total, cudaStream_t st) {
+  if (total <= 0) return cudaSuccess;
+  if (pad)
+    k_deconv_pad_batch<T><<<elementwise_grid(total), 256, 0, st>>>((const DeconvItem<T>*)items, n, total);
+  else
+    k_deconv_shuffle_batch<T><<<elementwise_grid(total), 256, 0, st>>>((const DeconvItem<T>*)items, n, total);
+  return cudaGetLastError();
+}
+
+size_t deconv_item_bytes(int precision) {
+  return precision == 0 ? sizeof(DeconvItem<float>) : sizeof(DeconvItem<double>);
+}
+
+int64_t fill_deconv_items(int precision, int dim, bool pad, const int* nf, const int* nm, const void* const* fac,
+                          const void* const* src, void* const* dst, int n, void* host_items) {
+  int64_t start = 0;
+  for (int p = 0; p < n; ++p) {
+    const int* f = nf + 3 * p;
+    const int* m = nm + 3 * p;
+    auto fill = [&](auto* it) {
+      using R = std::remove_pointer_t<decltype(it->fac[0])>;
+      for (int d = 0; d < 3; ++d) {
+        it->nf[d] = d < dim ? f[d] : 1;
+        it->nm[d] = d < dim ? m[d] : 1;
+        it->fac[d] = d < dim ? (R)fac[3 * p + d] : nullptr;
+      }
+      it->src = src[p];
+      it->dst = dst[p];
+      it->start = start;
+      start += pad ? (int64_t)it->nf[0] * it->nf[1] * it->nf[2] : (int64_t)it->nm[0] * it->nm[1] * it->nm[2];
+    };
+    if (precision == 0)
+      fill((DeconvItem<float>*)host_items + p);
+    else
+      fill((DeconvItem<double>*)host_items + p);
+  }
+  return start;
+}
+
+template cudaError_t launch_deconv_batch<float>(bool, const void*, int, int64_t, cudaStream_t);
+template cudaError_t launch_deconv_batch<double>(bool, const void*, int, int64_t, cudaStream_t);
 template cudaError_t launch_deconv_shuffle<float>(int, const int*, const int*, const float*, const float*,
                                                   const float*, const void*, void*, int, cudaStream_t);
 template cudaError_t launch_deconv_shuffle<double>(int, const int*, const int*, const double*, const double*,

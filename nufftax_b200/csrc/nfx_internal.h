@@ -16,21 +16,28 @@ namespace nfx {
 struct SortLayout {
   int64_t M;
   int nbins;
-  int chunk;        // points per warp in the counting passes
+  int ncell;        // cells per tile (keys of the first sort pass)
+  int chunk;        // points per CTA in the counting passes
   int nchunks;
-  int sort_warps;   // warps per block in the counting passes
-  size_t sort_smem; // dynamic shared memory of the counting passes
-  int64_t n_counts; // nbins * nchunks
+  int sort_warps;       // warps per CTA of the bin scatter pass
+  size_t sort_smem;     // its dynamic shared memory
+  int sort_warps_cell;  // same for the cell scatter pass
+  size_t sort_smem_cell;
+  int64_t n_counts; // max(nbins, ncell) * nchunks
   int64_t scan_blocks;
   int maxsub;       // points per subproblem
   int64_t max_subs; // upper bound on the number of subproblems
-  size_t off_keys, off_perm, off_counts, off_scan, off_bin_start, off_sub_bin, off_sub_start, off_nsub;
+  size_t off_keys, off_keys_cell, off_keys_by_cell, off_perm_cell, off_perm, off_counts, off_scan, off_bin_start,
+      off_sub_bin, off_sub_start, off_nsub;
   size_t total;
 };
 
 struct SortPtrs {
-  int* keys;
-  int* perm;
+  int* keys;          // bin key per point (input order)
+  int* keys_cell;     // cell-in-tile key per point (input order)
+  int* keys_by_cell;  // bin keys in cell-sorted order
+  int* perm_cell;     // cell-sorted order
+  int* perm;          // final (bin, cell) order
   int* counts;
   int* scan_tmp;
   int* bin_start;
@@ -81,6 +88,13 @@ template <typename T>
 cudaError_t launch_deconv_pad(int dim, const int nf[3], const int nm[3], const T* f1, const T* f2, const T* f3,
                               const void* f_in, void* fw_hat, int n_trans, cudaStream_t st);
 
+template <typename T>
+cudaError_t launch_deconv_batch(bool pad, const void* items, int n, int64_t total, cudaStream_t st);
+size_t deconv_item_bytes(int precision);
+// Fill a host table of batched deconvolution items; returns the total element count.
+int64_t fill_deconv_items(int precision, int dim, bool pad, const int* nf, const int* nm, const void* const* fac,
+                          const void* const* src, void* const* dst, int n, void* host_items);
+
 int num_sms();
 void set_error(const std::string& msg);
 
@@ -91,11 +105,16 @@ constexpr int warps_per_cta(size_t real_bytes, int dim, int ns) { return (real_b
 // per-warp staging of 32 points (weights, strengths, tile offsets).
 inline size_t spread_smem_bytes(size_t real_bytes, int dim, int ns, const Geom& g) {
   const int nw = warps_per_cta(real_bytes, dim, ns);
-  return 2 * real_bytes * (size_t)g.pad[2] * g.pad[1] * g.pitch + (size_t)nw * 32 * (dim * ns + 2) * real_bytes +
-         (size_t)nw * 32 * sizeof(int);
+  return 2 * real_bytes * (size_t)g.pad[2] * g.pad[1] * g.pitch +
+         ((size_t)dim * ns * (nw * 32 + 1) + (size_t)2 * nw * 32) * real_bytes + (size_t)nw * 32 * sizeof(int);
 }
 inline size_t tile_smem_bytes(size_t real_bytes, const Geom& g) {
   return 2 * real_bytes * (size_t)g.pad[2] * g.pad[1] * g.pitch;
+}
+inline size_t interp_smem_bytes(size_t real_bytes, int dim, int ns, const Geom& g) {
+  (void)dim;
+  (void)ns;
+  return tile_smem_bytes(real_bytes, g);
 }
 
 // Persistent grid size for a kernel: SMs x resident CTAs (cached per device,

@@ -8,7 +8,7 @@
 // lives in the file-scope array below, which every GPU that loads the library
 // holds until the process exits.
 //
-// * Limit: kNoAllocScratchBytes (64 MiB) of scratch, enough for about seven
+// * Limit: kNoAllocScratchBytes (64 MiB) of scratch, enough for about three
 //   million 2D points; a request needing more is rejected with
 //   NFX_ERR_UNSUPPORTED before any device work.
 // * Set-up: the first call on a device, with that device current, looks up the

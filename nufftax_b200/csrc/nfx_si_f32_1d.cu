@@ -7,4 +7,6 @@ template cudaError_t dispatch_spread<float, 1>(int, const PointArgs<float>&, con
 template cudaError_t dispatch_interp<float, 1>(int, const PointArgs<float>&, const void*, void*, cudaStream_t);
 template cudaError_t dispatch_grad<float, 1>(int, const PointArgs<float>&, const void*, const void*, void*, void*,
                                                void*, void*, cudaStream_t);
+template cudaError_t dispatch_batch<float, 1>(int, bool, const void*, int, const int*, int64_t, size_t,
+                                             cudaStream_t);
 }  // namespace nfx

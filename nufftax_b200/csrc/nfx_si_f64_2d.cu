@@ -7,4 +7,6 @@ template cudaError_t dispatch_spread<double, 2>(int, const PointArgs<double>&, c
 template cudaError_t dispatch_interp<double, 2>(int, const PointArgs<double>&, const void*, void*, cudaStream_t);
 template cudaError_t dispatch_grad<double, 2>(int, const PointArgs<double>&, const void*, const void*, void*, void*,
                                                void*, void*, cudaStream_t);
+template cudaError_t dispatch_batch<double, 2>(int, bool, const void*, int, const int*, int64_t, size_t,
+                                             cudaStream_t);
 }  // namespace nfx

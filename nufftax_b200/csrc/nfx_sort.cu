@@ -3,30 +3,57 @@
 // The reference has no sort (nufftax spreads unsorted points with atomics,
 // nufftax/core/pallas_spread.py:337-613).  Here every point gets the key of the
 // tile that holds its footprint's left cell (i0 = ceil(fold(x) - ns/2) wrapped
-// into [0, nf), divided by the tile edge, x-fastest), and the permutation is the
-// STABLE counting sort of those keys, so it equals numpy.argsort(keys,
-// kind="stable") bit for bit.
+// into [0, nf), divided by the tile edge, x-fastest) and the index of that cell
+// inside the tile, and the permutation is the STABLE sort by (bin, cell): it
+// equals numpy.argsort(bin * cells_per_tile + cell, kind="stable") bit for bit.
+// It is computed least-significant key first, as two stable counting passes
+// (cell, then bin); each pass is:
 //
-// Pass 1 (k_bin_count): one warp per chunk of consecutive points computes the
-//   keys and a per-chunk histogram in shared memory; the histogram is written to
-//   a bin-major matrix counts[bin][chunk].
-// Pass 2 (exclusive scan of that matrix): entry (bin, chunk) becomes the global
-//   position of the chunk's first point of that bin.
-// Pass 3 (k_bin_scatter): the same warps walk their chunk again in order; a
-//   __match_any_sync ballot ranks equal keys within each 32-point round and a
-//   shared-memory running count carries the rank across rounds, so ties keep
-//   their input order.
-// Pass 4 (k_subproblems): bins larger than max_subproblem points are split into
-//   subproblems so clustered inputs spread evenly over the SMs.
+// (1) count (k_bin_count, k_key_count): one CTA per chunk of consecutive
+//     elements builds the chunk's key histogram in shared memory and writes it
+//     to a key-major matrix counts[key][chunk];
+// (2) an exclusive scan of that matrix: entry (key, chunk) becomes the global
+//     position of the chunk's first element with that key;
+// (3) scatter (k_bin_scatter): one CTA per chunk again, each warp on a
+//     contiguous sub-chunk; ballots rank equal keys within each 32-element
+//     round (peer_mask: one ballot per key bit) and per-warp
+//     running counts (offset by the warps before it) carry the rank across
+//     rounds, so ties keep their input order.
+// Finally k_subproblems splits bins larger than max_subproblem points into
+// subproblems so clustered inputs spread evenly over the SMs.  Points of a
+// subproblem are then ordered by cell, which lets spreading merge runs of points
+// that share a cell and gives interpolation near-identical addresses per warp.
 #include "nfx_internal.h"
 
 namespace nfx {
 
+// Lanes of the warp holding the same key as this lane: one ballot per key bit.
+// Keys are in [-1, nkeys); the +1 shift keeps the inactive lanes (-1) apart
+// from every real key within `nbits` = bit length of nkeys.
+__device__ __forceinline__ unsigned peer_mask(int key, int nbits) {
+  const unsigned k = (unsigned)(key + 1);
+  unsigned m = 0xffffffffu;
+  for (int b = 0; b < nbits; ++b) {
+    const unsigned bit = (k >> b) & 1u;
+    const unsigned bal = __ballot_sync(0xffffffffu, bit);
+    m &= bit ? bal : ~bal;
+  }
+  return m;
+}
+
+__host__ __device__ inline int key_bits(int nkeys) {
+  int b = 0;
+  while ((1 << b) < nkeys + 1) ++b;
+  return b;
+}
+
+// Bin of the tile holding the footprint's left cell, and that cell's index
+// inside the tile (both x-fastest).
 template <typename T>
-__device__ __forceinline__ int point_key(const T* __restrict__ x, const T* __restrict__ y,
-                                         const T* __restrict__ z, int64_t p, const Geom& g, int ns_half) {
-  int key = 0;
-  int mult = 1;
+__device__ __forceinline__ void point_keys(const T* __restrict__ x, const T* __restrict__ y,
+                                           const T* __restrict__ z, int64_t p, const Geom& g, int ns_half, int& kbin,
+                                           int& kcell) {
+  int kb = 0, kc = 0, mb = 1, mc = 1;
   const T* cs[3] = {x, y, z};
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
@@ -34,64 +61,130 @@ __device__ __forceinline__ int point_key(const T* __restrict__ x, const T* __res
       T xs = scaled_coord(cs[d][p], g.nf[d], g.prenorm);
       int i0 = ceil_to_int(rn_sub(xs, (T)ns_half));
       int i0w = wrap_index(i0, g.nf[d]);
-      key += (i0w / g.tile[d]) * mult;
-      mult *= g.nb[d];
+      int bq = i0w / g.tile[d];
+      kb += bq * mb;
+      kc += (i0w - bq * g.tile[d]) * mc;
+      mb *= g.nb[d];
+      mc *= g.tile[d];
     }
   }
-  return key;
+  kbin = kb;
+  kcell = kc;
 }
 
+// Count pass of the cell sort: one CTA per chunk walks its points, 4 per thread
+// per trip so the coordinate loads overlap, writes both keys of every point and
+// counts the cell keys with shared-memory atomics.
 template <typename T>
 __global__ void k_bin_count(const T* __restrict__ x, const T* __restrict__ y, const T* __restrict__ z,
-                            int64_t M, Geom g, int ns_half, int chunk, int nchunks,
-                            int* __restrict__ keys, int* __restrict__ counts) {
+                            int64_t M, Geom g, int ns_half, int chunk, int nchunks, int ncell,
+                            int* __restrict__ keys_bin, int* __restrict__ keys_cell, int* __restrict__ counts) {
   extern __shared__ int s_hist[];
-  const int warps = blockDim.x >> 5;
-  const int w = threadIdx.x >> 5;
-  const int lane = threadIdx.x & 31;
-  const int ch = blockIdx.x * warps + w;
-  int* hist = s_hist + (size_t)w * g.nbins;
-  for (int b = lane; b < g.nbins; b += 32) hist[b] = 0;
-  __syncwarp();
-  if (ch < nchunks) {
-    const int64_t p0 = (int64_t)ch * chunk;
-    const int64_t p1 = (p0 + chunk < M) ? p0 + chunk : M;
-    for (int64_t p = p0 + lane; p < p1; p += 32) {
-      int key = point_key(x, y, z, p, g, ns_half);
-      keys[p] = key;
-      atomicAdd(&hist[key], 1);
-    }
-    __syncwarp();
-    for (int b = lane; b < g.nbins; b += 32) counts[(int64_t)b * nchunks + ch] = hist[b];
-  }
-}
-
-__global__ void k_bin_scatter(const int* __restrict__ keys, int64_t M, int nbins, int chunk, int nchunks,
-                              const int* __restrict__ offsets, int* __restrict__ perm) {
-  extern __shared__ int s_hist[];
-  const int warps = blockDim.x >> 5;
-  const int w = threadIdx.x >> 5;
-  const int lane = threadIdx.x & 31;
-  const int ch = blockIdx.x * warps + w;
-  int* hist = s_hist + (size_t)w * nbins;
-  for (int b = lane; b < nbins; b += 32) hist[b] = 0;
-  __syncwarp();
-  if (ch >= nchunks) return;
+  const int ch = blockIdx.x;
+  for (int b = threadIdx.x; b < ncell; b += blockDim.x) s_hist[b] = 0;
+  __syncthreads();
   const int64_t p0 = (int64_t)ch * chunk;
   const int64_t p1 = (p0 + chunk < M) ? p0 + chunk : M;
+  constexpr int U = 4;
+  for (int64_t base = p0; base < p1; base += (int64_t)U * blockDim.x) {
+    int kb[U], kc[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int64_t p = base + (int64_t)u * blockDim.x + threadIdx.x;
+      kb[u] = kc[u] = -1;
+      if (p < p1) point_keys(x, y, z, p, g, ns_half, kb[u], kc[u]);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int64_t p = base + (int64_t)u * blockDim.x + threadIdx.x;
+      if (kc[u] >= 0) {
+        keys_bin[p] = kb[u];
+        keys_cell[p] = kc[u];
+        atomicAdd(&s_hist[kc[u]], 1);
+      }
+    }
+  }
+  __syncthreads();
+  for (int b = threadIdx.x; b < ncell; b += blockDim.x) counts[(int64_t)b * nchunks + ch] = s_hist[b];
+}
+
+// Histogram of an int key array per chunk (second pass of the sort).
+__global__ void k_key_count(const int* __restrict__ keys, int64_t M, int nkeys, int chunk, int nchunks,
+                            int* __restrict__ counts) {
+  extern __shared__ int s_hist[];
+  const int ch = blockIdx.x;
+  for (int b = threadIdx.x; b < nkeys; b += blockDim.x) s_hist[b] = 0;
+  __syncthreads();
+  const int64_t p0 = (int64_t)ch * chunk;
+  const int64_t p1 = (p0 + chunk < M) ? p0 + chunk : M;
+  for (int64_t p = p0 + threadIdx.x; p < p1; p += blockDim.x) atomicAdd(&s_hist[keys[p]], 1);
+  __syncthreads();
+  for (int b = threadIdx.x; b < nkeys; b += blockDim.x) counts[(int64_t)b * nchunks + ch] = s_hist[b];
+}
+
+// Scatter pass: one CTA per chunk; warp w owns the contiguous sub-chunk w of
+// the chunk and its own histogram row hw[w][*].  (A) each warp counts its keys,
+// (B) a prefix over the warps turns the rows into each warp's starting rank per
+// key, (C) each warp walks its sub-chunk in order and ranks equal keys with
+// peer_mask, so the result is a stable sort.  Element i goes to
+// out[pos] = vals ? vals[i] : i, and aux_out[pos] = aux_in[i] carries a second
+// array along.
+__global__ void k_bin_scatter(const int* __restrict__ keys, const int* __restrict__ vals, const int* __restrict__ aux_in,
+                              int64_t M, int nkeys, int chunk, int nchunks, const int* __restrict__ offsets,
+                              int* __restrict__ out, int* __restrict__ aux_out) {
+  extern __shared__ int s_hw[];
+  const int W = blockDim.x >> 5;
+  const int w = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const int ch = blockIdx.x;
+  for (int i = threadIdx.x; i < W * nkeys; i += blockDim.x) s_hw[i] = 0;
+  __syncthreads();
+  const int64_t p0 = (int64_t)ch * chunk;
+  const int64_t p1 = (p0 + chunk < M) ? p0 + chunk : M;
+  const int64_t sub = (((p1 - p0) + W - 1) / W + 31) / 32 * 32;
+  const int64_t s0 = p0 + (int64_t)w * sub < p1 ? p0 + (int64_t)w * sub : p1;
+  const int64_t s1 = s0 + sub < p1 ? s0 + sub : p1;
+  int* hist = s_hw + (size_t)w * nkeys;
   const unsigned lt_mask = (1u << lane) - 1u;
-  for (int64_t base = p0; base < p1; base += 32) {
+  const int kbits = key_bits(nkeys);
+  // (A) count this warp's keys (its own histogram row: order does not matter)
+  for (int64_t p = s0 + lane; p < s1; p += 32) atomicAdd(&hist[keys[p]], 1);
+  __syncthreads();
+  // (B) hw[w][k] = global start of key k in this chunk + count of k in warps < w
+  for (int k = threadIdx.x; k < nkeys; k += blockDim.x) {
+    int run = offsets[(int64_t)k * nchunks + ch];
+    for (int v = 0; v < W; ++v) {
+      const int t = s_hw[(size_t)v * nkeys + k];
+      s_hw[(size_t)v * nkeys + k] = run;
+      run += t;
+    }
+  }
+  __syncthreads();
+  // (C) stable placement; the next round's inputs are loaded ahead
+  int key_next = s0 + lane < s1 ? keys[s0 + lane] : -1;
+  int val_next = (s0 + lane < s1 && vals != nullptr) ? vals[s0 + lane] : 0;
+  int aux_next = (s0 + lane < s1 && aux_in != nullptr) ? aux_in[s0 + lane] : 0;
+  for (int64_t base = s0; base < s1; base += 32) {
     const int64_t p = base + lane;
-    const bool valid = p < p1;
-    const int key = valid ? keys[p] : -1;
-    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    const bool valid = p < s1;
+    const int key = key_next;
+    const int val = vals != nullptr ? val_next : (int)p;
+    const int aux = aux_next;
+    const int64_t pn = base + 32 + lane;
+    key_next = pn < s1 ? keys[pn] : -1;
+    if (vals != nullptr) val_next = pn < s1 ? vals[pn] : 0;
+    if (aux_in != nullptr) aux_next = pn < s1 ? aux_in[pn] : 0;
+    const unsigned peers = peer_mask(key, kbits);
     const int rank = __popc(peers & lt_mask);
-    int before = 0;
-    if (valid) before = hist[key];
+    int pos = 0;
+    if (valid) pos = hist[key];
     __syncwarp();
-    if (valid && rank == 0) hist[key] = before + __popc(peers);
+    if (valid && rank == 0) hist[key] = pos + __popc(peers);
     __syncwarp();
-    if (valid) perm[offsets[(int64_t)key * nchunks + ch] + before + rank] = (int)p;
+    if (valid) {
+      out[pos + rank] = val;
+      if (aux_out != nullptr) aux_out[pos + rank] = aux;
+    }
   }
 }
 
@@ -248,19 +341,35 @@ cudaError_t exclusive_scan(const int* in, int* out, int64_t n, int* block_sums, 
 template <typename T>
 cudaError_t launch_sort(const SortLayout& L, const Geom& g, int ns, const void* x, const void* y, const void* z,
                         int64_t M, const SortPtrs& P, cudaStream_t st) {
-  const int threads = L.sort_warps * 32;
-  const unsigned blocks = (unsigned)((L.nchunks + L.sort_warps - 1) / L.sort_warps);
-  const size_t smem = L.sort_smem;
-  cudaError_t e0 = ensure_smem(reinterpret_cast<const void*>(k_bin_count<T>), smem);
-  if (e0 == cudaSuccess) e0 = ensure_smem(reinterpret_cast<const void*>(k_bin_scatter), smem);
-  if (e0 != cudaSuccess) return e0;
-  k_bin_count<T><<<blocks, threads, smem, st>>>((const T*)x, (const T*)y, (const T*)z, M, g, ns / 2, L.chunk,
-                                                L.nchunks, P.keys, P.counts);
-  cudaError_t e = cudaGetLastError();
+  const int ncell = g.tile[0] * g.tile[1] * g.tile[2];
+  const size_t cell_smem = (size_t)ncell * sizeof(int);
+  const size_t bin_smem = (size_t)g.nbins * sizeof(int);
+  cudaError_t e = ensure_smem(reinterpret_cast<const void*>(k_bin_count<T>), cell_smem);
+  if (e == cudaSuccess) e = ensure_smem(reinterpret_cast<const void*>(k_key_count), bin_smem);
+  if (e == cudaSuccess)
+    e = ensure_smem(reinterpret_cast<const void*>(k_bin_scatter),
+                    L.sort_smem > L.sort_smem_cell ? L.sort_smem : L.sort_smem_cell);
   if (e != cudaSuccess) return e;
-  e = exclusive_scan(P.counts, P.counts, L.n_counts, P.scan_tmp, st);
+  // pass A: stable by cell-in-tile (carrying each point's bin key along)
+  k_bin_count<T><<<(unsigned)L.nchunks, 256, cell_smem, st>>>((const T*)x, (const T*)y, (const T*)z, M, g, ns / 2,
+                                                              L.chunk, L.nchunks, ncell, P.keys, P.keys_cell,
+                                                              P.counts);
+  e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  k_bin_scatter<<<blocks, threads, smem, st>>>(P.keys, M, g.nbins, L.chunk, L.nchunks, P.counts, P.perm);
+  e = exclusive_scan(P.counts, P.counts, (int64_t)ncell * L.nchunks, P.scan_tmp, st);
+  if (e != cudaSuccess) return e;
+  k_bin_scatter<<<(unsigned)L.nchunks, L.sort_warps_cell * 32, L.sort_smem_cell, st>>>(
+      P.keys_cell, nullptr, P.keys, M, ncell, L.chunk, L.nchunks, P.counts, P.perm_cell, P.keys_by_cell);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  // pass B: stable by bin over the cell-ordered sequence
+  k_key_count<<<(unsigned)L.nchunks, 256, bin_smem, st>>>(P.keys_by_cell, M, g.nbins, L.chunk, L.nchunks, P.counts);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  e = exclusive_scan(P.counts, P.counts, (int64_t)g.nbins * L.nchunks, P.scan_tmp, st);
+  if (e != cudaSuccess) return e;
+  k_bin_scatter<<<(unsigned)L.nchunks, L.sort_warps * 32, L.sort_smem, st>>>(
+      P.keys_by_cell, P.perm_cell, nullptr, M, g.nbins, L.chunk, L.nchunks, P.counts, P.perm, nullptr);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   k_subproblems<<<1, 1024, 0, st>>>(P.counts, g.nbins, L.nchunks, (int)M, L.maxsub, P.bin_start, P.sub_bin,

@@ -71,26 +71,26 @@ __device__ __forceinline__ T coord(const PointArgs<T>& a, int d, int p) {
 // Spread
 // ---------------------------------------------------------------------------
 template <typename T, int DIM, int NS, int NW>
-__global__ void __launch_bounds__(NW * 32) k_spread(PointArgs<T> a, const cplx_t<T>* __restrict__ c,
-                                                    cplx_t<T>* __restrict__ fw) {
+__device__ __forceinline__ void spread_subproblem(const PointArgs<T>& a, const cplx_t<T>* __restrict__ c,
+                                                  cplx_t<T>* __restrict__ fw, int sidx, unsigned char* smem_raw) {
   using CT = cplx_t<T>;
   constexpr int CELLS = Pow<NS, DIM>::value;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int SW = NW * 32 + 1;  // staging stride: odd, so both the per-lane writes and
+                                   // the per-point reads across q hit distinct banks
   const Geom& g = a.g;
   const int tile_cells = g.pad[2] * g.pad[1] * g.pitch;
   T* s_re = reinterpret_cast<T*>(smem_raw);
   T* s_im = s_re + tile_cells;
-  T* s_w = s_im + tile_cells;                  // NW*32*DIM*NS
-  T* s_c = s_w + NW * 32 * DIM * NS;           // NW*32*2
-  int* s_off = reinterpret_cast<int*>(s_c + NW * 32 * 2);  // NW*32
+  T* s_w = s_im + tile_cells;          // [DIM*NS][SW]
+  T* s_cr = s_w + DIM * NS * SW;       // [NW*32]
+  T* s_ci = s_cr + NW * 32;            // [NW*32]
+  int* s_off = reinterpret_cast<int*>(s_ci + NW * 32);  // [NW*32]
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   const int row = g.pitch;
   const int plane = g.pitch * g.pad[1];
-  const int nsub = *a.s.nsub;
   const int used = g.pad[0] * g.pad[1] * g.pad[2];
-
-  for (int sidx = blockIdx.x; sidx < nsub; sidx += gridDim.x) {
+  {
     const int b = a.s.sub_bin[sidx];
     const int k0 = a.s.sub_start[sidx];
     const int k1 = min(k0 + a.s.maxsub, a.s.bin_start[b + 1]);
@@ -99,10 +99,21 @@ __global__ void __launch_bounds__(NW * 32) k_spread(PointArgs<T> a, const cplx_t
     for (int t = 0; t < a.n_trans; ++t) {
       for (int i = threadIdx.x; i < 2 * tile_cells; i += blockDim.x) s_re[i] = (T)0;
       __syncthreads();
-      for (int kb = k0 + warp * 32; kb < k1; kb += NW * 32) {
+      // Each warp takes a contiguous slice of the subproblem, so the cell
+      // order of the points carries across its batches.
+      const int per = ((k1 - k0 + NW - 1) / NW + 31) / 32 * 32;
+      const int w0 = min(k0 + warp * per, k1);
+      const int w1 = min(w0 + per, k1);
+      constexpr int R = (CELLS + 31) / 32;
+      constexpr bool MERGE = CELLS >= 32 && R <= 16;
+      T accr[MERGE ? R : 1], acci[MERGE ? R : 1];
+      int run_off = -1;
+#pragma unroll
+      for (int r = 0; r < (MERGE ? R : 1); ++r) accr[r] = acci[r] = (T)0;
+      for (int kb = w0; kb < w1; kb += 32) {
         const int k = kb + lane;
         const int slot = warp * 32 + lane;
-        if (k < k1) {
+        if (k < w1) {
           const int p = a.s.perm[k];
           int off = 0;
           bool inside = true;
@@ -116,38 +127,121 @@ __global__ void __launch_bounds__(NW * 32) k_spread(PointArgs<T> a, const cplx_t
             // the tile.
             inside = inside && (unsigned)l < (unsigned)g.tile[d];
             off += l * (d == 0 ? 1 : (d == 1 ? row : plane));
-            T* w = s_w + (slot * DIM + d) * NS;
 #pragma unroll
-            for (int q = 0; q < NS; ++q) w[q] = es_weight(rn_sub((T)(i0 + q), xs), a.beta, a.kc);
+            for (int q = 0; q < NS; ++q)
+              s_w[(d * NS + q) * SW + slot] = es_weight(rn_sub((T)(i0 + q), xs), a.beta, a.kc);
           }
           const CT cv = c[(int64_t)t * a.M + p];
           s_off[slot] = inside ? off : 0;
-          s_c[2 * slot] = inside ? cv.x : (T)0;
-          s_c[2 * slot + 1] = inside ? cv.y : (T)0;
+          s_cr[slot] = inside ? cv.x : (T)0;
+          s_ci[slot] = inside ? cv.y : (T)0;
         }
         __syncwarp();
-        const int cnt = min(32, k1 - kb);
-        const int items = cnt * CELLS;
-        for (int it = lane; it < items; it += 32) {
-          const int j = it / CELLS;
-          const int q = it - j * CELLS;
-          const int kx = q % NS;
-          const int ky = (q / NS) % NS;
-          const int kz = q / (NS * NS);
-          const int sj = warp * 32 + j;
-          const T* wj = s_w + sj * DIM * NS;
-          T w;
-          if (DIM == 1)
-            w = wj[kx];
-          else if (DIM == 2)
-            w = wj[NS + ky] * wj[kx];
-          else
-            w = (wj[2 * NS + kz] * wj[NS + ky]) * wj[kx];
-          const int addr = s_off[sj] + kz * plane + ky * row + kx;
-          atomicAdd(&s_re[addr], s_c[2 * sj] * w);
-          atomicAdd(&s_im[addr], s_c[2 * sj + 1] * w);
+        const int cnt = min(32, w1 - kb);
+        if constexpr (MERGE) {
+          // One point at a time, lane l on cells l, l+32, ...; consecutive
+          // points in the same cell add into registers and reach shared memory
+          // once per run.
+          for (int j = 0; j < cnt; ++j) {
+            const int sj = warp * 32 + j;
+            const int off = s_off[sj];
+            if (off != run_off) {
+              if (run_off >= 0) {
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                  const int q = lane + 32 * r;
+                  if (CELLS % 32 == 0 || q < CELLS) {
+                    const int addr = run_off + (q / (NS * NS)) * plane + ((q / NS) % NS) * row + q % NS;
+                    atomicAdd(&s_re[addr], accr[r]);
+                    atomicAdd(&s_im[addr], acci[r]);
+                  }
+                  accr[r] = acci[r] = (T)0;
+                }
+              }
+              run_off = off;
+            }
+            const T cr = s_cr[sj], ci = s_ci[sj];
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+              const int q = lane + 32 * r;
+              if (CELLS % 32 == 0 || q < CELLS) {
+                const int kx = q % NS;
+                const int ky = (q / NS) % NS;
+                const int kz = q / (NS * NS);
+                T w;
+                if (DIM == 1)
+                  w = s_w[kx * SW + sj];
+                else if (DIM == 2)
+                  w = s_w[(NS + ky) * SW + sj] * s_w[kx * SW + sj];
+                else
+                  w = (s_w[(2 * NS + kz) * SW + sj] * s_w[(NS + ky) * SW + sj]) * s_w[kx * SW + sj];
+                accr[r] += cr * w;
+                acci[r] += ci * w;
+              }
+            }
+          }
+        } else if (CELLS >= 32) {
+          // large footprints: one point at a time, straight to shared memory
+          for (int j = 0; j < cnt; ++j) {
+            const int sj = warp * 32 + j;
+            const T cr = s_cr[sj], ci = s_ci[sj];
+            const int off = s_off[sj];
+#pragma unroll 4
+            for (int r = 0; r < R; ++r) {
+              const int q = lane + 32 * r;
+              if (CELLS % 32 == 0 || q < CELLS) {
+                const int kx = q % NS;
+                const int ky = (q / NS) % NS;
+                const int kz = q / (NS * NS);
+                T w;
+                if (DIM == 1)
+                  w = s_w[kx * SW + sj];
+                else if (DIM == 2)
+                  w = s_w[(NS + ky) * SW + sj] * s_w[kx * SW + sj];
+                else
+                  w = (s_w[(2 * NS + kz) * SW + sj] * s_w[(NS + ky) * SW + sj]) * s_w[kx * SW + sj];
+                const int addr = off + kz * plane + ky * row + kx;
+                atomicAdd(&s_re[addr], cr * w);
+                atomicAdd(&s_im[addr], ci * w);
+              }
+            }
+          }
+        } else {
+          // small footprints: several points per instruction
+          const int items = cnt * CELLS;
+          for (int it = lane; it < items; it += 32) {
+            const int j = it / CELLS;
+            const int q = it - j * CELLS;
+            const int kx = q % NS;
+            const int ky = (q / NS) % NS;
+            const int kz = q / (NS * NS);
+            const int sj = warp * 32 + j;
+            T w;
+            if (DIM == 1)
+              w = s_w[kx * SW + sj];
+            else if (DIM == 2)
+              w = s_w[(NS + ky) * SW + sj] * s_w[kx * SW + sj];
+            else
+              w = (s_w[(2 * NS + kz) * SW + sj] * s_w[(NS + ky) * SW + sj]) * s_w[kx * SW + sj];
+            const int addr = s_off[sj] + kz * plane + ky * row + kx;
+            atomicAdd(&s_re[addr], s_cr[sj] * w);
+            atomicAdd(&s_im[addr], s_ci[sj] * w);
+          }
         }
         __syncwarp();
+      }
+      if constexpr (MERGE) {
+        if (run_off >= 0) {
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const int q = lane + 32 * r;
+            if (CELLS % 32 == 0 || q < CELLS) {
+              const int addr = run_off + (q / (NS * NS)) * plane + ((q / NS) % NS) * row + q % NS;
+              atomicAdd(&s_re[addr], accr[r]);
+              atomicAdd(&s_im[addr], acci[r]);
+            }
+          }
+        }
       }
       __syncthreads();
       CT* out = fw + (int64_t)t * a.grid_stride;
@@ -171,6 +265,14 @@ __global__ void __launch_bounds__(NW * 32) k_spread(PointArgs<T> a, const cplx_t
       __syncthreads();
     }
   }
+}
+
+template <typename T, int DIM, int NS, int NW>
+__global__ void __launch_bounds__(NW * 32) k_spread(PointArgs<T> a, const cplx_t<T>* __restrict__ c,
+                                                    cplx_t<T>* __restrict__ fw) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int nsub = *a.s.nsub;
+  for (int sidx = blockIdx.x; sidx < nsub; sidx += gridDim.x) spread_subproblem<T, DIM, NS, NW>(a, c, fw, sidx, smem_raw);
 }
 
 // ---------------------------------------------------------------------------
@@ -199,16 +301,14 @@ __device__ __forceinline__ void stage_tile(const Geom& g, const int o[3], const 
 // Interp
 // ---------------------------------------------------------------------------
 template <typename T, int DIM, int NS, int NW>
-__global__ void __launch_bounds__(NW * 32) k_interp(PointArgs<T> a, const cplx_t<T>* __restrict__ fw,
-                                                    cplx_t<T>* __restrict__ cout) {
+__device__ __forceinline__ void interp_subproblem(const PointArgs<T>& a, const cplx_t<T>* __restrict__ fw,
+                                                  cplx_t<T>* __restrict__ cout, int sidx, unsigned char* smem_raw) {
   using CT = cplx_t<T>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
   CT* s_tile = reinterpret_cast<CT*>(smem_raw);
   const Geom& g = a.g;
   const int row = g.pitch;
   const int plane = g.pitch * g.pad[1];
-  const int nsub = *a.s.nsub;
-  for (int sidx = blockIdx.x; sidx < nsub; sidx += gridDim.x) {
+  {
     const int b = a.s.sub_bin[sidx];
     const int k0 = a.s.sub_start[sidx];
     const int k1 = min(k0 + a.s.maxsub, a.s.bin_start[b + 1]);
@@ -276,6 +376,67 @@ __global__ void __launch_bounds__(NW * 32) k_interp(PointArgs<T> a, const cplx_t
         cout[(int64_t)t * a.M + p] = r;
       }
     }
+  }
+}
+
+template <typename T, int DIM, int NS, int NW>
+__global__ void __launch_bounds__(NW * 32) k_interp(PointArgs<T> a, const cplx_t<T>* __restrict__ fw,
+                                                    cplx_t<T>* __restrict__ cout) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int nsub = *a.s.nsub;
+  for (int sidx = blockIdx.x; sidx < nsub; sidx += gridDim.x)
+    interp_subproblem<T, DIM, NS, NW>(a, fw, cout, sidx, smem_raw);
+}
+
+// ---------------------------------------------------------------------------
+// Batched launches: many problems (own points, grid, tiling and sort) in one
+// persistent launch.  `items` is a device table; `sub_prefix[p]` is the number
+// of subproblems of problems < p (k_batch_prefix), so the CTAs walk one global
+// work queue of (problem, bin tile) items.
+// ---------------------------------------------------------------------------
+template <typename T>
+struct BatchItem {
+  PointArgs<T> a;
+  const void* src;  // spread: strengths; interp: fine grid
+  void* dst;        // spread: fine grid (zeroed by the caller); interp: values
+};
+
+__device__ __forceinline__ int batch_find(const int* __restrict__ prefix, int n, int g) {
+  int lo = 0, hi = n;  // largest p with prefix[p] <= g
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (prefix[mid] <= g)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+template <typename T, int DIM, int NS, int NW>
+__global__ void __launch_bounds__(NW * 32) k_spread_batch(const BatchItem<T>* __restrict__ items, int nitems,
+                                                          const int* __restrict__ sub_prefix) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int total = sub_prefix[nitems];
+  for (int gi = blockIdx.x; gi < total; gi += gridDim.x) {
+    const int p = batch_find(sub_prefix, nitems, gi);
+    const BatchItem<T>& it = items[p];
+    spread_subproblem<T, DIM, NS, NW>(it.a, (const cplx_t<T>*)it.src, (cplx_t<T>*)it.dst, gi - sub_prefix[p],
+                                      smem_raw);
+    __syncthreads();
+  }
+}
+
+template <typename T, int DIM, int NS, int NW>
+__global__ void __launch_bounds__(NW * 32) k_interp_batch(const BatchItem<T>* __restrict__ items, int nitems,
+                                                          const int* __restrict__ sub_prefix) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int total = sub_prefix[nitems];
+  for (int gi = blockIdx.x; gi < total; gi += gridDim.x) {
+    const int p = batch_find(sub_prefix, nitems, gi);
+    const BatchItem<T>& it = items[p];
+    interp_subproblem<T, DIM, NS, NW>(it.a, (const cplx_t<T>*)it.src, (cplx_t<T>*)it.dst, gi - sub_prefix[p],
+                                      smem_raw);
   }
 }
 
@@ -444,6 +605,44 @@ struct Launch {
     return cudaGetLastError();
   }
 };
+
+template <typename T, int DIM, int NS>
+struct BatchLaunch {
+  static constexpr int NW = warps_per_cta(sizeof(T), DIM, NS);
+  static cudaError_t spread(const void* items, int n, const int* prefix, int64_t max_subs, size_t smem,
+                            cudaStream_t st) {
+    int grid = 0;
+    cudaError_t e = kernel_grid(reinterpret_cast<const void*>(k_spread_batch<T, DIM, NS, NW>), NW * 32, smem, max_subs,
+                                grid);
+    if (e != cudaSuccess) return e;
+    k_spread_batch<T, DIM, NS, NW><<<grid, NW * 32, smem, st>>>((const BatchItem<T>*)items, n, prefix);
+    return cudaGetLastError();
+  }
+  static cudaError_t interp(const void* items, int n, const int* prefix, int64_t max_subs, size_t smem,
+                            cudaStream_t st) {
+    int grid = 0;
+    cudaError_t e = kernel_grid(reinterpret_cast<const void*>(k_interp_batch<T, DIM, NS, NW>), NW * 32, smem, max_subs,
+                                grid);
+    if (e != cudaSuccess) return e;
+    k_interp_batch<T, DIM, NS, NW><<<grid, NW * 32, smem, st>>>((const BatchItem<T>*)items, n, prefix);
+    return cudaGetLastError();
+  }
+};
+
+template <typename T, int DIM>
+cudaError_t dispatch_batch(int ns, bool spread, const void* items, int n, const int* prefix, int64_t max_subs,
+                           size_t smem, cudaStream_t st) {
+  switch (ns) {
+#define NFX_CASE(N)                                                                    \
+  case N:                                                                              \
+    return spread ? BatchLaunch<T, DIM, N>::spread(items, n, prefix, max_subs, smem, st) \
+                  : BatchLaunch<T, DIM, N>::interp(items, n, prefix, max_subs, smem, st);
+    NFX_CASE(2) NFX_CASE(4) NFX_CASE(6) NFX_CASE(8) NFX_CASE(10) NFX_CASE(12) NFX_CASE(14) NFX_CASE(16)
+#undef NFX_CASE
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
 
 template <typename T, int DIM>
 cudaError_t dispatch_spread(int ns, const PointArgs<T>& a, const void* c, void* fw, cudaStream_t st) {

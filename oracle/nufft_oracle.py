@@ -192,29 +192,33 @@ def cell_index(xs: np.ndarray, nspread: int) -> np.ndarray:
 
 
 def bin_keys(coords: Sequence[np.ndarray], nf: Sequence[int], nspread: int, tile: Sequence[int],
-             prenorm: bool) -> np.ndarray:
-    """Bin index of every point.
+             prenorm: bool):
+    """(bin key, cell key) of every point.
 
-    The point's left cell i0 = ceil(fold(x) - ns/2) is wrapped into [0, nf) and
-    divided by the tile edge; bins are numbered x-fastest:
-    key = (bz * nby + by) * nbx + bx.
+    The point's left cell i0 = ceil(fold(x) - ns/2) is wrapped into [0, nf); its
+    bin is i0 // tile per axis and its cell is i0 % tile per axis, both numbered
+    x-fastest: bin = (bz * nby + by) * nbx + bx, cell = (lz * ty + ly) * tx + lx.
     """
-    key = np.zeros(coords[0].shape[0], dtype=np.int64)
-    mult = 1
+    kb = np.zeros(coords[0].shape[0], dtype=np.int64)
+    kc = np.zeros(coords[0].shape[0], dtype=np.int64)
+    mb = mc = 1
     for d in range(len(coords)):
         x = premod(coords[d]) if prenorm else coords[d]
         i0 = cell_index(fold_rescale(x, nf[d]), nspread)
         i0w = np.mod(i0, nf[d])
         nb = -(-nf[d] // tile[d])
-        key += (i0w // tile[d]) * mult
-        mult *= nb
-    return key.astype(np.int32)
+        kb += (i0w // tile[d]) * mb
+        kc += (i0w % tile[d]) * mc
+        mb *= nb
+        mc *= tile[d]
+    return kb.astype(np.int32), kc.astype(np.int32)
 
 
-def bin_sort(keys: np.ndarray, nbins: int):
-    """Stable counting sort: (perm, bin_start) with perm[k] = index of k-th point."""
-    perm = np.argsort(keys, kind="stable").astype(np.int32)
-    counts = np.bincount(keys, minlength=nbins)
+def bin_sort(kbin: np.ndarray, kcell: np.ndarray, nbins: int, ncell: int):
+    """Stable sort by (bin, cell): (perm, bin_start), perm[k] = index of the k-th point."""
+    fine = kbin.astype(np.int64) * ncell + kcell.astype(np.int64)
+    perm = np.argsort(fine, kind="stable").astype(np.int32)
+    counts = np.bincount(kbin, minlength=nbins)
     bin_start = np.zeros(nbins + 1, dtype=np.int64)
     np.cumsum(counts, out=bin_start[1:])
     return perm, bin_start.astype(np.int32)

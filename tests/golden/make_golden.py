@@ -7,7 +7,8 @@ the oracle to the reference's own test oracles instead:
     nufftax tests/conftest.py:154-198 and tests/test_nufft3.py:26-72;
   * the oracle's own outputs on the same seeded inputs (regression values for
     the CUDA path and the oracle);
-  * bit-exact bin keys / stable permutation for float32 coordinates that include
+  * bit-exact bin / cell keys and the stable (bin, cell) permutation for float32
+    coordinates that include
     the folding edge cases (x = +-pi, values rounding to the grid end, values
     outside [-pi, pi)).
 Inputs are seeded, so the script is reproducible.
@@ -99,10 +100,12 @@ def make_sort(rng):
             X[i][500:1500] = (0.3 * rng.standard_normal(1000)).astype(np.float32)
         d = {f"x{i}": X[i] for i in range(dim)}
         nbins = int(np.prod([-(-n // t) for n, t in zip(nf, tile)]))
+        ncell = int(np.prod(tile))
         for prenorm in (0, 1):
-            keys = O.bin_keys(X, nf, ns, tile, bool(prenorm))
-            perm, bin_start = O.bin_sort(keys, nbins)
+            keys, cells = O.bin_keys(X, nf, ns, tile, bool(prenorm))
+            perm, bin_start = O.bin_sort(keys, cells, nbins, ncell)
             d[f"keys_p{prenorm}"] = keys
+            d[f"cells_p{prenorm}"] = cells
             d[f"perm_p{prenorm}"] = perm
             d[f"bin_start_p{prenorm}"] = bin_start
         d["nf"] = np.array(nf)

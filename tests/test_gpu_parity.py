@@ -74,8 +74,9 @@ def test_sort_random_bit_exact(dim, nf, dist, dtype):
     kp = nb.compute_kernel_params(1e-6)
     ps = PointSort([to_dev(x) for x in X], nf, kp, prenorm=True)
     keys, perm, bstart = ps.results()
-    okeys = O.bin_keys(X, nf, kp.nspread, ps.tile, True)
-    operm, obs = O.bin_sort(okeys, int(np.prod([-(-n // t) for n, t in zip(nf, ps.tile)])))
+    okeys, ocells = O.bin_keys(X, nf, kp.nspread, ps.tile, True)
+    operm, obs = O.bin_sort(okeys, ocells, int(np.prod([-(-n // t) for n, t in zip(nf, ps.tile)])),
+                            int(np.prod(ps.tile)))
     assert np.array_equal(keys.cpu().numpy(), okeys)
     assert np.array_equal(perm.cpu().numpy(), operm)
     assert np.array_equal(bstart.cpu().numpy(), obs)

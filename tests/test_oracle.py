@@ -90,16 +90,18 @@ def test_sort_fixture_reproduces(name):
     dim = len(d["nf"])
     X = [d[f"x{i}"] for i in range(dim)]
     nbins = int(np.prod([-(-n // t) for n, t in zip(d["nf"], d["tile"])]))
+    ncell = int(np.prod(d["tile"]))
     for p in (0, 1):
-        keys = O.bin_keys(X, d["nf"], int(d["ns"]), d["tile"], bool(p))
+        keys, cells = O.bin_keys(X, d["nf"], int(d["ns"]), d["tile"], bool(p))
         assert np.array_equal(keys, d[f"keys_p{p}"])
-        perm, bs = O.bin_sort(keys, nbins)
+        assert np.array_equal(cells, d[f"cells_p{p}"])
+        perm, bs = O.bin_sort(keys, cells, nbins, ncell)
         assert np.array_equal(perm, d[f"perm_p{p}"])
         assert np.array_equal(bs, d[f"bin_start_p{p}"])
-        # stable: within a bin the original order is kept
-        sk = keys[perm]
-        assert np.all(np.diff(sk) >= 0)
-        same = np.diff(sk) == 0
+        # ordered by (bin, cell); stable: equal keys keep the original order
+        fine = keys.astype(np.int64)[perm] * ncell + cells[perm]
+        assert np.all(np.diff(fine) >= 0)
+        same = np.diff(fine) == 0
         assert np.all(np.diff(perm)[same] > 0)
 
 
