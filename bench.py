@@ -513,6 +513,250 @@ def run_batched(args):
     print(json.dumps(line), flush=True)
 
 
+def run_grad3d(args):
+    """3D type 1, M = 8e6 uniform points, 128^3 modes, eps 1e-6, complex64:
+    loss = ||nufft3d1(x, y, z, c) - f_target||^2 and its gradients w.r.t. c, x, y, z
+    through the hand-written adjoint kernels (forward + backward per step).
+    --check adds, at full size: central finite differences in complex128 on 32
+    random entries, and the reference's spectral gradient formula (JVP with
+    k-weighted transforms, then transpose; nufftax/transforms/primitives.py:443-471)
+    evaluated with this library's type-2 transforms."""
+    import torch
+
+    import nufftax_b200 as nb
+
+    dev = torch.device("cuda", 0)
+    M, N, eps = int(8_000_000 * args.scale), (128, 128, 128), 1e-6
+    rng = np.random.default_rng(4)
+    X = [torch.from_numpy(rng.uniform(-np.pi, np.pi, M).astype(np.float32)).to(dev) for _ in range(3)]
+    c = torch.from_numpy((rng.standard_normal(M) + 1j * rng.standard_normal(M)).astype(np.complex64)).to(dev)
+    tgt = torch.from_numpy((rng.standard_normal(N[::-1]) + 1j * rng.standard_normal(N[::-1])).astype(np.complex64)
+                           ).to(dev)
+
+    def step():
+        nb.sort_cache.clear()
+        xs = [x.detach().requires_grad_(True) for x in X]
+        cc = c.detach().requires_grad_(True)
+        f = nb.nufft3d1(*xs, cc, N, eps=eps)
+        loss = (f - tgt).abs().pow(2).sum()
+        loss.backward()
+        return loss, cc.grad, [x.grad for x in xs]
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    tot = 0.0
+    for _ in range(args.steps):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        step()
+        b.record()
+        torch.cuda.synchronize()
+        tot += a.elapsed_time(b)
+    ms = tot / args.steps
+    line = {"metric": "differentiated 3D type-1 NU points/s (forward + backward w.r.t. c, x, y, z)",
+            "value": M / (ms / 1e3), "unit": "NU points/s", "ms_per_step": ms, "steps": args.steps,
+            "config": {"workload": f"M={M} uniform 3D, 128^3 modes, nf 256^3, eps 1e-6, complex64"}}
+    if args.check:
+        line["check"] = grad3d_check(M, N, rng)
+    print(json.dumps(line), flush=True)
+
+
+def grad3d_check(M, N, rng):
+    import torch
+
+    import nufftax_b200 as nb
+
+    dev = torch.device("cuda", 0)
+    out = {}
+    # (1) central finite differences, complex128, 32 random entries (both sides
+    # differentiate the same approximate transform, so eps does not limit agreement)
+    eps = 1e-7
+    X = [torch.from_numpy(rng.uniform(-np.pi, np.pi, M)).to(dev) for _ in range(3)]
+    c = torch.from_numpy(rng.standard_normal(M) + 1j * rng.standard_normal(M)).to(dev)
+    tgt = torch.from_numpy(rng.standard_normal(N[::-1]) + 1j * rng.standard_normal(N[::-1])).to(dev)
+    xs = [x.clone().requires_grad_(True) for x in X]
+    cc = c.clone().requires_grad_(True)
+    loss = (nb.nufft3d1(*xs, cc, N, eps=eps) - tgt).abs().pow(2).sum()
+    loss.backward()
+
+    def L():
+        with torch.no_grad():
+            return float((nb.nufft3d1(*xs, cc, N, eps=eps) - tgt).abs().pow(2).sum())
+
+    h = 1e-4
+    errs = []
+    for e in range(32):
+        j = int(rng.integers(M))
+        which = e % 5  # c.re, c.im, x, y, z
+        with torch.no_grad():
+            if which < 2:
+                unit = 1.0 if which == 0 else 1j
+                base = cc[j].item()
+                cc[j] = base + unit * h
+                lp = L()
+                cc[j] = base - unit * h
+                lm = L()
+                cc[j] = base
+                an = cc.grad[j].real.item() if which == 0 else cc.grad[j].imag.item()
+            else:
+                t = xs[which - 2]
+                base = t[j].item()
+                t[j] = base + h
+                lp = L()
+                t[j] = base - h
+                lm = L()
+                t[j] = base
+                an = t.grad[j].item()
+        fd = (lp - lm) / (2 * h)
+        errs.append(abs(an - fd) / max(abs(fd), 1e-300))
+    out["fd_c128_h1e-4_max_rel_err"] = max(errs)
+    out["fd_c128_h1e-4_median_rel_err"] = float(np.median(errs))
+    # (2) spectral formula of the reference (complex64 forward, eps 1e-6)
+    x32 = [x.float().requires_grad_(True) for x in X]
+    c64 = c.to(torch.complex64).requires_grad_(True)
+    t64 = tgt.to(torch.complex64)
+    f = nb.nufft3d1(*x32, c64, N, eps=1e-6)
+    G = 2 * (f.detach() - t64)
+    (f - t64).abs().pow(2).sum().backward()
+    rel = []
+    for d in range(3):
+        k = torch.arange(-(N[d] // 2), (N[d] - 1) // 2 + 1, device=dev, dtype=torch.float32)
+        shape = [1, 1, 1]
+        shape[2 - d] = N[d]
+        t2 = nb.nufft3d2(*[x.detach() for x in x32], (-1j * k.reshape(shape)) * G, eps=1e-6, isign=-1)
+        ref = (c64.detach().conj() * t2).real
+        rel.append(float((x32[d].grad - ref).norm() / ref.norm()))
+    dc_ref = nb.nufft3d2(*[x.detach() for x in x32], G, eps=1e-6, isign=-1)
+    out["spectral_formula_rel_l2_dx_dy_dz"] = rel
+    out["spectral_formula_rel_l2_dc"] = float((c64.grad - dc_ref).norm() / dc_ref.norm())
+    return out
+
+
+def served_requests(n, seed=5):
+    """The served mix: 50 % 2D type 1/2 (modes per axis from 128..512 in steps of
+    32, M log-uniform 1e3..4e6), 30 % 3D type 1/2 (modes per axis from 64..160 in
+    steps of 16, M log-uniform 1e4..8e6),
+    20 % 2D type 3 (sources uniform in [-pi, pi)^2, targets uniform in
+    [-300, 300]^2, M = K log-uniform 1e3..1e6); eps 1e-6, complex64.  Inputs are
+    generated on the device at admission from a per-request seed."""
+    import torch
+
+    from nufftax_b200 import compute_type3_grid_sizes_2d
+    from nufftax_b200.serve import Request
+
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for i in range(n):
+        u = rng.random()
+        kind = int(rng.integers(1, 3))
+        if u < 0.5:
+            dim = 2
+            M = int(np.exp(rng.uniform(np.log(1e3), np.log(4e6))))
+            nm = tuple(int(rng.choice(np.arange(128, 513, 32))) for _ in range(2))
+        elif u < 0.8:
+            dim = 3
+            M = int(np.exp(rng.uniform(np.log(1e4), np.log(8e6))))
+            nm = tuple(int(rng.choice(np.arange(64, 161, 16))) for _ in range(3))
+        else:
+            dim, kind = 2, 3
+            M = int(np.exp(rng.uniform(np.log(1e3), np.log(1e6))))
+            nm = compute_type3_grid_sizes_2d(np.pi, np.pi, 300.0, 300.0, eps=1e-6)
+
+        def make(device, kind=kind, dim=dim, M=M, nm=nm, sd=int(rng.integers(1 << 31))):
+            g = torch.Generator(device=device)
+            g.manual_seed(sd)
+            X = [(torch.rand(M, device=device, generator=g) * 2 - 1) * np.pi for _ in range(dim)]
+            if kind == 2:
+                shape = tuple(reversed(nm))
+                f = torch.complex(torch.randn(shape, device=device, generator=g),
+                                  torch.randn(shape, device=device, generator=g))
+                return X, f, None
+            c = torch.complex(torch.randn(M, device=device, generator=g), torch.randn(M, device=device, generator=g))
+            T = [(torch.rand(M, device=device, generator=g) * 2 - 1) * 300.0 for _ in range(dim)] if kind == 3 else None
+            return X, c, T
+
+        reqs.append(Request(kind=kind, dim=dim, n_modes=nm, M=M, K=M if kind == 3 else 0, make_inputs=make))
+    return reqs
+
+
+def run_serve(args):
+    """Served stream vs one-at-a-time plain execution; Poisson arrivals."""
+    import copy
+
+    import torch
+
+    import nufftax_b200 as nb
+    from nufftax_b200.serve import NufftServer
+
+    dev = torch.device("cuda", 0)
+    n = args.requests
+    reqs = served_requests(n)
+    # both paths start with warm cuFFT plans: one small transform per distinct shape
+    shapes = sorted({(r.kind, r.dim, tuple(r.n_modes)) for r in reqs})
+    for kind, dim, nm in shapes:
+        g = torch.Generator(device=dev)
+        X = [torch.rand(64, device=dev, generator=g) for _ in range(dim)]
+        if kind == 3:
+            c = torch.ones(64, dtype=torch.complex64, device=dev)
+            nb.nufft2d3(*X, c, *[x * 300 for x in X], nm)
+        elif kind == 1:
+            {2: nb.nufft2d1, 3: nb.nufft3d1}[dim](*X, torch.ones(64, dtype=torch.complex64, device=dev), nm)
+        else:
+            {2: nb.nufft2d2, 3: nb.nufft3d2}[dim](*X, torch.ones(tuple(reversed(nm)), dtype=torch.complex64,
+                                                                device=dev))
+    torch.cuda.synchronize()
+    # one-at-a-time: each request alone through the public API, synchronised
+    sample = [copy.copy(r) for r in reqs[: min(n, args.plain_sample)]]
+    for r in sample[:5]:
+        _plain(nb, r, dev)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for r in sample:
+        _plain(nb, r, dev)
+        torch.cuda.synchronize()
+    plain_s = time.perf_counter() - t0
+    plain_pts = sum(r.points() for r in sample) / plain_s
+    plain_rps = len(sample) / plain_s
+    out = {"metric": "served mixed stream NU points/s (p50/p99 latency)", "unit": "NU points/s",
+           "requests": n, "distinct_shapes": len(shapes),
+           "one_at_a_time": {"points_per_s": plain_pts, "requests_per_s": plain_rps,
+                                            "sample": len(sample)}, "loads": []}
+    rng = np.random.default_rng(11)
+    for load in args.loads:
+        rate = load * plain_rps
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, n))
+        server = NufftServer(dev, slots=args.slots, hbm_budget=150e9, keep_results=False)
+        batch = [copy.copy(r) for r in reqs]
+        # warm the caches (plans, grid pool) with the first few requests
+        server.serve([copy.copy(r) for r in reqs[:20]])
+        torch.cuda.synchronize()
+        server.completed = []
+        done = server.serve(batch, list(arrivals))
+        st = server.stats(done)
+        st["offered_load"] = load
+        st["offered_requests_per_s"] = rate
+        out["loads"].append(st)
+    best = max(out["loads"], key=lambda d: d["points_per_s"])
+    out["value"] = best["points_per_s"]
+    out["p50_ms"] = best["p50_ms"]
+    out["p99_ms"] = best["p99_ms"]
+    out["speedup_vs_one_at_a_time"] = best["points_per_s"] / plain_pts
+    print(json.dumps(out), flush=True)
+
+
+def _plain(nb, r, dev):
+    X, s, T = r.make_inputs(dev)
+    if r.kind == 1:
+        fn = {2: nb.nufft2d1, 3: nb.nufft3d1}[r.dim]
+        return fn(*X, s, r.n_modes, eps=r.eps)
+    if r.kind == 2:
+        fn = {2: nb.nufft2d2, 3: nb.nufft3d2}[r.dim]
+        return fn(*X, s, eps=r.eps)
+    return nb.nufft2d3(*X, s, *T, r.n_modes, eps=r.eps)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -523,11 +767,22 @@ def main():
     ap.add_argument("--case", choices=["radial", "clustered"], help="profile one point set only (no timing)")
     ap.add_argument("--reps", type=int, default=2)
     ap.add_argument("--scale", type=float, default=1.0)
-    ap.add_argument("--config", choices=["default", "batched"], default="default")
+    ap.add_argument("--config", choices=["default", "batched", "grad3d", "serve"], default="default")
+    ap.add_argument("--requests", type=int, default=10000)
+    ap.add_argument("--plain-sample", type=int, default=1000)
+    ap.add_argument("--slots", type=int, default=8)
+    ap.add_argument("--loads", type=float, nargs="+", default=[1.0, 2.0])
     ap.add_argument("--autotune", action="store_true")
+    ap.add_argument("--check", action="store_true")
     args = ap.parse_args()
     if args.config == "batched":
         run_batched(args)
+        return
+    if args.config == "grad3d":
+        run_grad3d(args)
+        return
+    if args.config == "serve":
+        run_serve(args)
         return
     if args.case:
         run_case(args)

@@ -145,6 +145,9 @@ int nfx_deconv_pad(int precision, int dim, const int nf[3], const int n_modes[3]
  * nufft2.py:317,383,454-457. */
 int nfx_fft(int precision, int dim, const int nf[3], int n_trans, void* data, int sign, void* stream);
 int nfx_fft_cache_clear(void);
+/* Bound the plan cache (default 1024 plans); the least recently used plan is
+ * destroyed, after a device synchronisation, when a new one needs room. */
+int nfx_fft_cache_limit(int max_plans);
 
 /* ---- batching: many problems in one launch --------------------------------
  * No counterpart in the reference (nufftax vmaps one problem's strengths).

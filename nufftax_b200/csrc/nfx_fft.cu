@@ -1,10 +1,11 @@
-// cuFFT glue: a mutex-guarded cache of batched in-place C2C/Z2Z plans keyed by
-// (device, precision, dims, batch).  Replaces the jnp.fft calls of
+// cuFFT glue: a mutex-guarded, size-limited (least recently used out) cache of
+// batched in-place C2C/Z2Z plans keyed by (device, precision, dims, batch).  Replaces the jnp.fft calls of
 // nufftax/transforms/nufft1.py:81,154,232-235 and nufft2.py:317,383,454-457:
 // sign = +1 is the unnormalised inverse transform (nufftax's ifftn(.) * prod(nf)),
 // sign = -1 the forward transform.
 #include <cufft.h>
 
+#include <cstdint>
 #include <map>
 #include <mutex>
 #include <string>
@@ -18,9 +19,28 @@ namespace nfx {
 namespace {
 using PlanKey = std::tuple<int, int, int, int, int, int, int>;  // dev, prec, dim, nf1, nf2, nf3, batch
 std::mutex g_plan_mu;
-std::map<PlanKey, cufftHandle>& plans() {
-  static std::map<PlanKey, cufftHandle> m;
+struct PlanEntry {
+  cufftHandle plan;
+  uint64_t last_use;
+};
+std::map<PlanKey, PlanEntry>& plans() {
+  static std::map<PlanKey, PlanEntry> m;
   return m;
+}
+uint64_t g_tick = 0;
+size_t g_plan_limit = 1024;
+
+// Keep at most g_plan_limit plans; the least recently used one is destroyed
+// after the device is idle (an in-flight transform may still use its work area).
+void evict_if_full() {
+  while (plans().size() >= g_plan_limit && !plans().empty()) {
+    auto victim = plans().begin();
+    for (auto it = plans().begin(); it != plans().end(); ++it)
+      if (it->second.last_use < victim->second.last_use) victim = it;
+    cudaDeviceSynchronize();
+    cufftDestroy(victim->second.plan);
+    plans().erase(victim);
+  }
 }
 
 int cufft_fail(cufftResult r, const char* where) {
@@ -58,12 +78,14 @@ int nfx_fft(int precision, int dim, const int nf[3], int n_trans, void* data, in
   cufftHandle plan;
   auto it = plans().find(key);
   if (it == plans().end()) {
+    evict_if_full();
     cufftResult r = cufftPlanMany(&plan, dim, n, nullptr, 1, (int)dist, nullptr, 1, (int)dist,
                                   precision == NFX_F32 ? CUFFT_C2C : CUFFT_Z2Z, n_trans);
     if (r != CUFFT_SUCCESS) return cufft_fail(r, "cufftPlanMany");
-    plans()[key] = plan;
+    plans()[key] = PlanEntry{plan, ++g_tick};
   } else {
-    plan = it->second;
+    plan = it->second.plan;
+    it->second.last_use = ++g_tick;
   }
   cufftResult r = cufftSetStream(plan, (cudaStream_t)stream);
   if (r != CUFFT_SUCCESS) return cufft_fail(r, "cufftSetStream");
@@ -78,8 +100,19 @@ int nfx_fft(int precision, int dim, const int nf[3], int n_trans, void* data, in
 
 int nfx_fft_cache_clear(void) {
   std::lock_guard<std::mutex> lk(g_plan_mu);
-  for (auto& kv : plans()) cufftDestroy(kv.second);
+  if (!plans().empty()) cudaDeviceSynchronize();
+  for (auto& kv : plans()) cufftDestroy(kv.second.plan);
   plans().clear();
+  return NFX_OK;
+}
+
+int nfx_fft_cache_limit(int max_plans) {
+  if (max_plans < 1) {
+    set_error("nfx_fft_cache_limit: need at least one plan");
+    return NFX_ERR_INVALID;
+  }
+  std::lock_guard<std::mutex> lk(g_plan_mu);
+  g_plan_limit = (size_t)max_plans;
   return NFX_OK;
 }
 

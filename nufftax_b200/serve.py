@@ -1,0 +1,260 @@
+"""Continuous-batching NUFFT server.
+
+Requests (type 1, 2 or 3; 1D/2D/3D; any size) arrive at any time.  The server
+admits a pending request as soon as a stream slot is free and its device-memory
+estimate fits the HBM budget (looking past a head request that does not fit, so
+small requests are not blocked behind a large one).  Every admitted request runs
+on its own CUDA stream, so requests that arrive while others are on the GPU
+overlap with them on the device; completion is detected with CUDA events and
+releases the slot and the memory.  Between requests the server keeps on the
+device: cuFFT plans (library cache), fine-grid buffers (a pool per shape, reused
+across requests) and sorted point sets (kept under a caller-chosen `points_id`
+and reused by later requests on the same points, ordered after the sort that
+produced them by an event).  Latency is measured from arrival to the host seeing
+the completion event; `stats()` gives p50/p99 and throughput.
+"""
+
+from __future__ import annotations
+
+import collections
+import dataclasses
+import math
+import threading
+import time
+from typing import Callable, Optional, Sequence
+
+import numpy as np
+import torch
+
+from ._plan import PointSort, deconv_pad, deconv_shuffle, fft_inplace, precision_of
+from .grid import compute_grid_size
+from .kernel import compute_kernel_params
+from .transforms import _fft_sign_type1, _fft_sign_type2, _type3_forward
+
+
+@dataclasses.dataclass
+class Request:
+    """One transform.  kind: 1, 2 or 3.  For types 1/2 `n_modes` are the modes
+    per axis; for type 3 `n_modes` is the type-3 grid (compute_type3_grid_size*).
+    Inputs are device tensors, or `make_inputs(device, stream)` builds them at
+    admission (returning the same fields)."""
+
+    kind: int
+    dim: int
+    n_modes: tuple
+    M: int
+    K: int = 0
+    coords: Optional[Sequence[torch.Tensor]] = None
+    strengths: Optional[torch.Tensor] = None  # type 1/3: c (M,); type 2: f (modes)
+    targets: Optional[Sequence[torch.Tensor]] = None  # type 3
+    make_inputs: Optional[Callable] = None
+    isign: Optional[int] = None
+    eps: float = 1e-6
+    points_id: Optional[object] = None
+    arrival: float = 0.0
+    # filled by the server
+    result: Optional[torch.Tensor] = None
+    admitted: float = 0.0
+    finished: float = 0.0
+    nbytes: int = 0
+
+    def points(self) -> int:
+        return self.M if self.kind != 3 else self.M + self.K
+
+
+def estimate_bytes(req: Request) -> int:
+    """Device bytes a request holds while in flight (inputs, outputs, sort
+    workspace, fine grid(s) and cuFFT work area), complex64."""
+    kp = compute_kernel_params(req.eps)
+    pts = req.M
+    inputs = pts * (4 * req.dim + 8)
+    sort_ws = pts * 22 + 4 * 1024 * 1024
+    if req.kind == 3:
+        nf = [compute_grid_size(n, 2.0, kp.nspread) for n in req.n_modes]
+        grid = 8 * math.prod(req.n_modes) + 2 * 8 * math.prod(nf)
+        out = req.K * (8 + 4 * req.dim) * 2
+        sort_ws += req.K * 22
+    else:
+        nf = [compute_grid_size(n, 2.0, kp.nspread) for n in req.n_modes]
+        grid = 2 * 8 * math.prod(nf)
+        out = 8 * max(pts, math.prod(req.n_modes))
+    return int(inputs + sort_ws + grid + out)
+
+
+class _Slot:
+    def __init__(self, device):
+        self.stream = torch.cuda.Stream(device=device)
+        self.req: Optional[Request] = None
+        self.done = torch.cuda.Event()
+        self.grids: list = []
+
+
+class NufftServer:
+    """slots: concurrent requests (one CUDA stream each); hbm_budget: bytes of
+    in-flight requests; keep_results=False drops each result once it is complete
+    (throughput runs); pool_fraction of the budget may stay resident as pooled
+    fine grids (least recently used shapes are dropped beyond it)."""
+
+    def __init__(self, device=None, slots: int = 8, hbm_budget: float = 150e9, lookahead: int = 16,
+                 keep_points: int = 64, keep_results: bool = True, pool_fraction: float = 0.1):
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.slots = [_Slot(self.device) for _ in range(slots)]
+        self.budget = int(hbm_budget)
+        self.in_use = 0
+        self.lookahead = lookahead
+        self.pending: collections.deque[Request] = collections.deque()
+        self.completed: list[Request] = []
+        self.grid_pool: "collections.OrderedDict[tuple, list[torch.Tensor]]" = collections.OrderedDict()
+        self.pool_bytes = 0
+        self.pool_cap = int(pool_fraction * hbm_budget)
+        self.keep_results = keep_results
+        self.points_cache: "collections.OrderedDict[object, tuple[PointSort, torch.cuda.Event]]" = \
+            collections.OrderedDict()
+        self.keep_points = keep_points
+        self.lock = threading.Lock()
+
+    # -- resident state -----------------------------------------------------------
+    def _grid(self, shape, dtype, slot: _Slot) -> torch.Tensor:
+        pool = self.grid_pool.get((shape, dtype))
+        if pool:
+            g = pool.pop()
+            self.pool_bytes -= g.numel() * g.element_size()
+        else:
+            g = torch.empty(shape, dtype=dtype, device=self.device)
+        slot.grids.append(((shape, dtype), g))
+        return g
+
+    def _return_grid(self, key, g):
+        self.grid_pool.setdefault(key, []).append(g)
+        self.grid_pool.move_to_end(key)
+        self.pool_bytes += g.numel() * g.element_size()
+        while self.pool_bytes > self.pool_cap and self.grid_pool:
+            k, lst = next(iter(self.grid_pool.items()))
+            while lst and self.pool_bytes > self.pool_cap:
+                old = lst.pop()
+                self.pool_bytes -= old.numel() * old.element_size()
+            if not lst:
+                del self.grid_pool[k]
+
+    def _sorted(self, req: Request, coords, nf, kp, slot: _Slot) -> PointSort:
+        key = (req.points_id, tuple(nf), kp.nspread) if req.points_id is not None else None
+        if key is not None and key in self.points_cache:
+            ps, ev = self.points_cache[key]
+            self.points_cache.move_to_end(key)
+            slot.stream.wait_event(ev)
+            return ps
+        ps = PointSort(list(coords), nf, kp, prenorm=True)
+        if key is not None:
+            ev = torch.cuda.Event()
+            ev.record(slot.stream)
+            self.points_cache[key] = (ps, ev)
+            while len(self.points_cache) > self.keep_points:
+                self.points_cache.popitem(last=False)
+        return ps
+
+    # -- execution ------------------------------------------------------------------
+    def _run(self, req: Request, slot: _Slot):
+        with torch.cuda.device(self.device), torch.cuda.stream(slot.stream):
+            if req.make_inputs is not None:
+                req.coords, req.strengths, req.targets = req.make_inputs(self.device)
+            kp = compute_kernel_params(req.eps)
+            if req.kind == 1:
+                isign = 1 if req.isign is None else req.isign
+                nf = tuple(compute_grid_size(n, 2.0, kp.nspread) for n in req.n_modes)
+                ps = self._sorted(req, req.coords, nf, kp, slot)
+                fw = self._grid((1,) + nf[::-1], req.strengths.dtype, slot)
+                ps.spread(req.strengths.reshape(1, -1), out=fw)
+                fft_inplace(fw, req.dim, _fft_sign_type1(isign))
+                req.result = deconv_shuffle(fw, req.n_modes, kp)[0]
+            elif req.kind == 2:
+                isign = -1 if req.isign is None else req.isign
+                nf = tuple(compute_grid_size(n, 2.0, kp.nspread) for n in req.n_modes)
+                fw = self._grid((1,) + nf[::-1], req.strengths.dtype, slot)
+                deconv_pad(req.strengths.reshape((1,) + req.strengths.shape), nf, kp, out=fw)
+                fft_inplace(fw, req.dim, _fft_sign_type2(isign))
+                ps = self._sorted(req, req.coords, nf, kp, slot)
+                req.result = ps.interp(fw)[0]
+            else:
+                isign = 1 if req.isign is None else req.isign
+                req.result = _type3_forward(list(req.coords), req.strengths.reshape(1, -1), list(req.targets),
+                                            tuple(req.n_modes), req.eps, isign, 2.0)[0]
+            slot.done.record(slot.stream)
+
+    def submit(self, req: Request):
+        if req.arrival == 0.0:
+            req.arrival = time.perf_counter()
+        req.nbytes = estimate_bytes(req)
+        with self.lock:
+            self.pending.append(req)
+
+    def _admit(self):
+        free = [s for s in self.slots if s.req is None]
+        if not free:
+            return
+        with self.lock:
+            i = 0
+            while free and i < min(self.lookahead, len(self.pending)):
+                req = self.pending[i]
+                if self.in_use + req.nbytes <= self.budget or (self.in_use == 0):
+                    del self.pending[i]
+                    slot = free.pop()
+                    slot.req = req
+                    self.in_use += req.nbytes
+                    req.admitted = time.perf_counter()
+                    self._run(req, slot)
+                else:
+                    i += 1
+
+    def _poll(self):
+        for s in self.slots:
+            if s.req is not None and s.done.query():
+                req = s.req
+                req.finished = time.perf_counter()
+                self.in_use -= req.nbytes
+                for key, g in s.grids:
+                    self._return_grid(key, g)
+                s.grids = []
+                s.req = None
+                if req.make_inputs is not None:  # inputs were generated here: release them
+                    req.coords = req.strengths = req.targets = None
+                if not self.keep_results:
+                    req.result = None
+                self.completed.append(req)
+
+    def busy(self) -> bool:
+        return bool(self.pending) or any(s.req is not None for s in self.slots)
+
+    def step(self):
+        self._poll()
+        self._admit()
+
+    def serve(self, requests: Sequence[Request], arrivals: Sequence[float] | None = None, idle_sleep: float = 2e-5):
+        """Feed requests at their arrival offsets (seconds from now) and run
+        until all complete.  Returns the completed requests."""
+        t0 = time.perf_counter()
+        arrivals = arrivals if arrivals is not None else [0.0] * len(requests)
+        order = sorted(range(len(requests)), key=lambda i: arrivals[i])
+        nxt = 0
+        while nxt < len(order) or self.busy():
+            now = time.perf_counter()
+            while nxt < len(order) and t0 + arrivals[order[nxt]] <= now:
+                r = requests[order[nxt]]
+                r.arrival = t0 + arrivals[order[nxt]]
+                self.submit(r)
+                nxt += 1
+            self.step()
+            if nxt < len(order) and not self.pending:
+                wait = t0 + arrivals[order[nxt]] - time.perf_counter()
+                if wait > 0:
+                    time.sleep(min(wait, 1e-3))
+            elif self.busy():
+                time.sleep(idle_sleep)
+        return self.completed
+
+    def stats(self, reqs: Sequence[Request] | None = None) -> dict:
+        reqs = list(reqs if reqs is not None else self.completed)
+        lat = np.array([r.finished - r.arrival for r in reqs]) * 1e3
+        pts = sum(r.points() for r in reqs)
+        span = max(r.finished for r in reqs) - min(r.arrival for r in reqs)
+        return {"requests": len(reqs), "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                "mean_ms": float(lat.mean()), "points": int(pts), "points_per_s": pts / span, "span_s": span}
