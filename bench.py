@@ -9,10 +9,13 @@ Workload (one step = one type-1 and one type-2 transform of each point set):
 Metric: NU points per second, counting M once per transform (2 * (Ma + Mb) per step).
 
 `value` times the steps with inputs resident in HBM (CUDA events, L2 flushed
-between steps by writing a 256 MB buffer outside the timed events).  `e2e` times
+between steps by writing a 256 MB buffer outside the timed events); the two
+point sets of a step run on two CUDA streams, so their work overlaps.  `e2e` times
 the same steps through the public API with pinned host buffers: host->device
 copies of x, y, c, f and device->host copies of the results are inside the
-timed region.  `--impl reference` times the CPU restatement of nufftax's
+timed region; uploads, compute and downloads run on separate streams so they
+overlap (the type 2 runs first, its result downloads while c uploads).
+`--impl reference` times the CPU restatement of nufftax's
 pure-JAX path (oracle/) on all host cores on a bounded sample.
 Multi-GPU runs are independent replicas (weak scaling), timed as the max over ranks.
 """
@@ -190,13 +193,22 @@ def run_gpu(args):
     kp = nb.compute_kernel_params(EPS)
     nf = tuple(nb.compute_grid_size(n, 2.0, kp.nspread) for n in N_MODES)
 
+    # Each point set runs on its own stream, so one set's work overlaps the
+    # other's; the step is the union (forked from and joined to the main stream).
+    main = torch.cuda.current_stream(dev)
+    set_streams = [torch.cuda.Stream(dev) for _ in sets]
+
     def step(ds):
         nb.sort_cache.clear()
         outs = []
-        for s in ds:
-            f1 = nb.nufft2d1(s["x"], s["y"], s["c"], N_MODES, eps=EPS)
-            c2 = nb.nufft2d2(s["x"], s["y"], s["f"], eps=EPS)
+        for s, st in zip(ds, set_streams):
+            st.wait_stream(main)
+            with torch.cuda.stream(st):
+                f1 = nb.nufft2d1(s["x"], s["y"], s["c"], N_MODES, eps=EPS)
+                c2 = nb.nufft2d2(s["x"], s["y"], s["f"], eps=EPS)
             outs.append((f1, c2))
+        for st in set_streams:
+            main.wait_stream(st)
         return outs
 
     # The clock sampler (200 ms period) runs from the warm-up through the timed
@@ -256,17 +268,51 @@ def run_gpu(args):
     h2d = sum(h[k].numel() * h[k].element_size() for h in host for k in ("x", "y", "c", "f"))
     d2h = sum(a.numel() * a.element_size() + b.numel() * b.element_size() for a, b in out_host)
 
+    # Per point set: an upload stream, the compute stream and a download stream.
+    # The type 2 goes first (it needs x, y, f), its result downloads while c
+    # uploads (PCIe is full duplex), then the type 1 reuses the sorted points.
+    up_streams = [torch.cuda.Stream(dev) for _ in sets]
+    down_streams = [torch.cuda.Stream(dev) for _ in sets]
+
     def e2e_step():
         nb.sort_cache.clear()
-        for h, (fo, co) in zip(host, out_host):
-            x = h["x"].to(dev, non_blocking=True)
-            y = h["y"].to(dev, non_blocking=True)
-            c = h["c"].to(dev, non_blocking=True)
-            f = h["f"].to(dev, non_blocking=True)
-            f1 = nb.nufft2d1(x, y, c, N_MODES, eps=EPS)
-            c2 = nb.nufft2d2(x, y, f, eps=EPS)
-            fo.copy_(f1, non_blocking=True)
-            co.copy_(c2, non_blocking=True)
+        live = []
+        for h, (fo, co), st, up, down in zip(host, out_host, set_streams, up_streams, down_streams):
+            for s_ in (st, up, down):
+                s_.wait_stream(main)
+            with torch.cuda.stream(up):
+                x = h["x"].to(dev, non_blocking=True)
+                y = h["y"].to(dev, non_blocking=True)
+                f = h["f"].to(dev, non_blocking=True)
+                xyf = torch.cuda.Event()
+                xyf.record(up)
+                c = h["c"].to(dev, non_blocking=True)
+                cin = torch.cuda.Event()
+                cin.record(up)
+            for t in (x, y, f, c):
+                t.record_stream(st)
+            st.wait_event(xyf)
+            with torch.cuda.stream(st):
+                c2 = nb.nufft2d2(x, y, f, eps=EPS)
+                t2done = torch.cuda.Event()
+                t2done.record(st)
+            down.wait_event(t2done)
+            with torch.cuda.stream(down):
+                co.copy_(c2, non_blocking=True)
+            c2.record_stream(down)
+            st.wait_event(cin)
+            with torch.cuda.stream(st):
+                f1 = nb.nufft2d1(x, y, c, N_MODES, eps=EPS)
+                t1done = torch.cuda.Event()
+                t1done.record(st)
+            down.wait_event(t1done)
+            with torch.cuda.stream(down):
+                fo.copy_(f1, non_blocking=True)
+            f1.record_stream(down)
+            live.append((x, y, f, c, c2, f1))
+        for s_ in set_streams + up_streams + down_streams:
+            main.wait_stream(s_)
+        return live
 
     for _ in range(max(1, args.warmup)):
         e2e_step()

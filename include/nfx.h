@@ -61,6 +61,15 @@ int nfx_version(void);
 const char* nfx_last_error(void);
 int nfx_num_sms(void);
 
+/* Polynomial form of the ES weights used by the float kernels (no counterpart
+ * in the reference, which evaluates exp/sqrt): coefficients a[q][d] of
+ * phi(q - (v + ns - 1) / 2) as a degree-`degree` polynomial in v in [-1, 1],
+ * written to coeffs[q * 16 + d]; max_abs_err is the worst float Horner error
+ * against the exp/sqrt form.  A fit is used when that error stays within
+ * 3e-8 + 2.4e-7 |phi| (two float ulps); degree 0 means none was found and the
+ * kernels evaluate exp/sqrt. */
+int nfx_es_poly(int nspread, double beta, double kc, float* coeffs, int* degree, double* max_abs_err);
+
 /* Fill tile[] / max_subproblem with the defaults the library would use. */
 int nfx_default_tiles(nfx_opts* opts);
 

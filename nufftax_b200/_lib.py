@@ -80,6 +80,7 @@ _SIGNATURES = {
     "nfx_version": ([], c_int),
     "nfx_last_error": ([], ctypes.c_char_p),
     "nfx_num_sms": ([], c_int),
+    "nfx_es_poly": ([c_int, c_double, c_double, POINTER(ctypes.c_float), POINTER(c_int), POINTER(c_double)], c_int),
     "nfx_default_tiles": ([POINTER(NfxOpts)], c_int),
     "nfx_sort_workspace_bytes": ([POINTER(NfxOpts), c_int64, POINTER(c_size_t)], c_int),
     "nfx_sort_points": ([POINTER(NfxOpts), _vp, _vp, _vp, c_int64, _vp, c_size_t, _vp], c_int),

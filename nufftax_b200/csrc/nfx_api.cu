@@ -1,5 +1,7 @@
 // extern "C" entry points of libnfx_b200 (declared in include/nfx.h).
 #include <algorithm>
+#include <cmath>
+#include <type_traits>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -358,10 +360,98 @@ static int prepare(const nfx_opts* in, int64_t M, const void* x, const void* y, 
   return NFX_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Polynomial ES weights (float path): for each q, Chebyshev interpolation of
+// v -> phi(q - (v + ns - 1) / 2) on [-1, 1] at D + 1 nodes, converted to
+// monomials in v; the degree is raised until Horner's rule in float (fmaf, as on
+// the device) is within kPolyAbs + kPolyRel * |phi| of the double exp/sqrt value
+// on a fine grid: two float ulps of the weight plus a small absolute floor (the
+// exp/sqrt form in float carries errors of the same size).
+// ---------------------------------------------------------------------------
+constexpr double kPolyAbs = 3e-8;
+constexpr double kPolyRel = 2.4e-7;
+
+static double es_phi(double z, double beta, double kc) {
+  const double arg = 1.0 - kc * z * z;
+  return arg >= 0.0 ? std::exp(beta * (std::sqrt(arg > 0.0 ? arg : 0.0) - 1.0)) : 0.0;
+}
+
+static bool fit_es_poly_uncached(int ns, double beta, double kc, EsPoly& out, double& err_out) {
+  for (int D = 4; D <= kPolyMaxDeg; ++D) {
+    double worst = 0.0, worst_ratio = 0.0;
+    EsPoly P;
+    P.deg = D;
+    for (int q = 0; q < ns; ++q) {
+      const int n = D + 1;
+      double cheb[kPolyMaxDeg + 1] = {0};
+      for (int j = 0; j < n; ++j) {
+        double acc = 0.0;
+        for (int k = 0; k < n; ++k) {
+          const double th = kPi * (k + 0.5) / n;
+          const double v = std::cos(th);
+          acc += es_phi(q - (v + ns - 1) / 2.0, beta, kc) * std::cos(j * th);
+        }
+        cheb[j] = (j == 0 ? 1.0 : 2.0) * acc / n;
+      }
+      // Chebyshev -> monomial: T_{j+1} = 2 v T_j - T_{j-1}
+      double Tm[kPolyMaxDeg + 2][kPolyMaxDeg + 2] = {{0}};
+      Tm[0][0] = 1.0;
+      if (D >= 1) Tm[1][1] = 1.0;
+      for (int j = 1; j < D; ++j)
+        for (int i = 0; i <= j + 1; ++i) Tm[j + 1][i] = (i > 0 ? 2.0 * Tm[j][i - 1] : 0.0) - Tm[j - 1][i];
+      double mono[kPolyMaxDeg + 1] = {0};
+      for (int j = 0; j <= D; ++j)
+        for (int i = 0; i <= j; ++i) mono[i] += cheb[j] * Tm[j][i];
+      for (int i = 0; i <= D; ++i) P.a[q][i] = (float)mono[i];
+      for (int t = 0; t <= 2000; ++t) {
+        const double v = -1.0 + 2.0 * t / 2000.0;
+        float h = P.a[q][D];
+        for (int d = D - 1; d >= 0; --d) h = std::fmaf(h, (float)v, P.a[q][d]);
+        const double ref = es_phi(q - (v + ns - 1) / 2.0, beta, kc);
+        const double e = std::fabs((double)h - ref);
+        const double ratio = e / (kPolyAbs + kPolyRel * std::fabs(ref));
+        worst = e > worst ? e : worst;
+        worst_ratio = ratio > worst_ratio ? ratio : worst_ratio;
+      }
+    }
+    if (worst_ratio <= 1.0) {
+      out = P;
+      err_out = worst;
+      return true;
+    }
+  }
+  return false;
+}
+
+static bool es_poly(int ns, double beta, double kc, EsPoly& out, double* err = nullptr) {
+  static std::mutex mu;
+  static std::map<std::tuple<int, double, double>, std::pair<EsPoly, double>> cache;
+  std::lock_guard<std::mutex> lk(mu);
+  auto key = std::make_tuple(ns, beta, kc);
+  auto it = cache.find(key);
+  if (it == cache.end()) {
+    EsPoly P;
+    P.deg = 0;
+    double e = -1.0;
+    if (!fit_es_poly_uncached(ns, beta, kc, P, e)) P.deg = 0;
+    it = cache.emplace(key, std::make_pair(P, e)).first;
+  }
+  out = it->second.first;
+  if (err) *err = it->second.second;
+  return out.deg > 0;
+}
+
+template <typename T>
+static void attach_poly(PointArgs<T>& a, int ns, double beta, double kc) {
+  a.poly.deg = 0;
+  if (std::is_same<T, float>::value) es_poly(ns, beta, kc, a.poly);
+}
+
 template <typename T>
 static cudaError_t spread_dim(const Prepared& P, const void* x, const void* y, const void* z, int64_t M, const void* c,
                               int n_trans, void* fw, const void* ws, cudaStream_t st) {
   PointArgs<T> a = make_args<T>(P.g, P.o.beta, P.o.kc, x, y, z, M, n_trans, view(P.L, ws));
+  attach_poly(a, P.o.nspread, P.o.beta, P.o.kc);
   switch (P.o.dim) {
     case 1:
       return dispatch_spread<T, 1>(P.o.nspread, a, c, fw, st);
@@ -376,6 +466,7 @@ template <typename T>
 static cudaError_t interp_dim(const Prepared& P, const void* x, const void* y, const void* z, int64_t M,
                               const void* fw, int n_trans, void* out, const void* ws, cudaStream_t st) {
   PointArgs<T> a = make_args<T>(P.g, P.o.beta, P.o.kc, x, y, z, M, n_trans, view(P.L, ws));
+  attach_poly(a, P.o.nspread, P.o.beta, P.o.kc);
   switch (P.o.dim) {
     case 1:
       return dispatch_interp<T, 1>(P.o.nspread, a, fw, out, st);
@@ -439,6 +530,22 @@ using namespace nfx;
 extern "C" {
 
 int nfx_version(void) { return 10000; }
+
+int nfx_es_poly(int nspread, double beta, double kc, float* coeffs, int* degree, double* max_abs_err) {
+  if (nspread < 2 || nspread > 16 || degree == nullptr) {
+    set_error("nfx_es_poly: invalid arguments");
+    return NFX_ERR_INVALID;
+  }
+  EsPoly P;
+  double err = -1.0;
+  es_poly(nspread, beta, kc, P, &err);
+  *degree = P.deg;
+  if (max_abs_err) *max_abs_err = err;
+  if (coeffs && P.deg > 0)
+    for (int q = 0; q < nspread; ++q)
+      for (int d = 0; d <= P.deg; ++d) coeffs[q * (kPolyMaxDeg + 1) + d] = P.a[q][d];
+  return NFX_OK;
+}
 const char* nfx_last_error(void) { return g_last_error.c_str(); }
 int nfx_num_sms(void) { return num_sms(); }
 
@@ -686,6 +793,7 @@ int nfx_batch_upload(const nfx_opts* common, int spread, const nfx_batch_problem
       BatchItem<float>* it = (BatchItem<float>*)host.data() + p;
       it->a = make_args<float>(P.g, P.o.beta, P.o.kc, probs[p].x, probs[p].y, probs[p].z, probs[p].M, 1,
                                view(P.L, probs[p].workspace));
+      attach_poly(it->a, P.o.nspread, P.o.beta, P.o.kc);
       it->src = probs[p].src;
       it->dst = probs[p].dst;
     } else {

@@ -109,6 +109,17 @@ __device__ __forceinline__ void red_add(double2* addr, double2 v) {
   atomicAdd(&addr->y, v.y);
 }
 
+// Polynomial form of the ES weights of one footprint (float path).  For a point
+// at scaled coordinate xs with left cell i0, every weight phi(i0 + q - xs),
+// q = 0..ns-1, is a smooth function of v = 2 (xs - i0) - (ns - 1) in (-1, 1];
+// a[q][d] are monomial coefficients in v fitted on the host (nfx_es_poly) to
+// within two float ulps of the exp/sqrt form, evaluated by Horner's rule.
+constexpr int kPolyMaxDeg = 15;
+struct EsPoly {
+  float a[16][kPolyMaxDeg + 1];
+  int deg;  // 0 = not used (exp/sqrt form)
+};
+
 // Grid geometry shared by the sort, spread and interp kernels (plain values).
 struct Geom {
   int dim;

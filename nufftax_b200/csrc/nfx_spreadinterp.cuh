@@ -21,6 +21,8 @@
 //    interpolated value and all coordinate gradients in one pass.
 #pragma once
 
+#include <type_traits>
+
 #include "nfx_internal.h"
 
 namespace nfx {
@@ -45,7 +47,28 @@ struct PointArgs {
   Geom g;
   T beta, kc;
   SortView s;
+  EsPoly poly;
 };
+
+// The NS weights of one axis: w[q] = phi(i0 + q - xs).  float with a fitted
+// polynomial: Horner in v = 2 (xs - i0) - (NS - 1) (exact in float: xs - i0 is
+// exact because xs and i0 are within NS of each other and i0 is an integer);
+// otherwise exp/sqrt (nufftax/core/kernel.py:79-111).
+template <typename T, int NS>
+__device__ __forceinline__ void axis_weights(const PointArgs<T>& a, int i0, T xs, T* w) {
+  if (std::is_same<T, float>::value && a.poly.deg > 0) {
+    const float v = 2.0f * (float)(xs - (T)i0) - (float)(NS - 1);
+#pragma unroll
+    for (int q = 0; q < NS; ++q) w[q] = (T)a.poly.a[q][a.poly.deg];
+    for (int d = a.poly.deg - 1; d >= 0; --d) {
+#pragma unroll
+      for (int q = 0; q < NS; ++q) w[q] = (T)fmaf((float)w[q], v, a.poly.a[q][d]);
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < NS; ++q) w[q] = es_weight(rn_sub((T)(i0 + q), xs), a.beta, a.kc);
+  }
+}
 
 __device__ __forceinline__ void bin_origin(const Geom& g, int b, int& o0, int& o1, int& o2) {
   int bx = b % g.nb[0];
@@ -127,9 +150,10 @@ __device__ __forceinline__ void spread_subproblem(const PointArgs<T>& a, const c
             // the tile.
             inside = inside && (unsigned)l < (unsigned)g.tile[d];
             off += l * (d == 0 ? 1 : (d == 1 ? row : plane));
+            T wq[NS];
+            axis_weights<T, NS>(a, i0, xs, wq);
 #pragma unroll
-            for (int q = 0; q < NS; ++q)
-              s_w[(d * NS + q) * SW + slot] = es_weight(rn_sub((T)(i0 + q), xs), a.beta, a.kc);
+            for (int q = 0; q < NS; ++q) s_w[(d * NS + q) * SW + slot] = wq[q];
           }
           const CT cv = c[(int64_t)t * a.M + p];
           s_off[slot] = inside ? off : 0;
@@ -330,8 +354,7 @@ __device__ __forceinline__ void interp_subproblem(const PointArgs<T>& a, const c
           const int l = wrap_index(i0, g.nf[d]) - o[d];
           inside = inside && (unsigned)l < (unsigned)g.tile[d];
           off += l * (d == 0 ? 1 : (d == 1 ? row : plane));
-#pragma unroll
-          for (int q = 0; q < NS; ++q) w[d][q] = es_weight(rn_sub((T)(i0 + q), xs), a.beta, a.kc);
+          axis_weights<T, NS>(a, i0, xs, w[d]);
         }
         if (!inside) {  // stale sort: see k_spread
           CT zero;
@@ -701,6 +724,7 @@ PointArgs<T> make_args(const Geom& g, double beta, double kc, const void* x, con
   a.beta = (T)beta;
   a.kc = (T)kc;
   a.s = s;
+  a.poly.deg = 0;
   return a;
 }
 

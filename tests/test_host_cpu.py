@@ -123,3 +123,33 @@ def test_product_does_not_import_oracle():
     pkg = pathlib.Path(nb.__file__).parent
     for f in pkg.rglob("*.py"):
         assert "oracle" not in f.read_text().replace("oracle is", ""), f
+
+
+@pytest.mark.parametrize("eps", [1e-6, 1e-9, 1e-12])
+def test_es_polynomial_matches_exp_sqrt(eps):
+    """The float kernels' polynomial ES weights (nfx_es_poly, host-side fit) stay
+    within two float ulps (+3e-8) of exp(beta (sqrt(1 - c z^2) - 1))."""
+    lib = _lib.load()
+    kp = nb.compute_kernel_params(eps)
+    co = (ctypes.c_float * 256)()
+    deg = ctypes.c_int()
+    err = ctypes.c_double()
+    assert lib.nfx_es_poly(kp.nspread, kp.beta, kp.c, co, byref(deg), byref(err)) == 0
+    assert deg.value > 0
+    a = np.frombuffer(co, dtype=np.float32).reshape(16, 16)
+    v = np.linspace(-1, 1, 1001).astype(np.float32)
+    for q in range(kp.nspread):
+        h = np.full_like(v, a[q, deg.value])
+        for d in range(deg.value - 1, -1, -1):
+            h = (h.astype(np.float64) * v + a[q, d]).astype(np.float32)
+        z = q - (v.astype(np.float64) + kp.nspread - 1) / 2
+        ref = O.es_kernel(z, kp.beta, kp.c)
+        assert np.all(np.abs(h - ref) <= 3e-8 + 2.4e-7 * np.abs(ref) + 1e-7)
+
+
+def test_es_polynomial_refused_for_narrow_kernel():
+    lib = _lib.load()
+    kp = nb.compute_kernel_params(1e-3)  # ns = 4: too much edge mass for a float-accurate fit
+    deg = ctypes.c_int()
+    assert lib.nfx_es_poly(kp.nspread, kp.beta, kp.c, None, byref(deg), None) == 0
+    assert deg.value == 0
