@@ -43,13 +43,20 @@ constexpr double kInvTwoPi = 1.0 / (2.0 * 3.141592653589793);
 
 // jnp.mod(x + pi, 2 pi) - pi: lax.rem (exact fmod) plus the sign fix of
 // jnp.remainder (add the divisor when the remainder is negative and non-zero).
+// For 0 <= x + pi < 2 pi the remainder is x + pi itself (fmod is exact), which
+// skips the slow general fmod for the common in-range inputs.
 template <typename T>
 __device__ __forceinline__ T premod(T x) {
   const T pi = (T)kPi;
   const T two_pi = (T)kTwoPi;
   T a = rn_add(x, pi);
-  T r = t_fmod(a, two_pi);
-  if (r != (T)0 && r < (T)0) r = rn_add(r, two_pi);
+  T r;
+  if (a >= (T)0 && a < two_pi) {
+    r = a;
+  } else {
+    r = t_fmod(a, two_pi);
+    if (r != (T)0 && r < (T)0) r = rn_add(r, two_pi);
+  }
   return rn_sub(r, pi);
 }
 
@@ -73,8 +80,12 @@ __device__ __forceinline__ int left_cell(T xs) {
   return ceil_to_int(rn_sub(xs, (T)(NS / 2)));
 }
 
-// Periodic wrap of any int into [0, n).
+// Periodic wrap of any int into [0, n); one compare-and-add for indices within
+// one period of the grid (the footprint's left cell always is), % otherwise.
 __device__ __forceinline__ int wrap_index(int i, int n) {
+  if (i >= 0 && i < n) return i;
+  if (i < 0 && i >= -n) return i + n;
+  if (i >= n && i - n < n) return i - n;
   int r = i % n;
   return r < 0 ? r + n : r;
 }

@@ -72,7 +72,7 @@ __device__ __forceinline__ void point_keys(const T* __restrict__ x, const T* __r
   kcell = kc;
 }
 
-// Count pass of the cell sort: one CTA per chunk walks its points, 4 per thread
+// Count pass of the cell sort: one CTA per chunk walks its points, 8 per thread
 // per trip so the coordinate loads overlap, writes both keys of every point and
 // counts the cell keys with shared-memory atomics.
 template <typename T>
@@ -85,7 +85,7 @@ __global__ void k_bin_count(const T* __restrict__ x, const T* __restrict__ y, co
   __syncthreads();
   const int64_t p0 = (int64_t)ch * chunk;
   const int64_t p1 = (p0 + chunk < M) ? p0 + chunk : M;
-  constexpr int U = 4;
+  constexpr int U = 8;
   for (int64_t base = p0; base < p1; base += (int64_t)U * blockDim.x) {
     int kb[U], kc[U];
 #pragma unroll
@@ -117,6 +117,7 @@ __global__ void k_key_count(const int* __restrict__ keys, int64_t M, int nkeys, 
   __syncthreads();
   const int64_t p0 = (int64_t)ch * chunk;
   const int64_t p1 = (p0 + chunk < M) ? p0 + chunk : M;
+#pragma unroll 8
   for (int64_t p = p0 + threadIdx.x; p < p1; p += blockDim.x) atomicAdd(&s_hist[keys[p]], 1);
   __syncthreads();
   for (int b = threadIdx.x; b < nkeys; b += blockDim.x) counts[(int64_t)b * nchunks + ch] = s_hist[b];
@@ -148,6 +149,7 @@ __global__ void k_bin_scatter(const int* __restrict__ keys, const int* __restric
   const unsigned lt_mask = (1u << lane) - 1u;
   const int kbits = key_bits(nkeys);
   // (A) count this warp's keys (its own histogram row: order does not matter)
+#pragma unroll 8
   for (int64_t p = s0 + lane; p < s1; p += 32) atomicAdd(&hist[keys[p]], 1);
   __syncthreads();
   // (B) hw[w][k] = global start of key k in this chunk + count of k in warps < w
@@ -160,30 +162,33 @@ __global__ void k_bin_scatter(const int* __restrict__ keys, const int* __restric
     }
   }
   __syncthreads();
-  // (C) stable placement; the next round's inputs are loaded ahead
-  int key_next = s0 + lane < s1 ? keys[s0 + lane] : -1;
-  int val_next = (s0 + lane < s1 && vals != nullptr) ? vals[s0 + lane] : 0;
-  int aux_next = (s0 + lane < s1 && aux_in != nullptr) ? aux_in[s0 + lane] : 0;
-  for (int64_t base = s0; base < s1; base += 32) {
-    const int64_t p = base + lane;
-    const bool valid = p < s1;
-    const int key = key_next;
-    const int val = vals != nullptr ? val_next : (int)p;
-    const int aux = aux_next;
-    const int64_t pn = base + 32 + lane;
-    key_next = pn < s1 ? keys[pn] : -1;
-    if (vals != nullptr) val_next = pn < s1 ? vals[pn] : 0;
-    if (aux_in != nullptr) aux_next = pn < s1 ? aux_in[pn] : 0;
-    const unsigned peers = peer_mask(key, kbits);
-    const int rank = __popc(peers & lt_mask);
-    int pos = 0;
-    if (valid) pos = hist[key];
-    __syncwarp();
-    if (valid && rank == 0) hist[key] = pos + __popc(peers);
-    __syncwarp();
-    if (valid) {
-      out[pos + rank] = val;
-      if (aux_out != nullptr) aux_out[pos + rank] = aux;
+  // (C) stable placement, four 32-element rounds per trip: the inputs of all four
+  // are loaded first so their latencies overlap
+  constexpr int R = 4;
+  for (int64_t base = s0; base < s1; base += 32 * R) {
+    int key[R], val[R], aux[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int64_t p = base + 32 * r + lane;
+      const bool valid = p < s1;
+      key[r] = valid ? keys[p] : -1;
+      val[r] = valid && vals != nullptr ? vals[p] : (int)p;
+      aux[r] = valid && aux_in != nullptr ? aux_in[p] : 0;
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const unsigned peers = peer_mask(key[r], kbits);
+      const int rank = __popc(peers & lt_mask);
+      const bool valid = key[r] >= 0;
+      int pos = 0;
+      if (valid) pos = hist[key[r]];
+      __syncwarp();
+      if (valid && rank == 0) hist[key[r]] = pos + __popc(peers);
+      __syncwarp();
+      if (valid) {
+        out[pos + rank] = val[r];
+        if (aux_out != nullptr) aux_out[pos + rank] = aux[r];
+      }
     }
   }
 }

@@ -351,3 +351,52 @@ def test_empty_points():
     c = nb.nufft2d2(torch.zeros(0, device=d), torch.zeros(0, device=d), torch.ones((8, 8), dtype=torch.complex64,
                                                                                    device=d))
     assert c.shape == (0,)
+
+
+# -- odd sizes, odd fine grids, batches, isign 0 ---------------------------------------
+@pytest.mark.parametrize("dim,n_modes", [(1, (63,)), (2, (31, 17)), (3, (9, 12, 7)), (2, (100, 50))])
+@pytest.mark.parametrize("uf", [2.0, 1.25])
+def test_odd_modes_and_grids(dim, n_modes, uf):
+    rng = np.random.default_rng(500 + dim)
+    M = 3000
+    eps = 1e-9
+    X = [rng.uniform(-np.pi, np.pi, M) for _ in range(dim)]
+    c = rand_c(rng, (2, M), np.complex128)
+    f = rand_c(rng, (2,) + tuple(reversed(n_modes)), np.complex128)
+    t1 = {1: nb.nufft1d1, 2: nb.nufft2d1, 3: nb.nufft3d1}[dim]
+    t2 = {1: nb.nufft1d2, 2: nb.nufft2d2, 3: nb.nufft3d2}[dim]
+    nm = n_modes[0] if dim == 1 else n_modes
+    Xd = [to_dev(x) for x in X]
+    a = t1(*Xd, to_dev(c), nm, eps=eps, upsampfac=uf).cpu().numpy()
+    b = t2(*Xd, to_dev(f), eps=eps, upsampfac=uf).cpu().numpy()
+    assert a.shape == (2,) + tuple(reversed(n_modes)) and b.shape == (2, M)
+    assert rel_l2(a, O.nufft_type1(X, c, n_modes, eps=eps, upsampfac=uf)) <= 2 * eps
+    assert rel_l2(b, O.nufft_type2(X, f, eps=eps, upsampfac=uf)) <= 2 * eps
+    if uf == 2.0:
+        assert rel_l2(a[0], O.direct_type1(X, c[0], n_modes)) < 10 * eps
+
+
+def test_isign_zero_follows_reference_fft_choice():
+    """isign = 0: type 1 takes the forward FFT (nufft1.py:81), type 2 the inverse (nufft2.py:81)."""
+    rng = np.random.default_rng(77)
+    X = [rng.uniform(-np.pi, np.pi, 500) for _ in range(2)]
+    c = rand_c(rng, 500, np.complex128)
+    f = rand_c(rng, (12, 10), np.complex128)
+    Xd = [to_dev(x) for x in X]
+    a = nb.nufft2d1(*Xd, to_dev(c), (10, 12), eps=1e-9, isign=0).cpu().numpy()
+    b = nb.nufft2d2(*Xd, to_dev(f), eps=1e-9, isign=0).cpu().numpy()
+    assert rel_l2(a, O.nufft_type1(X, c, (10, 12), eps=1e-9, isign=0)) <= 2e-9
+    assert rel_l2(b, O.nufft_type2(X, f, eps=1e-9, isign=0)) <= 2e-9
+
+
+def test_noncontiguous_and_mixed_dtype_inputs():
+    rng = np.random.default_rng(78)
+    xy = to_dev(rng.uniform(-np.pi, np.pi, (1000, 2)).astype(np.float32))
+    c = to_dev(rand_c(rng, 1000))
+    f = nb.nufft2d1(xy[:, 0], xy[:, 1], c, (16, 16)).cpu().numpy()  # strided coordinates
+    X = [xy[:, 0].cpu().numpy(), xy[:, 1].cpu().numpy()]
+    assert rel_l2(f, O.nufft_type1(X, c.cpu().numpy(), (16, 16))) <= 2e-6
+    # float64 coordinates with complex64 strengths compute in the strengths' precision
+    g = nb.nufft2d1(xy[:, 0].double(), xy[:, 1].double(), c, (16, 16))
+    assert g.dtype == torch.complex64
+    assert rel_l2(g.cpu().numpy(), f) < 1e-6
