@@ -496,7 +496,19 @@ def run_case(args):
         nb.nufft2d1(x, y, c, N_MODES, eps=EPS)
         nb.nufft2d2(x, y, f, eps=EPS)
     torch.cuda.synchronize()
-    print(json.dumps({"case": args.case, "M": s["M"], "reps": args.reps}))
+    out = {"case": args.case, "M": s["M"], "reps": args.reps}
+    if args.time_calls:
+        # per-call device time on one stream (CUDA events around each library call)
+        from nufftax_b200 import profiling
+
+        with profiling.record() as rec:
+            for _ in range(args.reps):
+                nb.sort_cache.clear()
+                nb.nufft2d1(x, y, c, N_MODES, eps=EPS)
+                nb.nufft2d2(x, y, f, eps=EPS)
+        torch.cuda.synchronize()
+        out["us_per_call"] = {k: round(1e3 * v["ms"] / max(v["calls"], 1), 2) for k, v in rec.summary().items()}
+    print(json.dumps(out))
 
 
 def batched_workload(seed=77, P=64):
@@ -832,6 +844,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--case", choices=["radial", "clustered"], help="profile one point set only (no timing)")
     ap.add_argument("--reps", type=int, default=2)
+    ap.add_argument("--time-calls", action="store_true", help="with --case: also print per-call device time")
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--config", choices=["default", "batched", "grad3d", "serve"], default="default")
     ap.add_argument("--requests", type=int, default=10000)

@@ -75,7 +75,8 @@ int nfx_default_tiles(nfx_opts* opts);
 
 /* ---- bin sort --------------------------------------------------------------
  * Bytes of workspace a sort of M points needs, and the sort itself: a stable
- * counting sort of the points by the tile of their footprint's left cell.  The
+ * radix sort of the points by (tile of their footprint's left cell, that cell
+ * within the tile).  The
  * workspace then holds the permutation and the bin/subproblem tables that every
  * *_sorted call below reads; it stays valid while the coordinates are unchanged.
  * (No counterpart in the reference, which spreads unsorted points.) */
@@ -83,7 +84,8 @@ int nfx_sort_workspace_bytes(const nfx_opts* opts, int64_t M, size_t* bytes);
 int nfx_sort_points(const nfx_opts* opts, const void* x, const void* y, const void* z, int64_t M, void* workspace,
                     size_t workspace_bytes, void* stream);
 /* Copy the sort results out of a workspace (device pointers, any may be NULL):
- * keys[M], perm[M] (int32) and bin_start[nbins + 1]. */
+ * keys[M] (bin of each point, input order), perm[M] (int32) and
+ * bin_start[nbins + 1]. */
 int nfx_sort_results(const nfx_opts* opts, int64_t M, const void* workspace, size_t workspace_bytes, int* keys,
                      int* perm, int* bin_start, int* nbins, void* stream);
 

@@ -70,6 +70,23 @@ def make_opts(precision: int, nf: Sequence[int], kp: KernelParams, prenorm: bool
     return o
 
 
+def sort_launches(opts, M: int) -> int:
+    """Kernels one nfx_sort_points call launches: keys (with the first digit's
+    counts), per radix pass a column scan and a scatter (plus a count for the
+    passes after the first), bin bounds and subproblems.  The composite key is
+    bin << cell_bits | cell; digits have at most 11 bits."""
+    if M == 0:
+        return 2
+    nbins = ncell = 1
+    for d in range(int(opts.dim)):
+        t = int(opts.tile[d])
+        nbins *= -(-int(opts.nf[d]) // t)
+        ncell *= t
+    bits = max(1, (ncell - 1).bit_length() + (nbins - 1).bit_length())
+    npass = 1 if bits <= 11 else (2 if bits <= 22 else 3)
+    return 3 * npass + 2
+
+
 class PointSort:
     """Bin-sorted non-uniform points on one fine grid."""
 
@@ -95,7 +112,7 @@ class PointSort:
         _lib.check(lib.nfx_sort_workspace_bytes(byref(self.opts), self.M, byref(nbytes)), "nfx_sort_workspace_bytes")
         self.ws_bytes = int(nbytes.value)
         self.ws = torch.empty(max(self.ws_bytes, 1), dtype=torch.uint8, device=self.device)
-        with torch.cuda.device(self.device), span("nfx_sort_points", self.device, 11 if self.M > 0 else 0):
+        with torch.cuda.device(self.device), span("nfx_sort_points", self.device, sort_launches(self.opts, self.M)):
             _lib.check(lib.nfx_sort_points(byref(self.opts), *self._xyz(), self.M, ptr(self.ws), self.ws_bytes,
                                            c_void_p(stream_of(self.device))), "nfx_sort_points")
 

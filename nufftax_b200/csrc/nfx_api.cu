@@ -73,6 +73,19 @@ cudaError_t ensure_smem(const void* fn, size_t smem) {
   return e;
 }
 
+cudaError_t prefer_max_smem(const void* fn) {
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, bool> done;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(mu);
+  auto k = std::make_pair(fn, dev);
+  if (done[k]) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  if (e == cudaSuccess) done[k] = true;
+  return e;
+}
+
 cudaError_t kernel_grid(const void* fn, int threads, size_t smem, int64_t max_work, int& grid) {
   static std::mutex mu;
   static std::map<std::tuple<const void*, int, size_t, int>, int> occ;
@@ -134,6 +147,7 @@ static void fill_geom(const nfx_opts* o, Geom& g) {
     g.tile[d] = act ? o->tile[d] : 1;
     g.nb[d] = act ? (g.nf[d] + g.tile[d] - 1) / g.tile[d] : 1;
     g.pad[d] = act ? g.tile[d] + o->nspread - 1 : 1;
+    g.tdiv[d] = make_fastdiv(g.tile[d]);
   }
   g.pitch = choose_pitch(g.pad[0], o->nspread);
   g.nbins = g.nb[0] * g.nb[1] * g.nb[2];
@@ -259,19 +273,9 @@ static void make_layout(const nfx_opts& o, const Geom& g, int64_t M, SortLayout&
   L.M = M;
   L.nbins = g.nbins;
   L.ncell = g.tile[0] * g.tile[1] * g.tile[2];
-  const int64_t nk = std::max<int64_t>(g.nbins, L.ncell);
-  const int64_t target = std::max<int64_t>((int64_t)1 << 20, M / 4);
-  int64_t chunk = 1024;
-  while (nk * ((M + chunk - 1) / chunk) > target && chunk < ((int64_t)1 << 30)) chunk *= 2;
-  L.chunk = (int)chunk;
-  L.nchunks = (int)std::max<int64_t>(1, (M + chunk - 1) / chunk);
-  // warps of the scatter passes: each needs a key-histogram row in shared memory
-  L.sort_warps = (int)std::max<int64_t>(1, std::min<int64_t>(8, (int64_t)kSmemBudget / ((int64_t)g.nbins * 4)));
-  L.sort_smem = (size_t)L.sort_warps * g.nbins * sizeof(int);
-  L.sort_warps_cell = (int)std::max<int64_t>(1, std::min<int64_t>(8, (int64_t)kSmemBudget / ((int64_t)L.ncell * 4)));
-  L.sort_smem_cell = (size_t)L.sort_warps_cell * L.ncell * sizeof(int);
-  L.n_counts = nk * L.nchunks;
-  L.scan_blocks = scan_blocks(L.n_counts);
+  radix_plan(g.nbins, L.ncell, L.cbits, L.bits, L.npass, L.dbits);
+  const int64_t B = (int64_t)1 << L.dbits;
+  L.nchunks = (int)((M + radix_chunk() - 1) / radix_chunk());
   L.maxsub = o.max_subproblem;
   L.max_subs = g.nbins + (M + L.maxsub - 1) / L.maxsub;
   size_t off = 0;
@@ -281,12 +285,12 @@ static void make_layout(const nfx_opts& o, const Geom& g, int64_t M, SortLayout&
     return at;
   };
   L.off_keys = take((size_t)M * 4);
-  L.off_keys_cell = take((size_t)M * 4);
-  L.off_keys_by_cell = take((size_t)M * 4);
-  L.off_perm_cell = take((size_t)M * 4);
+  L.off_keys_tmp = take((size_t)M * 4);
+  L.off_vals_tmp = take((size_t)M * 4);
+  L.off_keys_sorted = take((size_t)M * 4);
   L.off_perm = take((size_t)M * 4);
-  L.off_counts = take((size_t)L.n_counts * 4);
-  L.off_scan = take((size_t)L.scan_blocks * 4 + 4);
+  L.off_counts = take((size_t)L.nchunks * B * 4);
+  L.off_totals = take((size_t)B * 4);
   L.off_bin_start = take((size_t)(g.nbins + 1) * 4);
   L.off_sub_bin = take((size_t)L.max_subs * 4);
   L.off_sub_start = take((size_t)L.max_subs * 4);
@@ -294,16 +298,23 @@ static void make_layout(const nfx_opts& o, const Geom& g, int64_t M, SortLayout&
   L.total = off;
 }
 
+// The composite sort key (bin << cbits | cell) must stay a non-negative int.
+static bool key_fits(const SortLayout& L) {
+  if (L.bits <= 30) return true;
+  set_error("bins x cells per tile need " + std::to_string(L.bits) + " key bits (at most 30): use smaller tiles");
+  return false;
+}
+
 static SortPtrs carve(const SortLayout& L, void* ws) {
   char* b = (char*)ws;
   SortPtrs P;
   P.keys = (int*)(b + L.off_keys);
-  P.keys_cell = (int*)(b + L.off_keys_cell);
-  P.keys_by_cell = (int*)(b + L.off_keys_by_cell);
-  P.perm_cell = (int*)(b + L.off_perm_cell);
+  P.keys_tmp = (int*)(b + L.off_keys_tmp);
+  P.vals_tmp = (int*)(b + L.off_vals_tmp);
+  P.keys_sorted = (int*)(b + L.off_keys_sorted);
   P.perm = (int*)(b + L.off_perm);
   P.counts = (int*)(b + L.off_counts);
-  P.scan_tmp = (int*)(b + L.off_scan);
+  P.totals = (int*)(b + L.off_totals);
   P.bin_start = (int*)(b + L.off_bin_start);
   P.sub_bin = (int*)(b + L.off_sub_bin);
   P.sub_start = (int*)(b + L.off_sub_start);
@@ -353,6 +364,7 @@ static int prepare(const nfx_opts* in, int64_t M, const void* x, const void* y, 
   }
   fill_geom(&P.o, P.g);
   make_layout(P.o, P.g, M, P.L);
+  if (!key_fits(P.L)) return NFX_ERR_UNSUPPORTED;
   if (ws == nullptr || ws_bytes < P.L.total) {
     set_error("workspace too small: need " + std::to_string(P.L.total) + " bytes");
     return NFX_ERR_WORKSPACE;
@@ -363,8 +375,9 @@ static int prepare(const nfx_opts* in, int64_t M, const void* x, const void* y, 
 // ---------------------------------------------------------------------------
 // Polynomial ES weights (float path): for each q, Chebyshev interpolation of
 // v -> phi(q - (v + ns - 1) / 2) on [-1, 1] at D + 1 nodes, converted to
-// monomials in v; the degree is raised until Horner's rule in float (fmaf, as on
-// the device) is within kPolyAbs + kPolyRel * |phi| of the double exp/sqrt value
+// monomials in v; the degree is raised (up to the kernels' evaluation degree)
+// until Horner's rule in float (fmaf, as on the device) is within
+// kPolyAbs + kPolyRel * |phi| of the double exp/sqrt value
 // on a fine grid: two float ulps of the weight plus a small absolute floor (the
 // exp/sqrt form in float carries errors of the same size).
 // ---------------------------------------------------------------------------
@@ -377,9 +390,9 @@ static double es_phi(double z, double beta, double kc) {
 }
 
 static bool fit_es_poly_uncached(int ns, double beta, double kc, EsPoly& out, double& err_out) {
-  for (int D = 4; D <= kPolyMaxDeg; ++D) {
+  for (int D = 4; D <= kPolyEvalDeg; ++D) {
     double worst = 0.0, worst_ratio = 0.0;
-    EsPoly P;
+    EsPoly P = {};  // coefficients above D stay zero (the kernels run degree kPolyEvalDeg)
     P.deg = D;
     for (int q = 0; q < ns; ++q) {
       const int n = D + 1;
@@ -430,8 +443,7 @@ static bool es_poly(int ns, double beta, double kc, EsPoly& out, double* err = n
   auto key = std::make_tuple(ns, beta, kc);
   auto it = cache.find(key);
   if (it == cache.end()) {
-    EsPoly P;
-    P.deg = 0;
+    EsPoly P = {};
     double e = -1.0;
     if (!fit_es_poly_uncached(ns, beta, kc, P, e)) P.deg = 0;
     it = cache.emplace(key, std::make_pair(P, e)).first;
@@ -568,6 +580,7 @@ int nfx_sort_workspace_bytes(const nfx_opts* opts, int64_t M, size_t* bytes) {
   }
   fill_geom(&P.o, P.g);
   make_layout(P.o, P.g, M, P.L);
+  if (!key_fits(P.L)) return NFX_ERR_UNSUPPORTED;
   *bytes = P.L.total;
   return NFX_OK;
 }
@@ -598,7 +611,7 @@ int nfx_sort_results(const nfx_opts* opts, int64_t M, const void* ws, size_t ws_
   cudaStream_t s = (cudaStream_t)stream;
   SortPtrs ptr = carve(P.L, const_cast<void*>(ws));
   cudaError_t e = cudaSuccess;
-  if (keys && M > 0) e = cudaMemcpyAsync(keys, ptr.keys, (size_t)M * 4, cudaMemcpyDeviceToDevice, s);
+  if (keys && M > 0) e = bin_keys_of(P.L, ptr.keys, keys, s);
   if (e == cudaSuccess && perm && M > 0) e = cudaMemcpyAsync(perm, ptr.perm, (size_t)M * 4, cudaMemcpyDeviceToDevice, s);
   if (e == cudaSuccess && bin_start)
     e = cudaMemcpyAsync(bin_start, ptr.bin_start, (size_t)(P.g.nbins + 1) * 4, cudaMemcpyDeviceToDevice, s);

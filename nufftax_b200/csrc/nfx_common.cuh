@@ -120,16 +120,69 @@ __device__ __forceinline__ void red_add(double2* addr, double2 v) {
   atomicAdd(&addr->y, v.y);
 }
 
+// Paired FMA: (a.x * b.x + c.x, a.y * b.y + c.y), each rounded once to
+// nearest.  float uses Blackwell's fma.rn.f32x2 (one instruction, the same
+// results as two fmaf); double is two fma.
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
+  float2 d;
+  asm("{\n\t.reg .b64 ra, rb, rc, rd;\n\t"
+      "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\tmov.b64 rc, {%6, %7};\n\t"
+      "fma.rn.f32x2 rd, ra, rb, rc;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+      : "=f"(d.x), "=f"(d.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+  return d;
+}
+__device__ __forceinline__ double2 fma2(double2 a, double2 b, double2 c) {
+  double2 d;
+  d.x = fma(a.x, b.x, c.x);
+  d.y = fma(a.y, b.y, c.y);
+  return d;
+}
+// c + s * v for a real s and a complex v.
+__device__ __forceinline__ float2 fma_rc(float s, float2 v, float2 c) { return fma2(make_float2(s, s), v, c); }
+__device__ __forceinline__ double2 fma_rc(double s, double2 v, double2 c) { return fma2(make_double2(s, s), v, c); }
+
 // Polynomial form of the ES weights of one footprint (float path).  For a point
 // at scaled coordinate xs with left cell i0, every weight phi(i0 + q - xs),
 // q = 0..ns-1, is a smooth function of v = 2 (xs - i0) - (ns - 1) in (-1, 1];
 // a[q][d] are monomial coefficients in v fitted on the host (nfx_es_poly) to
-// within two float ulps of the exp/sqrt form, evaluated by Horner's rule.
+// within two float ulps of the exp/sqrt form, evaluated by Horner's rule.  The
+// kernels evaluate degree kPolyEvalDeg (coefficients above the fitted degree
+// are zero, which leaves Horner's result unchanged); widths whose weights need
+// a higher degree keep the exp/sqrt form.
 constexpr int kPolyMaxDeg = 15;
+constexpr int kPolyEvalDeg = 7;
 struct EsPoly {
   float a[16][kPolyMaxDeg + 1];
   int deg;  // 0 = not used (exp/sqrt form)
 };
+
+// Exact division of a non-negative int n < 2^31 by a fixed divisor d >= 1 as a
+// multiply-high and a shift: with p = 31 + ceil(log2 d) and m = ceil(2^p / d)
+// (which fits in 32 bits), n * m / 2^p = n / d + n e / (d 2^p) for some
+// 0 <= e < d, and the second term is below 1/d, so the floor is n / d.
+// d = 1 is marked by shr = -1 (quotient n).
+struct FastDiv {
+  unsigned mul;
+  int shr;  // p - 32, or -1 for d = 1
+};
+inline FastDiv make_fastdiv(int d) {
+  FastDiv f;
+  if (d <= 1) {
+    f.mul = 0;
+    f.shr = -1;
+    return f;
+  }
+  int l = 0;
+  while ((1ll << l) < d) ++l;
+  const int p = 31 + l;
+  f.mul = (unsigned)((((unsigned long long)1 << p) + (unsigned long long)d - 1) / (unsigned long long)d);
+  f.shr = p - 32;
+  return f;
+}
+__device__ __forceinline__ int fast_div(int n, FastDiv f) {
+  return f.shr < 0 ? n : (int)(__umulhi((unsigned)n, f.mul) >> f.shr);
+}
 
 // Grid geometry shared by the sort, spread and interp kernels (plain values).
 struct Geom {
@@ -141,6 +194,7 @@ struct Geom {
   int pitch;     // shared-memory row pitch along x (>= pad[0])
   int nbins;
   int prenorm;
+  FastDiv tdiv[3];  // division by tile[d]
 };
 
 }  // namespace nfx

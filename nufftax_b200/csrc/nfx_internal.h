@@ -16,30 +16,27 @@ namespace nfx {
 struct SortLayout {
   int64_t M;
   int nbins;
-  int ncell;        // cells per tile (keys of the first sort pass)
-  int chunk;        // points per CTA in the counting passes
-  int nchunks;
-  int sort_warps;       // warps per CTA of the bin scatter pass
-  size_t sort_smem;     // its dynamic shared memory
-  int sort_warps_cell;  // same for the cell scatter pass
-  size_t sort_smem_cell;
-  int64_t n_counts; // max(nbins, ncell) * nchunks
-  int64_t scan_blocks;
+  int ncell;        // cells per tile
+  int cbits;        // composite key = bin << cbits | cell
+  int bits;         // bits of the composite key
+  int npass;        // radix passes (digits of dbits bits, least significant first)
+  int dbits;
+  int nchunks;      // chunks of one radix pass
   int maxsub;       // points per subproblem
   int64_t max_subs; // upper bound on the number of subproblems
-  size_t off_keys, off_keys_cell, off_keys_by_cell, off_perm_cell, off_perm, off_counts, off_scan, off_bin_start,
+  size_t off_keys, off_keys_tmp, off_vals_tmp, off_keys_sorted, off_perm, off_counts, off_totals, off_bin_start,
       off_sub_bin, off_sub_start, off_nsub;
   size_t total;
 };
 
 struct SortPtrs {
-  int* keys;          // bin key per point (input order)
-  int* keys_cell;     // cell-in-tile key per point (input order)
-  int* keys_by_cell;  // bin keys in cell-sorted order
-  int* perm_cell;     // cell-sorted order
-  int* perm;          // final (bin, cell) order
-  int* counts;
-  int* scan_tmp;
+  int* keys;         // composite key per point (input order)
+  int* keys_tmp;     // ping-pong buffers of the radix passes
+  int* vals_tmp;
+  int* keys_sorted;  // composite keys in sorted order
+  int* perm;         // final (bin, cell) order
+  int* counts;       // nchunks x 2^dbits digit counts, then their column prefixes
+  int* totals;       // 2^dbits digit totals
   int* bin_start;
   int* sub_bin;
   int* sub_start;
@@ -57,8 +54,10 @@ struct SortView {
   int64_t max_subs;
 };
 
-int64_t scan_blocks(int64_t n);
-cudaError_t exclusive_scan(const int* in, int* out, int64_t n, int* block_sums, cudaStream_t st);
+void radix_plan(int nbins, int ncell, int& cbits, int& bits, int& npass, int& dbits);
+int radix_chunk();
+// out[i] = bin of point i (composite key / cells per tile)
+cudaError_t bin_keys_of(const SortLayout& L, const int* K, int* out, cudaStream_t st);
 
 template <typename T>
 cudaError_t launch_sort(const SortLayout& L, const Geom& g, int ns, const void* x, const void* y, const void* z,
@@ -101,12 +100,43 @@ void set_error(const std::string& msg);
 // Warps per CTA of the spread / interp / gradient kernels.
 constexpr int warps_per_cta(size_t real_bytes, int dim, int ns) { return (real_bytes == 8 && dim == 3) ? 4 : 8; }
 
+// Run-merging spread layout (2D/3D footprints of at least 32 cells): lane l of
+// a warp owns footprint column kx = l % ns and rows (y, or z*ns + y) grp*rpl ..
+// grp*rpl + rpl - 1 with grp = l / ns; the 32 / ns groups cover the ns^(dim-1)
+// rows.  A staged point is one slot of reals: c * w_x (ns complex), then the
+// y weights (padded to the rows the groups reach), then the z weights (3D),
+// each section an even number of reals so that it is written and read in
+// complex-sized pairs.  The slot length is 2 mod 4 reals: the pair stores of a
+// warp (one slot per lane) then hit distinct banks.  run_slot_reals is 0 when
+// the layout does not apply (1D, small footprints, more than 16 rows a lane).
+__host__ __device__ constexpr int run_groups(int ns) { return 32 / ns; }
+__host__ __device__ constexpr int run_rows(int dim, int ns) { return dim == 3 ? ns * ns : ns; }
+__host__ __device__ constexpr int run_rows_per_lane(int dim, int ns) {
+  return (run_rows(dim, ns) + run_groups(ns) - 1) / run_groups(ns);
+}
+__host__ __device__ constexpr int round_even(int n) { return (n + 1) / 2 * 2; }
+__host__ __device__ constexpr int run_wy(int dim, int ns) {
+  return round_even(dim == 2 ? run_groups(ns) * run_rows_per_lane(dim, ns) : ns);
+}
+__host__ __device__ constexpr int run_wz(int dim, int ns) {
+  return dim == 3 ? round_even((run_groups(ns) * run_rows_per_lane(dim, ns) + ns - 1) / ns) : 0;
+}
+__host__ __device__ constexpr int run_slot_base(int dim, int ns) { return 2 * ns + run_wy(dim, ns) + run_wz(dim, ns); }
+__host__ __device__ constexpr int run_slot_reals(int dim, int ns) {
+  return (dim >= 2 && run_rows(dim, ns) * ns >= 32 && run_rows_per_lane(dim, ns) <= 16)
+             ? run_slot_base(dim, ns) + (run_slot_base(dim, ns) % 4 == 0 ? 2 : 0)
+             : 0;
+}
+
 // Dynamic shared memory of the spread kernel: two planar tile planes plus the
-// per-warp staging of 32 points (weights, strengths, tile offsets).
+// per-warp staging of 32 points (weights, strengths; tile offsets for the
+// layout without run merging).
 inline size_t spread_smem_bytes(size_t real_bytes, int dim, int ns, const Geom& g) {
   const int nw = warps_per_cta(real_bytes, dim, ns);
-  return 2 * real_bytes * (size_t)g.pad[2] * g.pad[1] * g.pitch +
-         ((size_t)dim * ns * (nw * 32 + 1) + (size_t)2 * nw * 32) * real_bytes + (size_t)nw * 32 * sizeof(int);
+  const size_t tile = 2 * real_bytes * (size_t)g.pad[2] * g.pad[1] * g.pitch;
+  const int slot = run_slot_reals(dim, ns);
+  if (slot > 0) return tile + (size_t)nw * 32 * slot * real_bytes;
+  return tile + ((size_t)dim * ns * (nw * 32 + 1) + (size_t)2 * nw * 32) * real_bytes + (size_t)nw * 32 * sizeof(int);
 }
 inline size_t tile_smem_bytes(size_t real_bytes, const Geom& g) {
   return 2 * real_bytes * (size_t)g.pad[2] * g.pad[1] * g.pitch;
@@ -122,5 +152,7 @@ inline size_t interp_smem_bytes(size_t real_bytes, int dim, int ns, const Geom& 
 cudaError_t kernel_grid(const void* fn, int threads, size_t smem, int64_t max_work, int& grid);
 // Opt a kernel in to `smem` bytes of dynamic shared memory (cached per device).
 cudaError_t ensure_smem(const void* fn, size_t smem);
+// Ask for the largest shared-memory carveout for a kernel (cached per device).
+cudaError_t prefer_max_smem(const void* fn);
 
 }  // namespace nfx

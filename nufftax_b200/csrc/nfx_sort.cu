@@ -1,28 +1,35 @@
-// Bin sort of the non-uniform points: a stable counting sort on integer bin keys.
+// Bin sort of the non-uniform points: a stable LSD radix sort on one composite
+// integer key per point.
 //
 // The reference has no sort (nufftax spreads unsorted points with atomics,
-// nufftax/core/pallas_spread.py:337-613).  Here every point gets the key of the
-// tile that holds its footprint's left cell (i0 = ceil(fold(x) - ns/2) wrapped
-// into [0, nf), divided by the tile edge, x-fastest) and the index of that cell
-// inside the tile, and the permutation is the STABLE sort by (bin, cell): it
-// equals numpy.argsort(bin * cells_per_tile + cell, kind="stable") bit for bit.
-// It is computed least-significant key first, as two stable counting passes
-// (cell, then bin); each pass is:
+// nufftax/core/pallas_spread.py:337-613).  Here every point gets the key
+// K = bin << cbits | cell, where bin is the tile that holds its footprint's
+// left cell (i0 = ceil(fold(x) - ns/2) wrapped into [0, nf), divided by the
+// tile edge, x-fastest) and cell that cell's index inside the tile (cbits =
+// bits of cells per tile); the permutation is the STABLE sort by (bin, cell),
+// equal to numpy.argsort(bin * cells_per_tile + cell, kind="stable") bit for
+// bit.  Work is split into chunks of 4096 consecutive elements, one CTA each:
 //
-// (1) count (k_bin_count, k_key_count): one CTA per chunk of consecutive
-//     elements builds the chunk's key histogram in shared memory and writes it
-//     to a key-major matrix counts[key][chunk];
-// (2) an exclusive scan of that matrix: entry (key, chunk) becomes the global
-//     position of the chunk's first element with that key;
-// (3) scatter (k_bin_scatter): one CTA per chunk again, each warp on a
-//     contiguous sub-chunk; ballots rank equal keys within each 32-element
-//     round (peer_mask: one ballot per key bit) and per-warp
-//     running counts (offset by the warps before it) carry the rank across
-//     rounds, so ties keep their input order.
-// Finally k_subproblems splits bins larger than max_subproblem points into
-// subproblems so clustered inputs spread evenly over the SMs.  Points of a
-// subproblem are then ordered by cell, which lets spreading merge runs of points
-// that share a cell and gives interpolation near-identical addresses per warp.
+// (1) k_sort_keys computes K for every point (one pass over the coordinates)
+//     and each chunk's histogram of the first radix digit, written as row
+//     `chunk` of a chunk-major count matrix;
+// (2) per radix digit (1 to 3 digits of at most 11 bits, least significant
+//     first): k_digit_count (digits after the first) fills the matrix from the
+//     previous pass's output, k_col_scan turns every column into the counts of
+//     the chunks before each chunk plus the digit's total, and
+//     k_radix_scatter ranks equal digits stably within the chunk (one ballot
+//     per digit bit inside each 32-element round, per-warp running counts
+//     across rounds), stages the chunk in shared memory in digit order and
+//     writes it out as contiguous runs per digit;
+// (3) k_bin_bounds reads the bin starts off the sorted keys, and
+//     k_subproblems splits bins larger than max_subproblem points into
+//     subproblems so clustered inputs spread evenly over the SMs.  Points of
+//     a subproblem are ordered by cell, which lets spreading merge runs of
+//     points that share a cell and gives interpolation near-identical
+//     addresses per warp.
+// No CTA waits for another: every dependency is a kernel boundary.
+#include <algorithm>
+
 #include "nfx_internal.h"
 
 namespace nfx {
@@ -48,337 +55,471 @@ __host__ __device__ inline int key_bits(int nkeys) {
 }
 
 // Bin of the tile holding the footprint's left cell, and that cell's index
-// inside the tile (both x-fastest).
-template <typename T>
-__device__ __forceinline__ void point_keys(const T* __restrict__ x, const T* __restrict__ y,
-                                           const T* __restrict__ z, int64_t p, const Geom& g, int ns_half, int& kbin,
-                                           int& kcell) {
+// inside the tile (both x-fastest), from the point's coordinates.
+template <typename T, int DIM>
+__device__ __forceinline__ void cell_keys(const T (&c)[DIM], const Geom& g, int ns_half, int& kbin, int& kcell) {
   int kb = 0, kc = 0, mb = 1, mc = 1;
-  const T* cs[3] = {x, y, z};
 #pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    if (d < g.dim) {
-      T xs = scaled_coord(cs[d][p], g.nf[d], g.prenorm);
-      int i0 = ceil_to_int(rn_sub(xs, (T)ns_half));
-      int i0w = wrap_index(i0, g.nf[d]);
-      int bq = i0w / g.tile[d];
-      kb += bq * mb;
-      kc += (i0w - bq * g.tile[d]) * mc;
-      mb *= g.nb[d];
-      mc *= g.tile[d];
-    }
+  for (int d = 0; d < DIM; ++d) {
+    const T xs = scaled_coord(c[d], g.nf[d], g.prenorm);
+    const int i0w = wrap_index(ceil_to_int(rn_sub(xs, (T)ns_half)), g.nf[d]);
+    const int bq = fast_div(i0w, g.tdiv[d]);
+    kb += bq * mb;
+    kc += (i0w - bq * g.tile[d]) * mc;
+    mb *= g.nb[d];
+    mc *= g.tile[d];
   }
   kbin = kb;
   kcell = kc;
 }
 
-// Count pass of the cell sort: one CTA per chunk walks its points, 8 per thread
-// per trip so the coordinate loads overlap, writes both keys of every point and
-// counts the cell keys with shared-memory atomics.
-template <typename T>
-__global__ void k_bin_count(const T* __restrict__ x, const T* __restrict__ y, const T* __restrict__ z,
-                            int64_t M, Geom g, int ns_half, int chunk, int nchunks, int ncell,
-                            int* __restrict__ keys_bin, int* __restrict__ keys_cell, int* __restrict__ counts) {
-  extern __shared__ int s_hist[];
-  const int ch = blockIdx.x;
-  for (int b = threadIdx.x; b < ncell; b += blockDim.x) s_hist[b] = 0;
-  __syncthreads();
-  const int64_t p0 = (int64_t)ch * chunk;
-  const int64_t p1 = (p0 + chunk < M) ? p0 + chunk : M;
-  constexpr int U = 8;
-  for (int64_t base = p0; base < p1; base += (int64_t)U * blockDim.x) {
-    int kb[U], kc[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int64_t p = base + (int64_t)u * blockDim.x + threadIdx.x;
-      kb[u] = kc[u] = -1;
-      if (p < p1) point_keys(x, y, z, p, g, ns_half, kb[u], kc[u]);
-    }
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int64_t p = base + (int64_t)u * blockDim.x + threadIdx.x;
-      if (kc[u] >= 0) {
-        keys_bin[p] = kb[u];
-        keys_cell[p] = kc[u];
-        atomicAdd(&s_hist[kc[u]], 1);
-      }
-    }
-  }
-  __syncthreads();
-  for (int b = threadIdx.x; b < ncell; b += blockDim.x) counts[(int64_t)b * nchunks + ch] = s_hist[b];
-}
-
-// Histogram of an int key array per chunk (second pass of the sort).
-__global__ void k_key_count(const int* __restrict__ keys, int64_t M, int nkeys, int chunk, int nchunks,
-                            int* __restrict__ counts) {
-  extern __shared__ int s_hist[];
-  const int ch = blockIdx.x;
-  for (int b = threadIdx.x; b < nkeys; b += blockDim.x) s_hist[b] = 0;
-  __syncthreads();
-  const int64_t p0 = (int64_t)ch * chunk;
-  const int64_t p1 = (p0 + chunk < M) ? p0 + chunk : M;
-#pragma unroll 8
-  for (int64_t p = p0 + threadIdx.x; p < p1; p += blockDim.x) atomicAdd(&s_hist[keys[p]], 1);
-  __syncthreads();
-  for (int b = threadIdx.x; b < nkeys; b += blockDim.x) counts[(int64_t)b * nchunks + ch] = s_hist[b];
-}
-
-// Scatter pass: one CTA per chunk; warp w owns the contiguous sub-chunk w of
-// the chunk and its own histogram row hw[w][*].  (A) each warp counts its keys,
-// (B) a prefix over the warps turns the rows into each warp's starting rank per
-// key, (C) each warp walks its sub-chunk in order and ranks equal keys with
-// peer_mask, so the result is a stable sort.  Element i goes to
-// out[pos] = vals ? vals[i] : i, and aux_out[pos] = aux_in[i] carries a second
-// array along.
-__global__ void k_bin_scatter(const int* __restrict__ keys, const int* __restrict__ vals, const int* __restrict__ aux_in,
-                              int64_t M, int nkeys, int chunk, int nchunks, const int* __restrict__ offsets,
-                              int* __restrict__ out, int* __restrict__ aux_out) {
-  extern __shared__ int s_hw[];
-  const int W = blockDim.x >> 5;
-  const int w = threadIdx.x >> 5;
-  const int lane = threadIdx.x & 31;
-  const int ch = blockIdx.x;
-  for (int i = threadIdx.x; i < W * nkeys; i += blockDim.x) s_hw[i] = 0;
-  __syncthreads();
-  const int64_t p0 = (int64_t)ch * chunk;
-  const int64_t p1 = (p0 + chunk < M) ? p0 + chunk : M;
-  const int64_t sub = (((p1 - p0) + W - 1) / W + 31) / 32 * 32;
-  const int64_t s0 = p0 + (int64_t)w * sub < p1 ? p0 + (int64_t)w * sub : p1;
-  const int64_t s1 = s0 + sub < p1 ? s0 + sub : p1;
-  int* hist = s_hw + (size_t)w * nkeys;
-  const unsigned lt_mask = (1u << lane) - 1u;
-  const int kbits = key_bits(nkeys);
-  // (A) count this warp's keys (its own histogram row: order does not matter)
-#pragma unroll 8
-  for (int64_t p = s0 + lane; p < s1; p += 32) atomicAdd(&hist[keys[p]], 1);
-  __syncthreads();
-  // (B) hw[w][k] = global start of key k in this chunk + count of k in warps < w
-  for (int k = threadIdx.x; k < nkeys; k += blockDim.x) {
-    int run = offsets[(int64_t)k * nchunks + ch];
-    for (int v = 0; v < W; ++v) {
-      const int t = s_hw[(size_t)v * nkeys + k];
-      s_hw[(size_t)v * nkeys + k] = run;
-      run += t;
-    }
-  }
-  __syncthreads();
-  // (C) stable placement, four 32-element rounds per trip: the inputs of all four
-  // are loaded first so their latencies overlap
-  constexpr int R = 4;
-  for (int64_t base = s0; base < s1; base += 32 * R) {
-    int key[R], val[R], aux[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int64_t p = base + 32 * r + lane;
-      const bool valid = p < s1;
-      key[r] = valid ? keys[p] : -1;
-      val[r] = valid && vals != nullptr ? vals[p] : (int)p;
-      aux[r] = valid && aux_in != nullptr ? aux_in[p] : 0;
-    }
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const unsigned peers = peer_mask(key[r], kbits);
-      const int rank = __popc(peers & lt_mask);
-      const bool valid = key[r] >= 0;
-      int pos = 0;
-      if (valid) pos = hist[key[r]];
-      __syncwarp();
-      if (valid && rank == 0) hist[key[r]] = pos + __popc(peers);
-      __syncwarp();
-      if (valid) {
-        out[pos + rank] = val[r];
-        if (aux_out != nullptr) aux_out[pos + rank] = aux[r];
-      }
-    }
-  }
-}
-
-// bin_start[b] = offsets[b][0]; bin_start[nbins] = M.  Then subproblems: bin b
-// gets ceil(count_b / maxsub) of them.  One block; each thread owns a
-// contiguous run of bins.
-__global__ void k_subproblems(const int* __restrict__ offsets, int nbins, int nchunks, int M, int maxsub,
-                              int* __restrict__ bin_start, int* __restrict__ sub_bin,
-                              int* __restrict__ sub_start, int* __restrict__ nsub_out) {
-  __shared__ int s_warp[32];
-  const int tid = threadIdx.x;
-  const int nt = blockDim.x;
-  const int per = (nbins + nt - 1) / nt;
-  const int b0 = min(tid * per, nbins);
-  const int b1 = min(b0 + per, nbins);
-  int local = 0;
-  for (int b = b0; b < b1; ++b) {
-    int s = offsets[(int64_t)b * nchunks];
-    int e = (b + 1 < nbins) ? offsets[(int64_t)(b + 1) * nchunks] : M;
-    bin_start[b] = s;
-    local += (e - s + maxsub - 1) / maxsub;
-  }
-  if (tid == 0) bin_start[nbins] = M;
-  // block exclusive scan of `local`
-  const int lane = tid & 31, wid = tid >> 5;
-  int v = local;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    int n = __shfl_up_sync(0xffffffffu, v, o);
-    if (lane >= o) v += n;
-  }
-  if (lane == 31) s_warp[wid] = v;
-  __syncthreads();
-  if (wid == 0) {
-    int nw = nt >> 5;
-    int t = lane < nw ? s_warp[lane] : 0;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      int n = __shfl_up_sync(0xffffffffu, t, o);
-      if (lane >= o) t += n;
-    }
-    if (lane < nw) s_warp[lane] = t;
-  }
-  __syncthreads();
-  int excl = v - local + (wid > 0 ? s_warp[wid - 1] : 0);
-  if (tid == nt - 1) *nsub_out = excl + local;
-  for (int b = b0; b < b1; ++b) {
-    int s = offsets[(int64_t)b * nchunks];
-    int e = (b + 1 < nbins) ? offsets[(int64_t)(b + 1) * nchunks] : M;
-    for (int q = s; q < e; q += maxsub) {
-      sub_bin[excl] = b;
-      sub_start[excl] = q;
-      ++excl;
-    }
-  }
-}
-
-// ---- generic exclusive scan of int32 (three kernels, scratch = block sums) ----
-constexpr int kScanBlock = 512;
-constexpr int kScanItems = 8;
-constexpr int kScanTile = kScanBlock * kScanItems;
-
+// ---- block-wide exclusive scan of one int per thread ----------------------
 __device__ __forceinline__ int block_exclusive_scan(int v, int* s_warp, int& total) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   int inc = v;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
-    int n = __shfl_up_sync(0xffffffffu, inc, o);
+    const int n = __shfl_up_sync(0xffffffffu, inc, o);
     if (lane >= o) inc += n;
   }
   if (lane == 31) s_warp[wid] = inc;
   __syncthreads();
   if (wid == 0) {
-    int nw = blockDim.x >> 5;
+    const int nw = blockDim.x >> 5;
     int t = lane < nw ? s_warp[lane] : 0;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      int n = __shfl_up_sync(0xffffffffu, t, o);
+      const int n = __shfl_up_sync(0xffffffffu, t, o);
       if (lane >= o) t += n;
     }
     if (lane < nw) s_warp[lane] = t;
   }
   __syncthreads();
   total = s_warp[(blockDim.x >> 5) - 1];
-  int res = inc - v + (wid > 0 ? s_warp[wid - 1] : 0);
+  const int res = inc - v + (wid > 0 ? s_warp[wid - 1] : 0);
   __syncthreads();
   return res;
 }
 
-__global__ void k_scan_reduce(const int* __restrict__ in, int64_t n, int* __restrict__ block_sums) {
-  __shared__ int s_warp[32];
-  const int64_t base = (int64_t)blockIdx.x * kScanTile;
-  int sum = 0;
+
+constexpr int kRadixThreads = 256;
+constexpr int kRadixItems = 16;
+constexpr int kRadixChunk = kRadixThreads * kRadixItems;  // elements per chunk (one CTA)
+
+// ---- (1) composite keys + the first digit's per-chunk counts ---------------
+// One CTA per chunk of kRadixChunk consecutive points: K = bin << cbits | cell
+// for every point, and the chunk's histogram of digit 0 as row `chunk` of
+// counts (chunk-major, so the row is one coalesced write).
+template <typename T, int DIM>
+__global__ void __launch_bounds__(kRadixThreads) k_sort_keys(const T* __restrict__ x, const T* __restrict__ y,
+                                                            const T* __restrict__ z, int M, Geom g, int ns_half,
+                                                            int cbits, int dbits, int* __restrict__ K,
+                                                            int* __restrict__ counts) {
+  extern __shared__ int s_h[];
+  const int B = 1 << dbits;
+  const int mask = B - 1;
+  for (int i = threadIdx.x; i < B; i += blockDim.x) s_h[i] = 0;
+  __syncthreads();
+  const int c0 = blockIdx.x * kRadixChunk;
+  const T* cs[3] = {x, y, z};
+  // all coordinate loads first, so they are in flight together
+  T cv[kRadixItems][DIM];
 #pragma unroll
-  for (int i = 0; i < kScanItems; ++i) {
-    int64_t idx = base + (int64_t)i * kScanBlock + threadIdx.x;
-    if (idx < n) sum += in[idx];
+  for (int u = 0; u < kRadixItems; ++u) {
+    const int p = c0 + u * kRadixThreads + threadIdx.x;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) cv[u][d] = p < M ? cs[d][p] : (T)0;
+  }
+#pragma unroll
+  for (int u = 0; u < kRadixItems; ++u) {
+    const int p = c0 + u * kRadixThreads + threadIdx.x;
+    if (p < M) {
+      int kb, kc;
+      cell_keys<T, DIM>(cv[u], g, ns_half, kb, kc);
+      const int key = (kb << cbits) | kc;
+      K[p] = key;
+      atomicAdd(&s_h[key & mask], 1);
+    }
+  }
+  __syncthreads();
+  int* row = counts + (size_t)blockIdx.x * B;
+  for (int i = threadIdx.x; i < B; i += blockDim.x) row[i] = s_h[i];
+}
+
+// Per-chunk counts of digit (K >> shift) & (B - 1), for the passes after the first.
+__global__ void __launch_bounds__(kRadixThreads) k_digit_count(const int* __restrict__ kin, int M, int shift,
+                                                              int dbits, int* __restrict__ counts) {
+  extern __shared__ int s_h[];
+  const int B = 1 << dbits;
+  const int mask = B - 1;
+  for (int i = threadIdx.x; i < B; i += blockDim.x) s_h[i] = 0;
+  __syncthreads();
+  const int c0 = blockIdx.x * kRadixChunk;
+  int key[kRadixItems];
+#pragma unroll
+  for (int u = 0; u < kRadixItems; ++u) {
+    const int p = c0 + u * kRadixThreads + threadIdx.x;
+    key[u] = p < M ? kin[p] : -1;
+  }
+#pragma unroll
+  for (int u = 0; u < kRadixItems; ++u)
+    if (key[u] >= 0) atomicAdd(&s_h[(key[u] >> shift) & mask], 1);
+  __syncthreads();
+  int* row = counts + (size_t)blockIdx.x * B;
+  for (int i = threadIdx.x; i < B; i += blockDim.x) row[i] = s_h[i];
+}
+
+// ---- (2a) column scan of the counts -----------------------------------------
+// counts[chunk][d] becomes the number of digit-d elements in the chunks before
+// `chunk`; totals[d] = all of them.  A block takes 8 digit columns; its 1024
+// threads are 8 digits x 128 contiguous chunk groups, and warp d scans the
+// 128 group sums of digit d in shared memory.
+constexpr int kScanDigits = 8;
+constexpr int kScanGroups = 128;
+__global__ void __launch_bounds__(kScanDigits * kScanGroups) k_col_scan(int* __restrict__ counts, int nchunks, int B,
+                                                                        int* __restrict__ totals) {
+  __shared__ int s_sum[kScanGroups][kScanDigits + 1];
+  const int dl = threadIdx.x % kScanDigits;
+  const int gy = threadIdx.x / kScanDigits;
+  const int d = blockIdx.x * kScanDigits + dl;
+  const int per = (nchunks + kScanGroups - 1) / kScanGroups;
+  const int cg0 = min(gy * per, nchunks);
+  const int cg1 = min(cg0 + per, nchunks);
+  int sum = 0;
+  if (d < B) {
+#pragma unroll 8
+    for (int c = cg0; c < cg1; ++c) sum += counts[(size_t)c * B + d];
+  }
+  s_sum[gy][dl] = sum;
+  __syncthreads();
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (w < kScanDigits) {  // warp w: exclusive scan of digit w's group sums, 4 groups a lane
+    int v[kScanGroups / 32];
+    int t = 0;
+#pragma unroll
+    for (int j = 0; j < kScanGroups / 32; ++j) {
+      v[j] = s_sum[lane * (kScanGroups / 32) + j][w];
+      t += v[j];
+    }
+    int inc = t;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int n = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += n;
+    }
+    int run = inc - t;
+#pragma unroll
+    for (int j = 0; j < kScanGroups / 32; ++j) {
+      s_sum[lane * (kScanGroups / 32) + j][w] = run;
+      run += v[j];
+    }
+    const int dw = blockIdx.x * kScanDigits + w;
+    if (lane == 31 && dw < B) totals[dw] = inc;
+  }
+  __syncthreads();
+  if (d < B) {
+    int run = s_sum[gy][dl];
+#pragma unroll 8
+    for (int c = cg0; c < cg1; ++c) {
+      const size_t i = (size_t)c * B + d;
+      const int t = counts[i];
+      counts[i] = run;
+      run += t;
+    }
+  }
+}
+
+// ---- (2b) one stable scatter pass --------------------------------------------
+// Shared memory: per-warp digit counts (later reused for the staged chunk), the
+// chunk's digit starts and each digit's output offset.
+__host__ __device__ constexpr int radix_region_ints(int B) {
+  return (kRadixThreads / 32) * B > 2 * kRadixChunk ? (kRadixThreads / 32) * B : 2 * kRadixChunk;
+}
+__host__ __device__ constexpr size_t radix_smem_bytes(int B) {
+  return (size_t)(radix_region_ints(B) + 2 * B) * sizeof(int);
+}
+
+// kin/vin: this pass's input keys and values (vin == nullptr: the values are
+// the element indices); kout/vout: the output, stable by digit
+// (kin >> shift) & (2^dbits - 1).  prefix[chunk][d]: digit-d elements in the
+// chunks before this one; totals[d]: digit-d elements overall.
+template <int DPT>
+__global__ void __launch_bounds__(kRadixThreads) k_radix_scatter(const int* __restrict__ kin,
+                                                                const int* __restrict__ vin, int M, int shift,
+                                                                int dbits, const int* __restrict__ prefix,
+                                                                const int* __restrict__ totals,
+                                                                int* __restrict__ kout, int* __restrict__ vout) {
+  extern __shared__ int smem[];
+  __shared__ int s_warp[32];
+  constexpr int W = kRadixThreads / 32;
+  const int B = 1 << dbits;
+  const int mask = B - 1;
+  int* s_hw = smem;                             // [W][B] per-warp digit counts
+  int* s_key = smem;                            // [kRadixChunk] staged keys (after ranking)
+  int* s_val = smem + kRadixChunk;              // [kRadixChunk] staged values
+  int* s_dstart = smem + radix_region_ints(B);  // [B] digit starts within the chunk
+  int* s_gofs = s_dstart + B;                   // [B] output index - staged index, per digit
+  for (int i = threadIdx.x; i < W * B; i += blockDim.x) s_hw[i] = 0;
+  const int ch = blockIdx.x;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int c0 = ch * kRadixChunk;
+  const int wbase = c0 + w * (kRadixItems * 32);
+  int key[kRadixItems], val[kRadixItems], rk[kRadixItems];
+#pragma unroll
+  for (int r = 0; r < kRadixItems; ++r) {
+    const int p = wbase + r * 32 + lane;
+    const bool valid = p < M;
+    key[r] = valid ? kin[p] : -1;
+    val[r] = valid ? (vin != nullptr ? vin[p] : p) : 0;
+  }
+  // this thread's digits (a contiguous range): their totals and the counts of
+  // the chunks before this one, fetched now so the loads overlap the ranking
+  constexpr int kMaxDpt = DPT;  // ceil(2^dbits / threads)
+  const int d0 = min((int)threadIdx.x * DPT, B);
+  const int d1 = min(d0 + DPT, B);
+  int tot_d[kMaxDpt], pre_d[kMaxDpt];
+  const int* pre = prefix + (size_t)ch * B;
+#pragma unroll
+  for (int j = 0; j < kMaxDpt; ++j) {
+    tot_d[j] = d0 + j < d1 ? totals[d0 + j] : 0;
+    pre_d[j] = d0 + j < d1 ? pre[d0 + j] : 0;
+  }
+  __syncthreads();
+  // stable rank of each element among the equal digits of its warp: the first
+  // lane of each group of equal digits in a 32-element round adds the group's
+  // size to the warp's running count with one returning shared atomic (a warp's
+  // shared atomics complete in issue order, so rounds stay in order), and the
+  // group reads the old count from that lane
+  const unsigned lt = (1u << lane) - 1u;
+  int* hw = s_hw + w * B;
+  const int dbits1 = dbits + 1;  // digits shifted by one so the invalid lanes (-1) stay apart
+#pragma unroll
+  for (int r = 0; r < kRadixItems; ++r) {
+    const int d = key[r] >= 0 ? (key[r] >> shift) & mask : -1;
+    const unsigned peers = peer_mask(d, dbits1);
+    const int rank = __popc(peers & lt);
+    int pos = 0;
+    if (d >= 0 && rank == 0) pos = atomicAdd(&hw[d], __popc(peers));
+    pos = __shfl_sync(0xffffffffu, pos, __ffs(peers) - 1);
+    rk[r] = pos + rank;
+  }
+  __syncthreads();
+  // per digit: the warps' exclusive starts, the chunk's count, and the digit's
+  // global start (exclusive scan of the totals)
+  int cnt_d[kMaxDpt];
+  int mine = 0, tot = 0;
+#pragma unroll
+  for (int j = 0; j < kMaxDpt; ++j) {
+    const int d = d0 + j;
+    int c[W];
+#pragma unroll
+    for (int v = 0; v < W; ++v) c[v] = d < d1 ? s_hw[v * B + d] : 0;
+    int run = 0;
+#pragma unroll
+    for (int v = 0; v < W; ++v) {
+      if (d < d1) s_hw[v * B + d] = run;
+      run += c[v];
+    }
+    cnt_d[j] = run;
+    mine += run;
+    tot += tot_d[j];
   }
   int total;
-  block_exclusive_scan(sum, s_warp, total);
-  if (threadIdx.x == 0) block_sums[blockIdx.x] = total;
-}
-
-// Single block scans the block sums in place (nblocks <= kScanTile * something):
-// loops over tiles of kScanTile carrying the running total.
-__global__ void k_scan_sums(int* __restrict__ sums, int nblocks) {
-  __shared__ int s_warp[32];
-  int carry = 0;
-  for (int base = 0; base < nblocks; base += kScanBlock) {
-    int idx = base + threadIdx.x;
-    int v = idx < nblocks ? sums[idx] : 0;
-    int total;
-    int ex = block_exclusive_scan(v, s_warp, total);
-    if (idx < nblocks) sums[idx] = ex + carry;
-    carry += total;
-  }
-}
-
-__global__ void k_scan_apply(const int* __restrict__ in, int64_t n, const int* __restrict__ block_sums,
-                             int* __restrict__ out) {
-  __shared__ int s_warp[32];
-  const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
-  int vals[kScanItems];
-  int sum = 0;
+  int run = block_exclusive_scan(mine, s_warp, total);
+  int gbase = block_exclusive_scan(tot, s_warp, total);
 #pragma unroll
-  for (int i = 0; i < kScanItems; ++i) {
-    int64_t idx = base + i;
-    vals[i] = idx < n ? in[idx] : 0;
-    sum += vals[i];
+  for (int j = 0; j < kMaxDpt; ++j) {
+    const int d = d0 + j;
+    if (d < d1) {
+      s_dstart[d] = run;
+      s_gofs[d] = gbase + pre_d[j] - run;
+    }
+    run += cnt_d[j];
+    gbase += tot_d[j];
   }
+  __syncthreads();
+  // staged (digit-ordered) index of every element
+#pragma unroll
+  for (int r = 0; r < kRadixItems; ++r) {
+    if (key[r] >= 0) {
+      const int d = (key[r] >> shift) & mask;
+      rk[r] += s_dstart[d] + hw[d];
+    }
+  }
+  __syncthreads();  // the per-warp counts are dead: the region now holds the staged chunk
+#pragma unroll
+  for (int r = 0; r < kRadixItems; ++r) {
+    if (key[r] >= 0) {
+      s_key[rk[r]] = key[r];
+      s_val[rk[r]] = val[r];
+    }
+  }
+  __syncthreads();
+  const int n_here = M - c0 < kRadixChunk ? M - c0 : kRadixChunk;
+  for (int i = threadIdx.x; i < n_here; i += blockDim.x) {
+    const int k = s_key[i];
+    const int gpos = s_gofs[(k >> shift) & mask] + i;
+    if ((unsigned)gpos < (unsigned)M) {  // always: counts and keys come from the same array
+      kout[gpos] = k;
+      vout[gpos] = s_val[i];
+    }
+  }
+}
+
+// ---- (3) bin starts and subproblems ----------------------------------------
+// bin_start[b] = first sorted position whose key lies in bin b (M for bins past
+// the last point); position i writes the starts of every bin in
+// (bin of i-1, bin of i].  Each thread takes 4 consecutive positions (one
+// vector load).
+__global__ void k_bin_bounds(const int* __restrict__ Ks, int M, int cbits, int nbins, int* __restrict__ bin_start) {
+  const int nq = M / 4 + 1;  // quads covering positions 0..M
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nq; t += gridDim.x * blockDim.x) {
+    const int i0 = 4 * t;
+    int k[4];
+    if (i0 + 3 < M) {
+      const int4 v = *reinterpret_cast<const int4*>(Ks + i0);
+      k[0] = v.x;
+      k[1] = v.y;
+      k[2] = v.z;
+      k[3] = v.w;
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) k[j] = i0 + j < M ? Ks[i0 + j] : 0;
+    }
+    int bp = i0 > 0 ? min(Ks[i0 - 1] >> cbits, nbins) : -1;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int i = i0 + j;
+      if (i > M) break;
+      const int b = i < M ? min(k[j] >> cbits, nbins) : nbins;  // clamped: keys are in range
+      for (int bb = bp + 1; bb <= b; ++bb) bin_start[bb] = i;
+      bp = b;
+    }
+  }
+}
+
+// Bin b gets ceil(count_b / maxsub) subproblems.  One block: each thread
+// counts a contiguous run of bins, a block scan gives every bin its first
+// subproblem, and then (when the per-bin firsts fit in shared memory) all
+// threads fill the tables together, each locating its subproblem's bin by
+// binary search; otherwise each thread fills its own bins.
+constexpr int kSubSmemBins = 12288;
+__global__ void k_subproblems(const int* __restrict__ bin_start, int nbins, int maxsub, int max_subs,
+                              int* __restrict__ sub_bin, int* __restrict__ sub_start, int* __restrict__ nsub_out) {
+  __shared__ int s_warp[32];
+  extern __shared__ int s_first[];  // [nbins + 1] when nbins <= kSubSmemBins
+  const int tid = threadIdx.x;
+  const int nt = blockDim.x;
+  const int per = (nbins + nt - 1) / nt;
+  const int b0 = min(tid * per, nbins);
+  const int b1 = min(b0 + per, nbins);
+  int local = 0;
+  for (int b = b0; b < b1; ++b) local += max(bin_start[b + 1] - bin_start[b] + maxsub - 1, 0) / maxsub;
   int total;
-  int ex = block_exclusive_scan(sum, s_warp, total) + block_sums[blockIdx.x];
-#pragma unroll
-  for (int i = 0; i < kScanItems; ++i) {
-    int64_t idx = base + i;
-    if (idx < n) out[idx] = ex;
-    ex += vals[i];
+  int excl = block_exclusive_scan(local, s_warp, total);
+  const int nsub = min(total, max_subs);  // the tables hold max_subs entries (more only for corrupt bounds)
+  if (tid == 0) *nsub_out = nsub;
+  if (nbins <= kSubSmemBins) {
+    for (int b = b0; b < b1; ++b) {
+      s_first[b] = excl;
+      excl += max(bin_start[b + 1] - bin_start[b] + maxsub - 1, 0) / maxsub;
+    }
+    if (tid == 0) s_first[nbins] = total;
+    __syncthreads();
+    for (int sidx = tid; sidx < nsub; sidx += nt) {
+      int lo = 0, hi = nbins;  // last bin with s_first[bin] <= sidx
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (s_first[mid] <= sidx)
+          lo = mid;
+        else
+          hi = mid;
+      }
+      sub_bin[sidx] = lo;
+      sub_start[sidx] = bin_start[lo] + (sidx - s_first[lo]) * maxsub;
+    }
+  } else {
+    for (int b = b0; b < b1; ++b) {
+      const int e = bin_start[b + 1];
+      for (int q = bin_start[b]; q < e && excl < max_subs; q += maxsub) {
+        sub_bin[excl] = b;
+        sub_start[excl] = q;
+        ++excl;
+      }
+    }
   }
 }
 
-int64_t scan_blocks(int64_t n) { return (n + kScanTile - 1) / kScanTile; }
-
-cudaError_t exclusive_scan(const int* in, int* out, int64_t n, int* block_sums, cudaStream_t st) {
-  if (n <= 0) return cudaSuccess;
-  int64_t nb = scan_blocks(n);
-  k_scan_reduce<<<(unsigned)nb, kScanBlock, 0, st>>>(in, n, block_sums);
-  k_scan_sums<<<1, kScanBlock, 0, st>>>(block_sums, (int)nb);
-  k_scan_apply<<<(unsigned)nb, kScanBlock, 0, st>>>(in, n, block_sums, out);
-  return cudaGetLastError();
+__global__ void k_keys_to_bins(const int* __restrict__ K, int64_t M, int cbits, int* __restrict__ out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < M; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = K[i] >> cbits;
 }
 
 // ---------------------------------------------------------------------------
 
+// Key layout (cell bits, total bits), the number of passes and the digit width.
+void radix_plan(int nbins, int ncell, int& cbits, int& bits, int& npass, int& dbits) {
+  cbits = 0;
+  while ((1 << cbits) < ncell) ++cbits;
+  int bbits = 0;
+  while ((1 << bbits) < nbins) ++bbits;
+  bits = cbits + bbits > 0 ? cbits + bbits : 1;
+  npass = bits <= 11 ? 1 : (bits <= 22 ? 2 : 3);
+  dbits = (bits + npass - 1) / npass;
+}
+
+int radix_chunk() { return kRadixChunk; }
+
+cudaError_t bin_keys_of(const SortLayout& L, const int* K, int* out, cudaStream_t st) {
+  if (L.M == 0) return cudaSuccess;
+  const int grid = (int)std::min<int64_t>((L.M + 255) / 256, (int64_t)num_sms() * 8);
+  k_keys_to_bins<<<grid, 256, 0, st>>>(K, L.M, L.cbits, out);
+  return cudaGetLastError();
+}
+
 template <typename T>
 cudaError_t launch_sort(const SortLayout& L, const Geom& g, int ns, const void* x, const void* y, const void* z,
                         int64_t M, const SortPtrs& P, cudaStream_t st) {
-  const int ncell = g.tile[0] * g.tile[1] * g.tile[2];
-  const size_t cell_smem = (size_t)ncell * sizeof(int);
-  const size_t bin_smem = (size_t)g.nbins * sizeof(int);
-  cudaError_t e = ensure_smem(reinterpret_cast<const void*>(k_bin_count<T>), cell_smem);
-  if (e == cudaSuccess) e = ensure_smem(reinterpret_cast<const void*>(k_key_count), bin_smem);
-  if (e == cudaSuccess)
-    e = ensure_smem(reinterpret_cast<const void*>(k_bin_scatter),
-                    L.sort_smem > L.sort_smem_cell ? L.sort_smem : L.sort_smem_cell);
-  if (e != cudaSuccess) return e;
-  // pass A: stable by cell-in-tile (carrying each point's bin key along)
-  k_bin_count<T><<<(unsigned)L.nchunks, 256, cell_smem, st>>>((const T*)x, (const T*)y, (const T*)z, M, g, ns / 2,
-                                                              L.chunk, L.nchunks, ncell, P.keys, P.keys_cell,
-                                                              P.counts);
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
-  e = exclusive_scan(P.counts, P.counts, (int64_t)ncell * L.nchunks, P.scan_tmp, st);
-  if (e != cudaSuccess) return e;
-  k_bin_scatter<<<(unsigned)L.nchunks, L.sort_warps_cell * 32, L.sort_smem_cell, st>>>(
-      P.keys_cell, nullptr, P.keys, M, ncell, L.chunk, L.nchunks, P.counts, P.perm_cell, P.keys_by_cell);
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
-  // pass B: stable by bin over the cell-ordered sequence
-  k_key_count<<<(unsigned)L.nchunks, 256, bin_smem, st>>>(P.keys_by_cell, M, g.nbins, L.chunk, L.nchunks, P.counts);
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
-  e = exclusive_scan(P.counts, P.counts, (int64_t)g.nbins * L.nchunks, P.scan_tmp, st);
-  if (e != cudaSuccess) return e;
-  k_bin_scatter<<<(unsigned)L.nchunks, L.sort_warps * 32, L.sort_smem, st>>>(
-      P.keys_by_cell, P.perm_cell, nullptr, M, g.nbins, L.chunk, L.nchunks, P.counts, P.perm, nullptr);
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
-  k_subproblems<<<1, 1024, 0, st>>>(P.counts, g.nbins, L.nchunks, (int)M, L.maxsub, P.bin_start, P.sub_bin,
-                                    P.sub_start, P.nsub);
+  const int B = 1 << L.dbits;
+  cudaError_t e = cudaSuccess;
+  if (M > 0) {
+    const size_t hist_smem = (size_t)B * sizeof(int);
+    // digits per thread of the scatter: 2^dbits / 256, at least 1
+    auto scatter = B <= kRadixThreads ? k_radix_scatter<1>
+                                      : (B <= 2 * kRadixThreads ? k_radix_scatter<2>
+                                                                : (B <= 4 * kRadixThreads ? k_radix_scatter<4>
+                                                                                          : k_radix_scatter<8>));
+    e = ensure_smem(reinterpret_cast<const void*>(scatter), radix_smem_bytes(B));
+    if (e == cudaSuccess) e = prefer_max_smem(reinterpret_cast<const void*>(scatter));
+    if (e != cudaSuccess) return e;
+    const unsigned scan_grid = (unsigned)((B + kScanDigits - 1) / kScanDigits);
+    auto keys = g.dim == 1 ? k_sort_keys<T, 1> : (g.dim == 2 ? k_sort_keys<T, 2> : k_sort_keys<T, 3>);
+    keys<<<L.nchunks, kRadixThreads, hist_smem, st>>>((const T*)x, (const T*)y, (const T*)z, (int)M, g, ns / 2,
+                                                      L.cbits, L.dbits, P.keys, P.counts);
+    // ping-pong so that the last pass writes (keys_sorted, perm)
+    const int* kin = P.keys;
+    const int* vin = nullptr;
+    for (int ps = 0; ps < L.npass; ++ps) {
+      const int shift = ps * L.dbits;
+      if (ps > 0) k_digit_count<<<L.nchunks, kRadixThreads, hist_smem, st>>>(kin, (int)M, shift, L.dbits, P.counts);
+      k_col_scan<<<scan_grid, kScanDigits * kScanGroups, 0, st>>>(P.counts, L.nchunks, B, P.totals);
+      const bool to_final = ((L.npass - 1 - ps) % 2) == 0;
+      int* kout = to_final ? P.keys_sorted : P.keys_tmp;
+      int* vout = to_final ? P.perm : P.vals_tmp;
+      scatter<<<L.nchunks, kRadixThreads, radix_smem_bytes(B), st>>>(kin, vin, (int)M, shift, L.dbits, P.counts,
+                                                                     P.totals, kout, vout);
+      kin = kout;
+      vin = vout;
+    }
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  const int bgrid = (int)std::max<int64_t>(1, std::min<int64_t>((M / 4 + 256) / 256, (int64_t)num_sms() * 8));
+  k_bin_bounds<<<bgrid, 256, 0, st>>>(P.keys_sorted, (int)M, L.cbits, g.nbins, P.bin_start);
+  const int max_subs = (int)std::min<int64_t>(L.max_subs, INT32_MAX);
+  const size_t sub_smem = g.nbins <= kSubSmemBins ? (size_t)(g.nbins + 1) * sizeof(int) : 0;
+  k_subproblems<<<1, 1024, sub_smem, st>>>(P.bin_start, g.nbins, L.maxsub, max_subs, P.sub_bin, P.sub_start,
+                                           P.nsub);
   return cudaGetLastError();
 }
 

@@ -52,18 +52,26 @@ struct PointArgs {
 
 // The NS weights of one axis: w[q] = phi(i0 + q - xs).  float with a fitted
 // polynomial: Horner in v = 2 (xs - i0) - (NS - 1) (exact in float: xs - i0 is
-// exact because xs and i0 are within NS of each other and i0 is an integer);
-// otherwise exp/sqrt (nufftax/core/kernel.py:79-111).
+// exact because xs and i0 are within NS of each other and i0 is an integer),
+// degree kPolyEvalDeg, two weights per paired FMA, each coefficient a fixed
+// offset in the argument block; otherwise exp/sqrt (nufftax/core/kernel.py:79-111).
 template <typename T, int NS>
 __device__ __forceinline__ void axis_weights(const PointArgs<T>& a, int i0, T xs, T* w) {
   if (std::is_same<T, float>::value && a.poly.deg > 0) {
     const float v = 2.0f * (float)(xs - (T)i0) - (float)(NS - 1);
+    const float2 vv = make_float2(v, v);
+    float2 h[(NS + 1) / 2];
 #pragma unroll
-    for (int q = 0; q < NS; ++q) w[q] = (T)a.poly.a[q][a.poly.deg];
-    for (int d = a.poly.deg - 1; d >= 0; --d) {
+    for (int q = 0; q < NS; q += 2)
+      h[q / 2] = make_float2(a.poly.a[q][kPolyEvalDeg], q + 1 < NS ? a.poly.a[q + 1][kPolyEvalDeg] : 0.0f);
 #pragma unroll
-      for (int q = 0; q < NS; ++q) w[q] = (T)fmaf((float)w[q], v, a.poly.a[q][d]);
+    for (int d = kPolyEvalDeg - 1; d >= 0; --d) {
+#pragma unroll
+      for (int q = 0; q < NS; q += 2)
+        h[q / 2] = fma2(h[q / 2], vv, make_float2(a.poly.a[q][d], q + 1 < NS ? a.poly.a[q + 1][d] : 0.0f));
     }
+#pragma unroll
+    for (int q = 0; q < NS; ++q) w[q] = (T)((q & 1) ? h[q / 2].y : h[q / 2].x);
   } else {
 #pragma unroll
     for (int q = 0; q < NS; ++q) w[q] = es_weight(rn_sub((T)(i0 + q), xs), a.beta, a.kc);
@@ -93,9 +101,255 @@ __device__ __forceinline__ T coord(const PointArgs<T>& a, int d, int p) {
 // ---------------------------------------------------------------------------
 // Spread
 // ---------------------------------------------------------------------------
+
+// Adds a finished padded tile (planar) into the fine grid, one vectorised red
+// per non-zero cell: one warp per tile row, lanes along x (coalesced); periodic
+// wrap applied here.
+template <typename T>
+__device__ __forceinline__ void flush_tile(const Geom& g, const int o[3], const T* s_re, const T* s_im,
+                                           cplx_t<T>* __restrict__ out) {
+  const int row = g.pitch;
+  const int plane = g.pitch * g.pad[1];
+  const int nrows = g.pad[1] * g.pad[2];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int r = warp; r < nrows; r += nw) {
+    const int ly = r % g.pad[1];
+    const int lz = r / g.pad[1];
+    const int gy = wrap_up(o[1] + ly, g.nf[1]);
+    const int gz = wrap_up(o[2] + lz, g.nf[2]);
+    cplx_t<T>* dst = out + ((int64_t)gz * g.nf[1] + gy) * g.nf[0];
+    const T* sr = s_re + lz * plane + ly * row;
+    const T* si = s_im + lz * plane + ly * row;
+    for (int lx = lane; lx < g.pad[0]; lx += 32) {
+      const T vr = sr[lx], vi = si[lx];
+      if (vr != (T)0 || vi != (T)0) {
+        cplx_t<T> v;
+        v.x = vr;
+        v.y = vi;
+        red_add(dst + wrap_up(o[0] + lx, g.nf[0]), v);
+      }
+    }
+  }
+}
+
+// Folds a point's coordinates xv, computes its tile offset and per-axis
+// weights.  Returns false for a point outside its bin's tile (possible only
+// when coordinates changed after the sort: such a point is dropped instead of
+// indexing out of the tile).
+template <typename T, int DIM, int NS>
+__device__ __forceinline__ bool footprint(const PointArgs<T>& a, const T (&xv)[DIM], const int o[3], int row,
+                                          int plane, int& off, T (&w)[DIM][NS]) {
+  const Geom& g = a.g;
+  bool inside = true;
+  off = 0;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    const T xs = scaled_coord(xv[d], g.nf[d], g.prenorm);
+    const int i0 = left_cell<T, NS>(xs);
+    const int l = wrap_index(i0, g.nf[d]) - o[d];
+    inside = inside && (unsigned)l < (unsigned)g.tile[d];
+    off += l * (d == 0 ? 1 : (d == 1 ? row : plane));
+    axis_weights<T, NS>(a, i0, xs, w[d]);
+  }
+  return inside;
+}
+
+template <typename T, int DIM>
+__device__ __forceinline__ void load_coords(const PointArgs<T>& a, int p, T (&xv)[DIM]) {
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) xv[d] = coord(a, d, p);
+}
+
+template <typename T, int DIM, int NS>
+__device__ __forceinline__ bool point_footprint(const PointArgs<T>& a, int p, const int o[3], int row, int plane,
+                                                int& off, T (&w)[DIM][NS]) {
+  T xv[DIM];
+  load_coords<T, DIM>(a, p, xv);
+  return footprint<T, DIM, NS>(a, xv, o, row, plane, off, w);
+}
+
+// Run-merging spread (2D/3D, footprints of at least 32 cells).  Each warp walks
+// a contiguous, cell-ordered slice of the subproblem 32 points at a time: every
+// lane stages one point (c * w_x, the y and z weights) in a shared slot, then
+// the warp takes the 32 points one after another with lane l accumulating, in
+// registers, footprint column kx = l % ns of rows grp*rpl .. grp*rpl + rpl - 1
+// (grp = l / ns).  Consecutive points in the same cell share the footprint, so
+// the registers reach shared memory (atomics, distinct addresses within an
+// instruction) only when the cell changes; where the runs start is one ballot
+// per batch, so the walk itself waits on no shared load for its branches.  The
+// next batch's point indices, coordinates and strengths are fetched while the
+// current batch is walked.
 template <typename T, int DIM, int NS, int NW>
-__device__ __forceinline__ void spread_subproblem(const PointArgs<T>& a, const cplx_t<T>* __restrict__ c,
-                                                  cplx_t<T>* __restrict__ fw, int sidx, unsigned char* smem_raw) {
+__device__ __forceinline__ void spread_subproblem_runs(const PointArgs<T>& a, const cplx_t<T>* __restrict__ c,
+                                                       cplx_t<T>* __restrict__ fw, int sidx, unsigned char* smem_raw) {
+  using CT = cplx_t<T>;
+  constexpr int G = run_groups(NS);
+  constexpr int RPL = run_rows_per_lane(DIM, NS);
+  constexpr int NR = run_rows(DIM, NS);
+  constexpr int WY = run_wy(DIM, NS);
+  constexpr int WZ = run_wz(DIM, NS);
+  constexpr int SLOT = run_slot_reals(DIM, NS);
+  static_assert(SLOT > 0, "run-merging layout does not apply");
+  constexpr int YOFF = 2 * NS;       // y weights within a slot
+  constexpr int ZOFF = 2 * NS + WY;  // z weights within a slot (3D)
+  const Geom& g = a.g;
+  const int tile_cells = g.pad[2] * g.pad[1] * g.pitch;
+  T* s_re = reinterpret_cast<T*>(smem_raw);
+  T* s_im = s_re + tile_cells;
+  T* s_st = s_im + tile_cells;  // [NW*32][SLOT]
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const int row = g.pitch;
+  const int plane = g.pitch * g.pad[1];
+  // this lane's column and row group; lanes past the groups mirror the last
+  // group's loads and never flush
+  const int kx = lane % NS;
+  const bool lane_on = lane / NS < G;
+  const int grp = lane_on ? lane / NS : G - 1;
+  T* my_slot = s_st + (warp * 32 + lane) * SLOT;
+  const T* warp_slots = s_st + warp * 32 * SLOT;
+
+  const int b = a.s.sub_bin[sidx];
+  const int k0 = a.s.sub_start[sidx];
+  const int k1 = min(k0 + a.s.maxsub, a.s.bin_start[b + 1]);
+  int o[3];
+  bin_origin(g, b, o[0], o[1], o[2]);
+  for (int t = 0; t < a.n_trans; ++t) {
+    const CT* ct = c + (int64_t)t * a.M;
+    for (int i = threadIdx.x; i < 2 * tile_cells; i += blockDim.x) s_re[i] = (T)0;
+    __syncthreads();
+    const int per = ((k1 - k0 + NW - 1) / NW + 31) / 32 * 32;
+    const int w0 = min(k0 + warp * per, k1);
+    const int w1 = min(w0 + per, k1);
+    CT acc[RPL];
+#pragma unroll
+    for (int r = 0; r < RPL; ++r) acc[r].x = acc[r].y = (T)0;
+    int run_off = -1;
+    auto flush_run = [&]() {
+#pragma unroll
+      for (int r = 0; r < RPL; ++r) {
+        const int rho = grp * RPL + r;
+        if (lane_on && rho < NR) {
+          const int addr = run_off + (DIM == 3 ? (rho / NS) * plane + (rho % NS) * row : rho * row) + kx;
+          atomicAdd(&s_re[addr], acc[r].x);
+          atomicAdd(&s_im[addr], acc[r].y);
+        }
+        acc[r].x = acc[r].y = (T)0;
+      }
+    };
+    // software pipeline: coordinates and strength of this lane's point in the
+    // current batch (xn, cn) and the point index of the next batch (pn)
+    T xn[DIM];
+    CT cn;
+    cn.x = cn.y = (T)0;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) xn[d] = (T)0;
+    int pn = w0 + lane < w1 ? a.s.perm[w0 + lane] : -1;
+    if (pn >= 0) {
+      load_coords<T, DIM>(a, pn, xn);
+      cn = ct[pn];
+    }
+    pn = w0 + 32 + lane < w1 ? a.s.perm[w0 + 32 + lane] : -1;
+    for (int kb = w0; kb < w1; kb += 32) {
+      const bool valid = kb + lane < w1;
+      T xv[DIM];
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) xv[d] = xn[d];
+      CT cv = cn;
+      if (pn >= 0) {  // next batch
+        load_coords<T, DIM>(a, pn, xn);
+        cn = ct[pn];
+      }
+      pn = kb + 64 + lane < w1 ? a.s.perm[kb + 64 + lane] : -1;
+      int off = 0;
+      if (valid) {
+        T w[DIM][NS];
+        const bool inside = footprint<T, DIM, NS>(a, xv, o, row, plane, off, w);
+        if (!inside) {
+          cv.x = cv.y = (T)0;
+          off = 0;
+        }
+#pragma unroll
+        for (int q = 0; q < NS; ++q) {
+          CT v;
+          v.x = cv.x * w[0][q];
+          v.y = cv.y * w[0][q];
+          reinterpret_cast<CT*>(my_slot)[q] = v;
+        }
+#pragma unroll
+        for (int q = 0; q < WY; q += 2) {
+          CT v;
+          v.x = q < NS ? w[1][q] : (T)0;
+          v.y = q + 1 < NS ? w[1][q + 1] : (T)0;
+          reinterpret_cast<CT*>(my_slot + YOFF)[q / 2] = v;
+        }
+        if constexpr (DIM == 3) {
+#pragma unroll
+          for (int q = 0; q < WZ; q += 2) {
+            CT v;
+            v.x = q < NS ? w[2][q] : (T)0;
+            v.y = q + 1 < NS ? w[2][q + 1] : (T)0;
+            reinterpret_cast<CT*>(my_slot + ZOFF)[q / 2] = v;
+          }
+        }
+      }
+      // lane j starts a run when its cell differs from point j-1's
+      int prev = __shfl_up_sync(0xffffffffu, off, 1);
+      if (lane == 0) prev = run_off;
+      const unsigned starts = __ballot_sync(0xffffffffu, valid && off != prev);
+      __syncwarp();
+      const int cnt = min(32, w1 - kb);
+      for (int j = 0; j < cnt; ++j) {
+        if ((starts >> j) & 1u) {
+          if (run_off >= 0) flush_run();
+          run_off = __shfl_sync(0xffffffffu, off, j);
+        }
+        const T* sp = warp_slots + j * SLOT;
+        const CT cw = reinterpret_cast<const CT*>(sp)[kx];
+        T wr[RPL];
+        if constexpr (DIM == 2) {
+          const T* wy = sp + YOFF + grp * RPL;
+          if constexpr (RPL % 2 == 0) {
+#pragma unroll
+            for (int r = 0; r < RPL; r += 2) {
+              const CT pr = *reinterpret_cast<const CT*>(wy + r);
+              wr[r] = pr.x;
+              wr[r + 1] = pr.y;
+            }
+          } else {
+#pragma unroll
+            for (int r = 0; r < RPL; ++r) wr[r] = wy[r];
+          }
+        } else if constexpr (RPL % NS == 0) {
+          const T* wz = sp + ZOFF + grp * (RPL / NS);
+#pragma unroll
+          for (int r = 0; r < RPL; ++r) wr[r] = wz[r / NS] * sp[YOFF + r % NS];
+        } else {
+#pragma unroll
+          for (int r = 0; r < RPL; ++r) {
+            const int rho = grp * RPL + r;
+            wr[r] = sp[ZOFF + rho / NS] * sp[YOFF + rho % NS];
+          }
+        }
+#pragma unroll
+        for (int r = 0; r < RPL; ++r) acc[r] = fma_rc(wr[r], cw, acc[r]);
+      }
+      __syncwarp();
+    }
+    if (run_off >= 0) flush_run();
+    __syncthreads();
+    flush_tile<T>(g, o, s_re, s_im, fw + (int64_t)t * a.grid_stride);
+    __syncthreads();
+  }
+}
+
+// Spread of one subproblem, footprints below 32 cells (1D, small ns) or with
+// more than 16 rows a lane (3D, ns >= 9).  Points are staged 32 at a time per
+// warp (weights axis-major), then walked footprint cell by footprint cell with
+// shared-memory atomics on distinct addresses within each instruction.
+template <typename T, int DIM, int NS, int NW>
+__device__ __forceinline__ void spread_subproblem_cells(const PointArgs<T>& a, const cplx_t<T>* __restrict__ c,
+                                                        cplx_t<T>* __restrict__ fw, int sidx, unsigned char* smem_raw) {
   using CT = cplx_t<T>;
   constexpr int CELLS = Pow<NS, DIM>::value;
   constexpr int SW = NW * 32 + 1;  // staging stride: odd, so both the per-lane writes and
@@ -112,183 +366,100 @@ __device__ __forceinline__ void spread_subproblem(const PointArgs<T>& a, const c
   const int lane = threadIdx.x & 31;
   const int row = g.pitch;
   const int plane = g.pitch * g.pad[1];
-  const int used = g.pad[0] * g.pad[1] * g.pad[2];
-  {
-    const int b = a.s.sub_bin[sidx];
-    const int k0 = a.s.sub_start[sidx];
-    const int k1 = min(k0 + a.s.maxsub, a.s.bin_start[b + 1]);
-    int o[3];
-    bin_origin(g, b, o[0], o[1], o[2]);
-    for (int t = 0; t < a.n_trans; ++t) {
-      for (int i = threadIdx.x; i < 2 * tile_cells; i += blockDim.x) s_re[i] = (T)0;
-      __syncthreads();
-      // Each warp takes a contiguous slice of the subproblem, so the cell
-      // order of the points carries across its batches.
-      const int per = ((k1 - k0 + NW - 1) / NW + 31) / 32 * 32;
-      const int w0 = min(k0 + warp * per, k1);
-      const int w1 = min(w0 + per, k1);
-      constexpr int R = (CELLS + 31) / 32;
-      constexpr bool MERGE = CELLS >= 32 && R <= 16;
-      T accr[MERGE ? R : 1], acci[MERGE ? R : 1];
-      int run_off = -1;
+  const int b = a.s.sub_bin[sidx];
+  const int k0 = a.s.sub_start[sidx];
+  const int k1 = min(k0 + a.s.maxsub, a.s.bin_start[b + 1]);
+  int o[3];
+  bin_origin(g, b, o[0], o[1], o[2]);
+  for (int t = 0; t < a.n_trans; ++t) {
+    for (int i = threadIdx.x; i < 2 * tile_cells; i += blockDim.x) s_re[i] = (T)0;
+    __syncthreads();
+    const int per = ((k1 - k0 + NW - 1) / NW + 31) / 32 * 32;
+    const int w0 = min(k0 + warp * per, k1);
+    const int w1 = min(w0 + per, k1);
+    for (int kb = w0; kb < w1; kb += 32) {
+      const int k = kb + lane;
+      const int slot = warp * 32 + lane;
+      if (k < w1) {
+        const int p = a.s.perm[k];
+        int off;
+        T w[DIM][NS];
+        const bool inside = point_footprint<T, DIM, NS>(a, p, o, row, plane, off, w);
 #pragma unroll
-      for (int r = 0; r < (MERGE ? R : 1); ++r) accr[r] = acci[r] = (T)0;
-      for (int kb = w0; kb < w1; kb += 32) {
-        const int k = kb + lane;
-        const int slot = warp * 32 + lane;
-        if (k < w1) {
-          const int p = a.s.perm[k];
-          int off = 0;
-          bool inside = true;
+        for (int d = 0; d < DIM; ++d)
 #pragma unroll
-          for (int d = 0; d < DIM; ++d) {
-            const T xs = scaled_coord(coord(a, d, p), g.nf[d], g.prenorm);
-            const int i0 = left_cell<T, NS>(xs);
-            const int l = wrap_index(i0, g.nf[d]) - o[d];
-            // A point outside its bin's tile can only come from coordinates
-            // changed after the sort; it is dropped instead of indexing out of
-            // the tile.
-            inside = inside && (unsigned)l < (unsigned)g.tile[d];
-            off += l * (d == 0 ? 1 : (d == 1 ? row : plane));
-            T wq[NS];
-            axis_weights<T, NS>(a, i0, xs, wq);
-#pragma unroll
-            for (int q = 0; q < NS; ++q) s_w[(d * NS + q) * SW + slot] = wq[q];
-          }
-          const CT cv = c[(int64_t)t * a.M + p];
-          s_off[slot] = inside ? off : 0;
-          s_cr[slot] = inside ? cv.x : (T)0;
-          s_ci[slot] = inside ? cv.y : (T)0;
-        }
-        __syncwarp();
-        const int cnt = min(32, w1 - kb);
-        if constexpr (MERGE) {
-          // One point at a time, lane l on cells l, l+32, ...; consecutive
-          // points in the same cell add into registers and reach shared memory
-          // once per run.
-          for (int j = 0; j < cnt; ++j) {
-            const int sj = warp * 32 + j;
-            const int off = s_off[sj];
-            if (off != run_off) {
-              if (run_off >= 0) {
-#pragma unroll
-                for (int r = 0; r < R; ++r) {
-                  const int q = lane + 32 * r;
-                  if (CELLS % 32 == 0 || q < CELLS) {
-                    const int addr = run_off + (q / (NS * NS)) * plane + ((q / NS) % NS) * row + q % NS;
-                    atomicAdd(&s_re[addr], accr[r]);
-                    atomicAdd(&s_im[addr], acci[r]);
-                  }
-                  accr[r] = acci[r] = (T)0;
-                }
-              }
-              run_off = off;
-            }
-            const T cr = s_cr[sj], ci = s_ci[sj];
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-              const int q = lane + 32 * r;
-              if (CELLS % 32 == 0 || q < CELLS) {
-                const int kx = q % NS;
-                const int ky = (q / NS) % NS;
-                const int kz = q / (NS * NS);
-                T w;
-                if (DIM == 1)
-                  w = s_w[kx * SW + sj];
-                else if (DIM == 2)
-                  w = s_w[(NS + ky) * SW + sj] * s_w[kx * SW + sj];
-                else
-                  w = (s_w[(2 * NS + kz) * SW + sj] * s_w[(NS + ky) * SW + sj]) * s_w[kx * SW + sj];
-                accr[r] += cr * w;
-                acci[r] += ci * w;
-              }
-            }
-          }
-        } else if (CELLS >= 32) {
-          // large footprints: one point at a time, straight to shared memory
-          for (int j = 0; j < cnt; ++j) {
-            const int sj = warp * 32 + j;
-            const T cr = s_cr[sj], ci = s_ci[sj];
-            const int off = s_off[sj];
-#pragma unroll 4
-            for (int r = 0; r < R; ++r) {
-              const int q = lane + 32 * r;
-              if (CELLS % 32 == 0 || q < CELLS) {
-                const int kx = q % NS;
-                const int ky = (q / NS) % NS;
-                const int kz = q / (NS * NS);
-                T w;
-                if (DIM == 1)
-                  w = s_w[kx * SW + sj];
-                else if (DIM == 2)
-                  w = s_w[(NS + ky) * SW + sj] * s_w[kx * SW + sj];
-                else
-                  w = (s_w[(2 * NS + kz) * SW + sj] * s_w[(NS + ky) * SW + sj]) * s_w[kx * SW + sj];
-                const int addr = off + kz * plane + ky * row + kx;
-                atomicAdd(&s_re[addr], cr * w);
-                atomicAdd(&s_im[addr], ci * w);
-              }
-            }
-          }
-        } else {
-          // small footprints: several points per instruction
-          const int items = cnt * CELLS;
-          for (int it = lane; it < items; it += 32) {
-            const int j = it / CELLS;
-            const int q = it - j * CELLS;
-            const int kx = q % NS;
-            const int ky = (q / NS) % NS;
-            const int kz = q / (NS * NS);
-            const int sj = warp * 32 + j;
-            T w;
-            if (DIM == 1)
-              w = s_w[kx * SW + sj];
-            else if (DIM == 2)
-              w = s_w[(NS + ky) * SW + sj] * s_w[kx * SW + sj];
-            else
-              w = (s_w[(2 * NS + kz) * SW + sj] * s_w[(NS + ky) * SW + sj]) * s_w[kx * SW + sj];
-            const int addr = s_off[sj] + kz * plane + ky * row + kx;
-            atomicAdd(&s_re[addr], s_cr[sj] * w);
-            atomicAdd(&s_im[addr], s_ci[sj] * w);
-          }
-        }
-        __syncwarp();
+          for (int q = 0; q < NS; ++q) s_w[(d * NS + q) * SW + slot] = w[d][q];
+        const CT cv = c[(int64_t)t * a.M + p];
+        s_off[slot] = inside ? off : 0;
+        s_cr[slot] = inside ? cv.x : (T)0;
+        s_ci[slot] = inside ? cv.y : (T)0;
       }
-      if constexpr (MERGE) {
-        if (run_off >= 0) {
-#pragma unroll
+      __syncwarp();
+      const int cnt = min(32, w1 - kb);
+      if constexpr (CELLS >= 32) {
+        // large footprints: one point at a time, straight to shared memory
+        constexpr int R = (CELLS + 31) / 32;
+        for (int j = 0; j < cnt; ++j) {
+          const int sj = warp * 32 + j;
+          const T cr = s_cr[sj], ci = s_ci[sj];
+          const int off = s_off[sj];
+#pragma unroll 4
           for (int r = 0; r < R; ++r) {
             const int q = lane + 32 * r;
             if (CELLS % 32 == 0 || q < CELLS) {
-              const int addr = run_off + (q / (NS * NS)) * plane + ((q / NS) % NS) * row + q % NS;
-              atomicAdd(&s_re[addr], accr[r]);
-              atomicAdd(&s_im[addr], acci[r]);
+              const int kx = q % NS;
+              const int ky = (q / NS) % NS;
+              const int kz = q / (NS * NS);
+              T w;
+              if (DIM == 1)
+                w = s_w[kx * SW + sj];
+              else if (DIM == 2)
+                w = s_w[(NS + ky) * SW + sj] * s_w[kx * SW + sj];
+              else
+                w = (s_w[(2 * NS + kz) * SW + sj] * s_w[(NS + ky) * SW + sj]) * s_w[kx * SW + sj];
+              const int addr = off + kz * plane + ky * row + kx;
+              atomicAdd(&s_re[addr], cr * w);
+              atomicAdd(&s_im[addr], ci * w);
             }
           }
         }
-      }
-      __syncthreads();
-      CT* out = fw + (int64_t)t * a.grid_stride;
-      for (int i = threadIdx.x; i < used; i += blockDim.x) {
-        const int lx = i % g.pad[0];
-        const int r = i / g.pad[0];
-        const int ly = r % g.pad[1];
-        const int lz = r / g.pad[1];
-        const int si = lz * plane + ly * row + lx;
-        const T vr = s_re[si], vi = s_im[si];
-        if (vr != (T)0 || vi != (T)0) {
-          const int gx = wrap_up(o[0] + lx, g.nf[0]);
-          const int gy = wrap_up(o[1] + ly, g.nf[1]);
-          const int gz = wrap_up(o[2] + lz, g.nf[2]);
-          CT v;
-          v.x = vr;
-          v.y = vi;
-          red_add(out + ((int64_t)gz * g.nf[1] + gy) * g.nf[0] + gx, v);
+      } else {
+        // small footprints: several points per instruction
+        const int items = cnt * CELLS;
+        for (int it = lane; it < items; it += 32) {
+          const int j = it / CELLS;
+          const int q = it - j * CELLS;
+          const int kx = q % NS;
+          const int ky = (q / NS) % NS;
+          const int kz = q / (NS * NS);
+          const int sj = warp * 32 + j;
+          T w;
+          if (DIM == 1)
+            w = s_w[kx * SW + sj];
+          else if (DIM == 2)
+            w = s_w[(NS + ky) * SW + sj] * s_w[kx * SW + sj];
+          else
+            w = (s_w[(2 * NS + kz) * SW + sj] * s_w[(NS + ky) * SW + sj]) * s_w[kx * SW + sj];
+          const int addr = s_off[sj] + kz * plane + ky * row + kx;
+          atomicAdd(&s_re[addr], s_cr[sj] * w);
+          atomicAdd(&s_im[addr], s_ci[sj] * w);
         }
       }
-      __syncthreads();
+      __syncwarp();
     }
+    __syncthreads();
+    flush_tile<T>(g, o, s_re, s_im, fw + (int64_t)t * a.grid_stride);
+    __syncthreads();
   }
+}
+
+template <typename T, int DIM, int NS, int NW>
+__device__ __forceinline__ void spread_subproblem(const PointArgs<T>& a, const cplx_t<T>* __restrict__ c,
+                                                  cplx_t<T>* __restrict__ fw, int sidx, unsigned char* smem_raw) {
+  if constexpr (run_slot_reals(DIM, NS) > 0)
+    spread_subproblem_runs<T, DIM, NS, NW>(a, c, fw, sidx, smem_raw);
+  else
+    spread_subproblem_cells<T, DIM, NS, NW>(a, c, fw, sidx, smem_raw);
 }
 
 template <typename T, int DIM, int NS, int NW>
@@ -370,13 +541,11 @@ __device__ __forceinline__ void interp_subproblem(const PointArgs<T>& a, const c
 #pragma unroll
           for (int ky = 0; ky < (DIM >= 2 ? NS : 1); ++ky) {
             const CT* rp = base + kz * plane + ky * row;
-            T xr = 0, xi = 0;
+            CT xa;
+            xa.x = xa.y = (T)0;
 #pragma unroll
-            for (int kx = 0; kx < NS; ++kx) {
-              const CT v = rp[kx];
-              xr += v.x * w[0][kx];
-              xi += v.y * w[0][kx];
-            }
+            for (int kx = 0; kx < NS; ++kx) xa = fma_rc(w[0][kx], rp[kx], xa);
+            const T xr = xa.x, xi = xa.y;
             if (DIM >= 2) {
               zr += xr * w[DIM >= 2 ? 1 : 0][ky];
               zi += xi * w[DIM >= 2 ? 1 : 0][ky];
@@ -521,15 +690,15 @@ __global__ void __launch_bounds__(NW * 32) k_grad(PointArgs<T> a, const cplx_t<T
 #pragma unroll
           for (int ky = 0; ky < (DIM >= 2 ? NS : 1); ++ky) {
             const CT* rp = base + kz * plane + ky * row;
-            T xr = 0, xi = 0, xr1 = 0, xi1 = 0;
+            CT xa, xa1;
+            xa.x = xa.y = xa1.x = xa1.y = (T)0;
 #pragma unroll
             for (int kx = 0; kx < NS; ++kx) {
               const CT v = rp[kx];
-              xr += v.x * w[0][kx];
-              xi += v.y * w[0][kx];
-              xr1 += v.x * dw[0][kx];
-              xi1 += v.y * dw[0][kx];
+              xa = fma_rc(w[0][kx], v, xa);
+              xa1 = fma_rc(dw[0][kx], v, xa1);
             }
+            const T xr = xa.x, xi = xa.y, xr1 = xa1.x, xi1 = xa1.y;
             if (DIM >= 2) {
               const T wy = w[DIM >= 2 ? 1 : 0][ky], dwy = dw[DIM >= 2 ? 1 : 0][ky];
               zr0 += xr * wy;

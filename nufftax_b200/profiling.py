@@ -17,7 +17,7 @@ import torch
 _state = threading.local()
 
 # kernels launched by one call of each library entry point
-LAUNCHES = {"nfx_sort_points": 11, "nfx_spread_sorted": 1, "nfx_interp_sorted": 1, "nfx_spread_grad_sorted": 1,
+LAUNCHES = {"nfx_sort_points": 8, "nfx_spread_sorted": 1, "nfx_interp_sorted": 1, "nfx_spread_grad_sorted": 1,
             "nfx_interp_grad_sorted": 1, "nfx_deconv_shuffle": 1, "nfx_deconv_pad": 1, "nfx_t3_prepare": 0,
             "nfx_t3_finish": 1, "nfx_fft": 0}
 
