@@ -103,28 +103,35 @@ constexpr int warps_per_cta(size_t real_bytes, int dim, int ns) { return (real_b
 // Run-merging spread layout (2D/3D footprints of at least 32 cells): lane l of
 // a warp owns footprint column kx = l % ns and rows (y, or z*ns + y) grp*rpl ..
 // grp*rpl + rpl - 1 with grp = l / ns; the 32 / ns groups cover the ns^(dim-1)
-// rows.  A staged point is one slot of reals: c * w_x (ns complex), then the
-// y weights (padded to the rows the groups reach), then the z weights (3D),
-// each section an even number of reals so that it is written and read in
-// complex-sized pairs.  The slot length is 2 mod 4 reals: the pair stores of a
-// warp (one slot per lane) then hit distinct banks.  run_slot_reals is 0 when
-// the layout does not apply (1D, small footprints, more than 16 rows a lane).
+// rows.  A staged point is one slot of reals: c * w_x (ns complex), then the y
+// weights and (3D) the z weights.  Sections are padded to the rows the groups
+// reach and to whole 16-byte chunks; the slot length (4 mod 8 floats, 2 mod 4
+// doubles) makes the 16-byte stores of a warp (one slot per lane) hit distinct
+// banks.  The walk reads the weights with scalar loads: every lane of a group
+// reads the same word (one broadcast wavefront), which keeps the shared-memory
+// pipe less busy than wider loads would.
+// run_slot_reals is 0 when the layout does not apply (1D, small footprints,
+// more than 16 rows a lane).
 __host__ __device__ constexpr int run_groups(int ns) { return 32 / ns; }
 __host__ __device__ constexpr int run_rows(int dim, int ns) { return dim == 3 ? ns * ns : ns; }
 __host__ __device__ constexpr int run_rows_per_lane(int dim, int ns) {
   return (run_rows(dim, ns) + run_groups(ns) - 1) / run_groups(ns);
 }
-__host__ __device__ constexpr int round_even(int n) { return (n + 1) / 2 * 2; }
+__host__ __device__ constexpr int round4(int n) { return (n + 3) / 4 * 4; }
+// reals of the y and z sections
 __host__ __device__ constexpr int run_wy(int dim, int ns) {
-  return round_even(dim == 2 ? run_groups(ns) * run_rows_per_lane(dim, ns) : ns);
+  return dim == 2 ? round4(run_groups(ns) * run_rows_per_lane(dim, ns)) : round4(ns);
 }
 __host__ __device__ constexpr int run_wz(int dim, int ns) {
-  return dim == 3 ? round_even((run_groups(ns) * run_rows_per_lane(dim, ns) + ns - 1) / ns) : 0;
+  return dim == 3 ? round4((run_groups(ns) * run_rows_per_lane(dim, ns) + ns - 1) / ns) : 0;
 }
-__host__ __device__ constexpr int run_slot_base(int dim, int ns) { return 2 * ns + run_wy(dim, ns) + run_wz(dim, ns); }
-__host__ __device__ constexpr int run_slot_reals(int dim, int ns) {
+__host__ __device__ constexpr int run_slot_base(int dim, int ns) {
+  return round4(2 * ns) + run_wy(dim, ns) + run_wz(dim, ns);
+}
+__host__ __device__ constexpr int run_slot_reals(int dim, int ns, int real_bytes) {
   return (dim >= 2 && run_rows(dim, ns) * ns >= 32 && run_rows_per_lane(dim, ns) <= 16)
-             ? run_slot_base(dim, ns) + (run_slot_base(dim, ns) % 4 == 0 ? 2 : 0)
+             ? (real_bytes == 4 ? run_slot_base(dim, ns) + (run_slot_base(dim, ns) % 8 == 0 ? 4 : 0)
+                                : run_slot_base(dim, ns) + 2)
              : 0;
 }
 
@@ -134,8 +141,8 @@ __host__ __device__ constexpr int run_slot_reals(int dim, int ns) {
 inline size_t spread_smem_bytes(size_t real_bytes, int dim, int ns, const Geom& g) {
   const int nw = warps_per_cta(real_bytes, dim, ns);
   const size_t tile = 2 * real_bytes * (size_t)g.pad[2] * g.pad[1] * g.pitch;
-  const int slot = run_slot_reals(dim, ns);
-  if (slot > 0) return tile + (size_t)nw * 32 * slot * real_bytes;
+  const int slot = run_slot_reals(dim, ns, (int)real_bytes);
+  if (slot > 0) return ((tile + 15) & ~(size_t)15) + (size_t)nw * 32 * slot * real_bytes;  // 16-byte aligned slots
   return tile + ((size_t)dim * ns * (nw * 32 + 1) + (size_t)2 * nw * 32) * real_bytes + (size_t)nw * 32 * sizeof(int);
 }
 inline size_t tile_smem_bytes(size_t real_bytes, const Geom& g) {

@@ -8,10 +8,13 @@
 //  * spread (nufftax/core/spread.py:285-339, 435-494, 596-658; Pallas twin
 //    nufftax/core/pallas_spread.py:337-613): points are staged 32 at a time per
 //    warp (each lane folds one point and evaluates its d*ns ES weights once);
-//    the warp then walks the 32 footprints cell by cell, lane l taking cells
-//    l, l+32, ... of the same point, so every shared-memory atomic of one
-//    instruction hits a distinct address (no same-address serialisation even for
-//    heavily clustered points).  The finished tile is flushed with one vectorised
+//    the warp then walks the 32 footprints one after another.  For 2D/3D
+//    footprints of at least 32 cells each lane owns one footprint column and a
+//    block of rows and sums consecutive same-cell points in registers
+//    (spread_subproblem_runs); smaller footprints go cell by cell with
+//    shared-memory atomics (spread_subproblem_cells).  Every shared-memory
+//    atomic of one instruction hits a distinct address, so clustered points do
+//    not serialise.  The finished tile is flushed with one vectorised
 //    `red.global.add.v2.f32` per non-zero cell, coalesced along x.
 //  * interp (nufftax/core/spread.py:342-381, 497-540, 661-709): the padded tile
 //    is staged into shared memory with coalesced loads, then each thread
@@ -168,17 +171,94 @@ __device__ __forceinline__ bool point_footprint(const PointArgs<T>& a, int p, co
   return footprint<T, DIM, NS>(a, xv, o, row, plane, off, w);
 }
 
+// Slot helpers of the run-merging spread: 16-byte chunks of four floats or two
+// doubles (slots are 16-byte aligned, see run_slot_reals).
+__device__ __forceinline__ void store16(float* p, float a, float b, float c, float d) {
+  *reinterpret_cast<float4*>(p) = make_float4(a, b, c, d);
+}
+__device__ __forceinline__ void store16(double* p, double a, double b) {
+  *reinterpret_cast<double2*>(p) = make_double2(a, b);
+}
+
+// Writes one point's slot: c * w_x, then the y weights and (3D) the z
+// weights; padding entries are zero.
+template <typename T, int DIM, int NS>
+__device__ __forceinline__ void stage_slot(T* sp, cplx_t<T> cv, const T (&w)[DIM][NS]) {
+  constexpr int WY = run_wy(DIM, NS);
+  constexpr int WZ = run_wz(DIM, NS);
+  constexpr int YOFF = round4(2 * NS);
+  constexpr int ZOFF = YOFF + WY;
+  static_assert(NS % 2 == 0, "even widths only");
+  if constexpr (sizeof(T) == 4) {
+#pragma unroll
+    for (int q = 0; q < NS; q += 2)
+      store16(sp + 2 * q, cv.x * w[0][q], cv.y * w[0][q], cv.x * w[0][q + 1], cv.y * w[0][q + 1]);
+#pragma unroll
+    for (int q = 0; q < WY; q += 4)
+      store16(sp + YOFF + q, q < NS ? w[1][q] : (T)0, q + 1 < NS ? w[1][q + 1] : (T)0,
+              q + 2 < NS ? w[1][q + 2] : (T)0, q + 3 < NS ? w[1][q + 3] : (T)0);
+    if constexpr (DIM == 3) {
+#pragma unroll
+      for (int q = 0; q < WZ; q += 4)
+        store16(sp + ZOFF + q, q < NS ? w[DIM - 1][q] : (T)0, q + 1 < NS ? w[DIM - 1][q + 1] : (T)0,
+                q + 2 < NS ? w[DIM - 1][q + 2] : (T)0, q + 3 < NS ? w[DIM - 1][q + 3] : (T)0);
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < NS; ++q) store16(sp + 2 * q, cv.x * w[0][q], cv.y * w[0][q]);
+#pragma unroll
+    for (int q = 0; q < WY; q += 2)
+      store16(sp + YOFF + q, q < NS ? w[1][q] : (T)0, q + 1 < NS ? w[1][q + 1] : (T)0);
+    if constexpr (DIM == 3) {
+#pragma unroll
+      for (int q = 0; q < WZ; q += 2)
+        store16(sp + ZOFF + q, q < NS ? w[DIM - 1][q] : (T)0, q + 1 < NS ? w[DIM - 1][q + 1] : (T)0);
+    }
+  }
+}
+
+// Adds one staged point to this lane's accumulators: acc[r] += w_row(r) * (c w_x),
+// w_row the y weight of row r (2D) or z weight * y weight (3D).
+template <typename T, int DIM, int NS>
+__device__ __forceinline__ void add_slot(const T* sp, int kx, int grp, cplx_t<T> (&acc)[run_rows_per_lane(DIM, NS)]) {
+  using CT = cplx_t<T>;
+  constexpr int RPL = run_rows_per_lane(DIM, NS);
+  constexpr int WY = run_wy(DIM, NS);
+  constexpr int YOFF = round4(2 * NS);
+  constexpr int ZOFF = YOFF + WY;
+  const CT cw = reinterpret_cast<const CT*>(sp)[kx];
+  if constexpr (DIM == 2) {
+    const T* wy = sp + YOFF + grp * RPL;
+#pragma unroll
+    for (int r = 0; r < RPL; ++r) acc[r] = fma_rc(wy[r], cw, acc[r]);
+  } else if constexpr (RPL % NS == 0) {
+    const T* wz = sp + ZOFF + grp * (RPL / NS);
+#pragma unroll
+    for (int zz = 0; zz < RPL / NS; ++zz) {
+      const T z = wz[zz];
+#pragma unroll
+      for (int q = 0; q < NS; ++q) acc[zz * NS + q] = fma_rc(z * sp[YOFF + q], cw, acc[zz * NS + q]);
+    }
+  } else {
+#pragma unroll
+    for (int r = 0; r < RPL; ++r) {
+      const int rho = grp * RPL + r;
+      acc[r] = fma_rc(sp[ZOFF + rho / NS] * sp[YOFF + rho % NS], cw, acc[r]);
+    }
+  }
+}
+
 // Run-merging spread (2D/3D, footprints of at least 32 cells).  Each warp walks
 // a contiguous, cell-ordered slice of the subproblem 32 points at a time: every
-// lane stages one point (c * w_x, the y and z weights) in a shared slot, then
-// the warp takes the 32 points one after another with lane l accumulating, in
-// registers, footprint column kx = l % ns of rows grp*rpl .. grp*rpl + rpl - 1
-// (grp = l / ns).  Consecutive points in the same cell share the footprint, so
-// the registers reach shared memory (atomics, distinct addresses within an
-// instruction) only when the cell changes; where the runs start is one ballot
-// per batch, so the walk itself waits on no shared load for its branches.  The
-// next batch's point indices, coordinates and strengths are fetched while the
-// current batch is walked.
+// lane stages one point in a shared slot (stage_slot), then the warp takes the
+// 32 points one after another with lane l accumulating, in registers,
+// footprint column kx = l % ns of rows grp*rpl .. grp*rpl + rpl - 1
+// (grp = l / ns; add_slot).  Consecutive points in the same cell share the
+// footprint, so the registers reach shared memory (atomics, distinct addresses
+// within an instruction) only when the cell changes.  One ballot per batch
+// marks where runs start; the walk goes run by run, each run an unrolled loop
+// with no branch per point.  The next batch's point indices, coordinates and
+// strengths are fetched while the current batch is walked.
 template <typename T, int DIM, int NS, int NW>
 __device__ __forceinline__ void spread_subproblem_runs(const PointArgs<T>& a, const cplx_t<T>* __restrict__ c,
                                                        cplx_t<T>* __restrict__ fw, int sidx, unsigned char* smem_raw) {
@@ -186,17 +266,14 @@ __device__ __forceinline__ void spread_subproblem_runs(const PointArgs<T>& a, co
   constexpr int G = run_groups(NS);
   constexpr int RPL = run_rows_per_lane(DIM, NS);
   constexpr int NR = run_rows(DIM, NS);
-  constexpr int WY = run_wy(DIM, NS);
-  constexpr int WZ = run_wz(DIM, NS);
-  constexpr int SLOT = run_slot_reals(DIM, NS);
+  constexpr int SLOT = run_slot_reals(DIM, NS, (int)sizeof(T));
   static_assert(SLOT > 0, "run-merging layout does not apply");
-  constexpr int YOFF = 2 * NS;       // y weights within a slot
-  constexpr int ZOFF = 2 * NS + WY;  // z weights within a slot (3D)
   const Geom& g = a.g;
   const int tile_cells = g.pad[2] * g.pad[1] * g.pitch;
   T* s_re = reinterpret_cast<T*>(smem_raw);
   T* s_im = s_re + tile_cells;
-  T* s_st = s_im + tile_cells;  // [NW*32][SLOT]
+  // slots start 16-byte aligned after the two tile planes
+  T* s_st = reinterpret_cast<T*>(smem_raw + ((2 * (size_t)tile_cells * sizeof(T) + 15) & ~(size_t)15));
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   const int row = g.pitch;
@@ -269,29 +346,7 @@ __device__ __forceinline__ void spread_subproblem_runs(const PointArgs<T>& a, co
           cv.x = cv.y = (T)0;
           off = 0;
         }
-#pragma unroll
-        for (int q = 0; q < NS; ++q) {
-          CT v;
-          v.x = cv.x * w[0][q];
-          v.y = cv.y * w[0][q];
-          reinterpret_cast<CT*>(my_slot)[q] = v;
-        }
-#pragma unroll
-        for (int q = 0; q < WY; q += 2) {
-          CT v;
-          v.x = q < NS ? w[1][q] : (T)0;
-          v.y = q + 1 < NS ? w[1][q + 1] : (T)0;
-          reinterpret_cast<CT*>(my_slot + YOFF)[q / 2] = v;
-        }
-        if constexpr (DIM == 3) {
-#pragma unroll
-          for (int q = 0; q < WZ; q += 2) {
-            CT v;
-            v.x = q < NS ? w[2][q] : (T)0;
-            v.y = q + 1 < NS ? w[2][q + 1] : (T)0;
-            reinterpret_cast<CT*>(my_slot + ZOFF)[q / 2] = v;
-          }
-        }
+        stage_slot<T, DIM, NS>(my_slot, cv, w);
       }
       // lane j starts a run when its cell differs from point j-1's
       int prev = __shfl_up_sync(0xffffffffu, off, 1);
@@ -299,40 +354,22 @@ __device__ __forceinline__ void spread_subproblem_runs(const PointArgs<T>& a, co
       const unsigned starts = __ballot_sync(0xffffffffu, valid && off != prev);
       __syncwarp();
       const int cnt = min(32, w1 - kb);
-      for (int j = 0; j < cnt; ++j) {
+      int j = 0;
+      const T* sp = warp_slots;
+      while (j < cnt) {  // one run (or the rest of one) per trip
         if ((starts >> j) & 1u) {
           if (run_off >= 0) flush_run();
           run_off = __shfl_sync(0xffffffffu, off, j);
         }
-        const T* sp = warp_slots + j * SLOT;
-        const CT cw = reinterpret_cast<const CT*>(sp)[kx];
-        T wr[RPL];
-        if constexpr (DIM == 2) {
-          const T* wy = sp + YOFF + grp * RPL;
-          if constexpr (RPL % 2 == 0) {
-#pragma unroll
-            for (int r = 0; r < RPL; r += 2) {
-              const CT pr = *reinterpret_cast<const CT*>(wy + r);
-              wr[r] = pr.x;
-              wr[r + 1] = pr.y;
-            }
-          } else {
-#pragma unroll
-            for (int r = 0; r < RPL; ++r) wr[r] = wy[r];
-          }
-        } else if constexpr (RPL % NS == 0) {
-          const T* wz = sp + ZOFF + grp * (RPL / NS);
-#pragma unroll
-          for (int r = 0; r < RPL; ++r) wr[r] = wz[r / NS] * sp[YOFF + r % NS];
-        } else {
-#pragma unroll
-          for (int r = 0; r < RPL; ++r) {
-            const int rho = grp * RPL + r;
-            wr[r] = sp[ZOFF + rho / NS] * sp[YOFF + rho % NS];
-          }
+        const unsigned later = j < 31 ? starts >> (j + 1) : 0u;
+        const int je = later != 0u ? min(j + __ffs(later), cnt) : cnt;
+        for (; j + 4 <= je; j += 4, sp += 4 * SLOT) {
+          add_slot<T, DIM, NS>(sp, kx, grp, acc);
+          add_slot<T, DIM, NS>(sp + SLOT, kx, grp, acc);
+          add_slot<T, DIM, NS>(sp + 2 * SLOT, kx, grp, acc);
+          add_slot<T, DIM, NS>(sp + 3 * SLOT, kx, grp, acc);
         }
-#pragma unroll
-        for (int r = 0; r < RPL; ++r) acc[r] = fma_rc(wr[r], cw, acc[r]);
+        for (; j < je; ++j, sp += SLOT) add_slot<T, DIM, NS>(sp, kx, grp, acc);
       }
       __syncwarp();
     }
@@ -456,7 +493,7 @@ __device__ __forceinline__ void spread_subproblem_cells(const PointArgs<T>& a, c
 template <typename T, int DIM, int NS, int NW>
 __device__ __forceinline__ void spread_subproblem(const PointArgs<T>& a, const cplx_t<T>* __restrict__ c,
                                                   cplx_t<T>* __restrict__ fw, int sidx, unsigned char* smem_raw) {
-  if constexpr (run_slot_reals(DIM, NS) > 0)
+  if constexpr (run_slot_reals(DIM, NS, (int)sizeof(T)) > 0)
     spread_subproblem_runs<T, DIM, NS, NW>(a, c, fw, sidx, smem_raw);
   else
     spread_subproblem_cells<T, DIM, NS, NW>(a, c, fw, sidx, smem_raw);
