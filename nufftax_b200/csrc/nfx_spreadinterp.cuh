@@ -56,25 +56,23 @@ struct PointArgs {
 // The NS weights of one axis: w[q] = phi(i0 + q - xs).  float with a fitted
 // polynomial: Horner in v = 2 (xs - i0) - (NS - 1) (exact in float: xs - i0 is
 // exact because xs and i0 are within NS of each other and i0 is an integer),
-// degree kPolyEvalDeg, two weights per paired FMA, each coefficient a fixed
-// offset in the argument block; otherwise exp/sqrt (nufftax/core/kernel.py:79-111).
+// degree kPolyEvalDeg, each coefficient a fixed offset in the argument block
+// (an operand of its FMA, no load); otherwise exp/sqrt
+// (nufftax/core/kernel.py:79-111).
 template <typename T, int NS>
 __device__ __forceinline__ void axis_weights(const PointArgs<T>& a, int i0, T xs, T* w) {
   if (std::is_same<T, float>::value && a.poly.deg > 0) {
     const float v = 2.0f * (float)(xs - (T)i0) - (float)(NS - 1);
-    const float2 vv = make_float2(v, v);
-    float2 h[(NS + 1) / 2];
+    float h[NS];
 #pragma unroll
-    for (int q = 0; q < NS; q += 2)
-      h[q / 2] = make_float2(a.poly.a[q][kPolyEvalDeg], q + 1 < NS ? a.poly.a[q + 1][kPolyEvalDeg] : 0.0f);
+    for (int q = 0; q < NS; ++q) h[q] = a.poly.a[q][kPolyEvalDeg];
 #pragma unroll
     for (int d = kPolyEvalDeg - 1; d >= 0; --d) {
 #pragma unroll
-      for (int q = 0; q < NS; q += 2)
-        h[q / 2] = fma2(h[q / 2], vv, make_float2(a.poly.a[q][d], q + 1 < NS ? a.poly.a[q + 1][d] : 0.0f));
+      for (int q = 0; q < NS; ++q) h[q] = fmaf(h[q], v, a.poly.a[q][d]);
     }
 #pragma unroll
-    for (int q = 0; q < NS; ++q) w[q] = (T)((q & 1) ? h[q / 2].y : h[q / 2].x);
+    for (int q = 0; q < NS; ++q) w[q] = (T)h[q];
   } else {
 #pragma unroll
     for (int q = 0; q < NS; ++q) w[q] = es_weight(rn_sub((T)(i0 + q), xs), a.beta, a.kc);
@@ -217,8 +215,15 @@ __device__ __forceinline__ void stage_slot(T* sp, cplx_t<T> cv, const T (&w)[DIM
   }
 }
 
+// Footprint row (y, or z * ns + y) of a lane's accumulator r: each group owns
+// rpl consecutive rows.
+template <int DIM, int NS>
+__device__ __forceinline__ int run_row(int grp, int r) {
+  return grp * run_rows_per_lane(DIM, NS) + r;
+}
+
 // Adds one staged point to this lane's accumulators: acc[r] += w_row(r) * (c w_x),
-// w_row the y weight of row r (2D) or z weight * y weight (3D).
+// w_row the y weight of row run_row(r) (2D) or z weight * y weight (3D).
 template <typename T, int DIM, int NS>
 __device__ __forceinline__ void add_slot(const T* sp, int kx, int grp, cplx_t<T> (&acc)[run_rows_per_lane(DIM, NS)]) {
   using CT = cplx_t<T>;
@@ -247,6 +252,10 @@ __device__ __forceinline__ void add_slot(const T* sp, int kx, int grp, cplx_t<T>
     }
   }
 }
+
+// Batches of 32 points with at least this many run starts (mean run of 4 or
+// less) skip the register accumulation and add each point directly.
+constexpr int kSparseRuns = 8;
 
 // Run-merging spread (2D/3D, footprints of at least 32 cells).  Each warp walks
 // a contiguous, cell-ordered slice of the subproblem 32 points at a time: every
@@ -302,14 +311,19 @@ __device__ __forceinline__ void spread_subproblem_runs(const PointArgs<T>& a, co
 #pragma unroll
     for (int r = 0; r < RPL; ++r) acc[r].x = acc[r].y = (T)0;
     int run_off = -1;
+    // tile offset of accumulator r relative to a footprint's origin, -1 when
+    // this lane does not own that row
+    auto cell_of = [&](int r) {
+      const int rho = run_row<DIM, NS>(grp, r);
+      return (lane_on && rho < NR) ? (DIM == 3 ? (rho / NS) * plane + (rho % NS) * row : rho * row) + kx : -1;
+    };
     auto flush_run = [&]() {
 #pragma unroll
       for (int r = 0; r < RPL; ++r) {
-        const int rho = grp * RPL + r;
-        if (lane_on && rho < NR) {
-          const int addr = run_off + (DIM == 3 ? (rho / NS) * plane + (rho % NS) * row : rho * row) + kx;
-          atomicAdd(&s_re[addr], acc[r].x);
-          atomicAdd(&s_im[addr], acc[r].y);
+        const int cr = cell_of(r);
+        if (cr >= 0) {
+          atomicAdd(&s_re[run_off + cr], acc[r].x);
+          atomicAdd(&s_im[run_off + cr], acc[r].y);
         }
         acc[r].x = acc[r].y = (T)0;
       }
@@ -356,6 +370,30 @@ __device__ __forceinline__ void spread_subproblem_runs(const PointArgs<T>& a, co
       const int cnt = min(32, w1 - kb);
       int j = 0;
       const T* sp = warp_slots;
+      if (__popc(starts) >= kSparseRuns) {
+        // short runs: points before the first run start finish the pending
+        // run; every later point is added to shared memory directly
+        const int first = __ffs(starts) - 1;
+        for (; j < first; ++j, sp += SLOT) add_slot<T, DIM, NS>(sp, kx, grp, acc);
+        if (run_off >= 0) flush_run();
+        for (; j < cnt; ++j, sp += SLOT) {
+          const int pj = __shfl_sync(0xffffffffu, off, j);
+          CT one[RPL];
+#pragma unroll
+          for (int r = 0; r < RPL; ++r) one[r].x = one[r].y = (T)0;
+          add_slot<T, DIM, NS>(sp, kx, grp, one);
+#pragma unroll
+          for (int r = 0; r < RPL; ++r) {
+            const int cr = cell_of(r);
+            if (cr >= 0) {
+              atomicAdd(&s_re[pj + cr], one[r].x);
+              atomicAdd(&s_im[pj + cr], one[r].y);
+            }
+          }
+        }
+        run_off = __shfl_sync(0xffffffffu, off, cnt - 1);  // accumulators are empty
+        j = cnt;
+      }
       while (j < cnt) {  // one run (or the rest of one) per trip
         if ((starts >> j) & 1u) {
           if (run_off >= 0) flush_run();
