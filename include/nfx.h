@@ -53,7 +53,8 @@ typedef struct nfx_opts {
                           transforms do (nufftax/transforms/nufft1.py:71); 0: fold
                           only, as the core spread / interp functions do */
   int tile[3];         /* bin edge per axis in cells; 0 = default */
-  int max_subproblem;  /* points per subproblem; 0 = default */
+  int max_subproblem;  /* points per subproblem; 0 = default (2048 in 3D; in 1D/2D
+                          1024, doubled up to 4096 while M / (2 * size) >= 1480) */
 } nfx_opts;
 
 /* Library identity and last error of the calling thread. */
@@ -70,7 +71,8 @@ int nfx_num_sms(void);
  * kernels evaluate exp/sqrt. */
 int nfx_es_poly(int nspread, double beta, double kc, float* coeffs, int* degree, double* max_abs_err);
 
-/* Fill tile[] / max_subproblem with the defaults the library would use. */
+/* Fill tile[] with the defaults the library would use (max_subproblem = 0 is
+ * left as is: its default depends on the number of points). */
 int nfx_default_tiles(nfx_opts* opts);
 
 /* ---- bin sort --------------------------------------------------------------

@@ -223,7 +223,8 @@ static int validate_opts(const nfx_opts* o) {
   return NFX_OK;
 }
 
-// Resolve tile[] = 0 / max_subproblem = 0 to defaults, keep the bin count and
+// Resolve tile[] = 0 to defaults (max_subproblem = 0 stays "auto": the sort
+// layout picks it from M), keep the bin count and
 // the shared memory of every kernel within budget.
 static int resolve_opts(const nfx_opts* in, nfx_opts& o) {
   int st = validate_opts(in);
@@ -278,7 +279,6 @@ static int resolve_opts(const nfx_opts* in, nfx_opts& o) {
       o = trial;
     }
   }
-  if (o.max_subproblem == 0) o.max_subproblem = (o.dim == 3) ? 2048 : 1024;
   Geom g;
   fill_geom(&o, g);
   if (g.nbins > kMaxBins) {
@@ -298,6 +298,18 @@ static int resolve_opts(const nfx_opts* in, nfx_opts& o) {
 
 static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
 
+// Default subproblem size (max_subproblem = 0): 2048 points in 3D; in 1D/2D
+// 1024, doubled (up to 4096) while the points still fill about two subproblems
+// per resident spread CTA (148 SMs x 5), so large dense sets flush their tiles
+// to the fine grid less often without starving the SMs.
+static int auto_max_subproblem(int dim, int64_t M) {
+  if (dim == 3) return 2048;
+  constexpr int64_t kSubTarget = 1480;
+  int maxsub = 1024;
+  while (maxsub < 4096 && M / (2 * (int64_t)maxsub) >= kSubTarget) maxsub *= 2;
+  return maxsub;
+}
+
 static void make_layout(const nfx_opts& o, const Geom& g, int64_t M, SortLayout& L) {
   L.M = M;
   L.nbins = g.nbins;
@@ -305,7 +317,7 @@ static void make_layout(const nfx_opts& o, const Geom& g, int64_t M, SortLayout&
   radix_plan(g.nbins, L.ncell, L.cbits, L.bits, L.npass, L.dbits);
   const int64_t B = (int64_t)1 << L.dbits;
   L.nchunks = (int)((M + radix_chunk() - 1) / radix_chunk());
-  L.maxsub = o.max_subproblem;
+  L.maxsub = o.max_subproblem > 0 ? o.max_subproblem : auto_max_subproblem(o.dim, M);
   L.max_subs = g.nbins + (M + L.maxsub - 1) / L.maxsub;
   size_t off = 0;
   auto take = [&](size_t bytes) {

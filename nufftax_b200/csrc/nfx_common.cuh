@@ -122,15 +122,19 @@ __device__ __forceinline__ void red_add(double2* addr, double2 v) {
 
 // Paired FMA: (a.x * b.x + c.x, a.y * b.y + c.y), each rounded once to
 // nearest.  float uses Blackwell's fma.rn.f32x2 (one instruction, the same
-// results as two fmaf); double is two fma.
+// results as two fmaf) on 64-bit register pairs; the packing is plain C++ so
+// the compiler can keep pairs in adjacent registers and hoist it out of loops.
+// double is two fma.
+__device__ __forceinline__ unsigned long long pack2(float2 v) {
+  return (unsigned long long)__float_as_uint(v.x) | ((unsigned long long)__float_as_uint(v.y) << 32);
+}
+__device__ __forceinline__ float2 unpack2(unsigned long long v) {
+  return make_float2(__uint_as_float((unsigned)v), __uint_as_float((unsigned)(v >> 32)));
+}
 __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
-  float2 d;
-  asm("{\n\t.reg .b64 ra, rb, rc, rd;\n\t"
-      "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\tmov.b64 rc, {%6, %7};\n\t"
-      "fma.rn.f32x2 rd, ra, rb, rc;\n\tmov.b64 {%0, %1}, rd;\n\t}"
-      : "=f"(d.x), "=f"(d.y)
-      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
-  return d;
+  unsigned long long d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(pack2(a)), "l"(pack2(b)), "l"(pack2(c)));
+  return unpack2(d);
 }
 __device__ __forceinline__ double2 fma2(double2 a, double2 b, double2 c) {
   double2 d;
@@ -141,6 +145,9 @@ __device__ __forceinline__ double2 fma2(double2 a, double2 b, double2 c) {
 // c + s * v for a real s and a complex v.
 __device__ __forceinline__ float2 fma_rc(float s, float2 v, float2 c) { return fma2(make_float2(s, s), v, c); }
 __device__ __forceinline__ double2 fma_rc(double s, double2 v, double2 c) { return fma2(make_double2(s, s), v, c); }
+// (s, s) as a complex-typed pair, for a real weight used with many values.
+__device__ __forceinline__ float2 splat2(float s) { return make_float2(s, s); }
+__device__ __forceinline__ double2 splat2(double s) { return make_double2(s, s); }
 
 // Polynomial form of the ES weights of one footprint (float path).  For a point
 // at scaled coordinate xs with left cell i0, every weight phi(i0 + q - xs),

@@ -610,6 +610,9 @@ __device__ __forceinline__ void interp_subproblem(const PointArgs<T>& a, const c
         }
         T ar = 0, ai = 0;
         const CT* base = s_tile + off;
+        CT wxp[NS];  // (w_x, w_x) pairs, built once per point
+#pragma unroll
+        for (int kx = 0; kx < NS; ++kx) wxp[kx] = splat2(w[0][kx]);
 #pragma unroll 1
         for (int kz = 0; kz < (DIM == 3 ? NS : 1); ++kz) {
           T zr = 0, zi = 0;
@@ -619,7 +622,7 @@ __device__ __forceinline__ void interp_subproblem(const PointArgs<T>& a, const c
             CT xa;
             xa.x = xa.y = (T)0;
 #pragma unroll
-            for (int kx = 0; kx < NS; ++kx) xa = fma_rc(w[0][kx], rp[kx], xa);
+            for (int kx = 0; kx < NS; ++kx) xa = fma2(wxp[kx], rp[kx], xa);
             const T xr = xa.x, xi = xa.y;
             if (DIM >= 2) {
               zr += xr * w[DIM >= 2 ? 1 : 0][ky];
