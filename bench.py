@@ -191,11 +191,11 @@ ALG_BYTES = {
 
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch per point set,
-# from ncu --set full captures of `bench.py --case radial|clustered --reps 2` (the step
+# from ncu --set full captures of `bench.py --case radial|clustered --reps 1` (the step
 # launches each kernel once per set, so the per-launch figure is their mean).
 MEASURED_TRAFFIC = {
-    "nfx_spread_sorted": {"radial": 17.28e6, "clustered": 119.32e6},
-    "nfx_interp_sorted": {"radial": 13.47e6, "clustered": 104.96e6},
+    "nfx_spread_sorted": {"radial": 17.3e6, "clustered": 117.0e6},
+    "nfx_interp_sorted": {"radial": 13.5e6, "clustered": 108.4e6},
 }
 
 

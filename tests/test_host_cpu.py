@@ -44,10 +44,27 @@ def test_default_tiles_and_workspace():
     lib = _lib.load()
     o = _opts()
     assert lib.nfx_default_tiles(byref(o)) == 0
-    assert list(o.tile)[:2] == [32, 32] and o.max_subproblem > 0
+    # max_subproblem = 0 stays "auto": the sort layout picks it from M
+    assert list(o.tile)[:2] == [32, 32] and o.max_subproblem == 0
     b = c_size_t(0)
     assert lib.nfx_sort_workspace_bytes(byref(o), 4_000_000, byref(b)) == 0
     assert 8 * 4_000_000 < b.value < 64 * 4_000_000
+
+
+@pytest.mark.parametrize("M,expected", [(500_000, 1024), (3_000_000, 1024), (4_000_000, 2048),
+                                        (20_000_000, 4096)])
+def test_auto_subproblem_size(M, expected):
+    """2D default: 1024, doubled (up to 4096) while M / (2 * size) >= 1480; the
+    workspace of max_subproblem = 0 equals that of the explicit size."""
+    lib = _lib.load()
+    auto, explicit = _opts(), _opts()
+    assert lib.nfx_default_tiles(byref(auto)) == 0
+    assert lib.nfx_default_tiles(byref(explicit)) == 0
+    explicit.max_subproblem = expected
+    ba, be = c_size_t(0), c_size_t(0)
+    assert lib.nfx_sort_workspace_bytes(byref(auto), M, byref(ba)) == 0
+    assert lib.nfx_sort_workspace_bytes(byref(explicit), M, byref(be)) == 0
+    assert ba.value == be.value
     o3 = _opts(3, (256, 256, 256))
     assert lib.nfx_default_tiles(byref(o3)) == 0
     assert all(t > 0 for t in o3.tile)
