@@ -126,33 +126,35 @@ constexpr size_t kSmemBudget = 200 * 1024;
 
 static size_t real_bytes(int precision) { return precision == NFX_F64 ? 8 : 4; }
 
-// Row pitch (cells) of the shared-memory tile.  2D footprints of at least 32
-// cells use the run-merging spread, whose flush has lane (grp, kx) add to row
-// grp * rpl + r, column kx: the pitch (at most a quarter longer than the row)
-// is the one whose rows put those 32 words in the fewest shared-memory banks
-// per instruction.  Otherwise rows of one footprint are `ns` cells wide and a
-// warp covers 32/ns rows: a pitch that is an odd multiple of ns (mod 32) puts
-// those rows in disjoint bank ranges (at most ~12% longer).
-static int flush_conflicts(int pitch, int ns) {
-  const int G = run_groups(ns), rpl = run_rows_per_lane(2, ns);
+// Row pitch (cells) of the shared-memory tile.  Footprints of at least 32
+// cells in 2D/3D use the run-merging spread, whose flush has lane (grp, kx)
+// add to footprint row rho = grp * rpl + r (2D: y = rho; 3D: z = rho / ns,
+// y = rho % ns), column kx: the pitch (at most a quarter longer than the row)
+// is the one that puts those 32 words in the fewest shared-memory banks per
+// instruction.  Otherwise rows of one footprint are `ns` cells wide and a warp
+// covers 32/ns rows: a pitch that is an odd multiple of ns (mod 32) puts those
+// rows in disjoint bank ranges (at most ~12% longer).
+static int flush_conflicts(int pitch, int plane, int ns, int dim) {
+  const int G = run_groups(ns), rpl = run_rows_per_lane(dim, ns), nr = run_rows(dim, ns);
   int worst = 0;
   for (int r = 0; r < rpl; ++r) {
     int bank[32] = {0};
     for (int grp = 0; grp < G; ++grp) {
       const int rho = grp * rpl + r;
-      if (rho >= ns) continue;
-      for (int kx = 0; kx < ns; ++kx) ++bank[(rho * pitch + kx) % 32];
+      if (rho >= nr) continue;
+      const int base = dim == 3 ? (rho / ns) * plane + (rho % ns) * pitch : rho * pitch;
+      for (int kx = 0; kx < ns; ++kx) ++bank[(base + kx) % 32];
     }
     for (int k = 0; k < 32; ++k) worst += bank[k] > 1 ? bank[k] - 1 : 0;
   }
   return worst;
 }
 
-static int choose_pitch(int pad0, int ns, int dim) {
-  if (dim == 2 && run_slot_reals(2, ns, 4) > 0) {
-    int best = pad0, best_c = flush_conflicts(pad0, ns);
+static int choose_pitch(int pad0, int pad1, int ns, int dim) {
+  if (dim >= 2 && run_slot_reals(dim, ns, 4) > 0) {
+    int best = pad0, best_c = flush_conflicts(pad0, pad0 * pad1, ns, dim);
     for (int p = pad0 + 1; p <= pad0 + std::max(1, pad0 / 4) && best_c > 0; ++p) {
-      const int c = flush_conflicts(p, ns);
+      const int c = flush_conflicts(p, p * pad1, ns, dim);
       if (c < best_c) {
         best = p;
         best_c = c;
@@ -178,7 +180,7 @@ static void fill_geom(const nfx_opts* o, Geom& g) {
     g.pad[d] = act ? g.tile[d] + o->nspread - 1 : 1;
     g.tdiv[d] = make_fastdiv(g.tile[d]);
   }
-  g.pitch = choose_pitch(g.pad[0], o->nspread, o->dim);
+  g.pitch = choose_pitch(g.pad[0], g.pad[1], o->nspread, o->dim);
   g.nbins = g.nb[0] * g.nb[1] * g.nb[2];
   g.prenorm = o->prenorm;
 }

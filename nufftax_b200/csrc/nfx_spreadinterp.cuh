@@ -215,15 +215,8 @@ __device__ __forceinline__ void stage_slot(T* sp, cplx_t<T> cv, const T (&w)[DIM
   }
 }
 
-// Footprint row (y, or z * ns + y) of a lane's accumulator r: each group owns
-// rpl consecutive rows.
-template <int DIM, int NS>
-__device__ __forceinline__ int run_row(int grp, int r) {
-  return grp * run_rows_per_lane(DIM, NS) + r;
-}
-
 // Adds one staged point to this lane's accumulators: acc[r] += w_row(r) * (c w_x),
-// w_row the y weight of row run_row(r) (2D) or z weight * y weight (3D).
+// w_row the y weight of row grp * rpl + r (2D) or z weight * y weight (3D).
 template <typename T, int DIM, int NS>
 __device__ __forceinline__ void add_slot(const T* sp, int kx, int grp, cplx_t<T> (&acc)[run_rows_per_lane(DIM, NS)]) {
   using CT = cplx_t<T>;
@@ -249,6 +242,56 @@ __device__ __forceinline__ void add_slot(const T* sp, int kx, int grp, cplx_t<T>
     for (int r = 0; r < RPL; ++r) {
       const int rho = grp * RPL + r;
       acc[r] = fma_rc(sp[ZOFF + rho / NS] * sp[YOFF + rho % NS], cw, acc[r]);
+    }
+  }
+}
+
+// Adds one staged point straight to the shared tile at footprint origin `off`.
+// lane_cell: tile offset of this lane's first cell (row grp * rpl, column kx)
+// from the origin, -1 when the lane owns no cell; rows r after the first are
+// r rows further (2D), or r / ns planes and r % ns rows further (3D with rpl a
+// multiple of ns: compile-time in r).
+template <typename T, int DIM, int NS>
+__device__ __forceinline__ void add_slot_direct(const T* sp, int kx, int grp, int off, T* s_re, T* s_im,
+                                                int lane_cell, int row, int plane) {
+  using CT = cplx_t<T>;
+  constexpr int RPL = run_rows_per_lane(DIM, NS);
+  constexpr int NR = run_rows(DIM, NS);
+  constexpr int WY = run_wy(DIM, NS);
+  constexpr int YOFF = round4(2 * NS);
+  constexpr int ZOFF = YOFF + WY;
+  if (lane_cell < 0) return;
+  const CT cw = reinterpret_cast<const CT*>(sp)[kx];
+  T* pr = s_re + off + lane_cell;
+  T* pi = s_im + off + lane_cell;
+  auto add = [&](int o, T w) {
+    atomicAdd(pr + o, w * cw.x);
+    atomicAdd(pi + o, w * cw.y);
+  };
+  if constexpr (DIM == 2) {
+    const T* wy = sp + YOFF + grp * RPL;
+#pragma unroll
+    for (int r = 0; r < RPL; ++r)
+      if (grp * RPL + r < NR) add(r * row, wy[r]);
+  } else if constexpr (RPL % NS == 0) {
+    const T* wz = sp + ZOFF + grp * (RPL / NS);
+    T wy[NS];
+#pragma unroll
+    for (int q = 0; q < NS; ++q) wy[q] = sp[YOFF + q];
+#pragma unroll
+    for (int zz = 0; zz < RPL / NS; ++zz) {
+      const T z = wz[zz];
+#pragma unroll
+      for (int q = 0; q < NS; ++q) add(zz * plane + q * row, z * wy[q]);
+    }
+  } else {
+#pragma unroll
+    for (int r = 0; r < RPL; ++r) {
+      const int rho = grp * RPL + r;
+      if (rho < NR) {
+        const int rz = rho / NS, ry = rho - rz * NS;
+        add((rz - (grp * RPL) / NS) * plane + (ry - (grp * RPL) % NS) * row, sp[ZOFF + rz] * sp[YOFF + ry]);
+      }
     }
   }
 }
@@ -311,22 +354,34 @@ __device__ __forceinline__ void spread_subproblem_runs(const PointArgs<T>& a, co
 #pragma unroll
     for (int r = 0; r < RPL; ++r) acc[r].x = acc[r].y = (T)0;
     int run_off = -1;
-    // tile offset of accumulator r relative to a footprint's origin, -1 when
-    // this lane does not own that row
-    auto cell_of = [&](int r) {
-      const int rho = run_row<DIM, NS>(grp, r);
-      return (lane_on && rho < NR) ? (DIM == 3 ? (rho / NS) * plane + (rho % NS) * row : rho * row) + kx : -1;
-    };
+    // this lane's first cell (row grp * rpl, column kx) relative to a
+    // footprint's origin; -1 for lanes past the groups
+    const int rho0 = grp * RPL;
+    const int lane_cell = lane_on ? (DIM == 3 ? (rho0 / NS) * plane + (rho0 % NS) * row : rho0 * row) + kx : -1;
     auto flush_run = [&]() {
+      if (lane_cell >= 0) {
+        T* pr = s_re + run_off + lane_cell;
+        T* pi = s_im + run_off + lane_cell;
 #pragma unroll
-      for (int r = 0; r < RPL; ++r) {
-        const int cr = cell_of(r);
-        if (cr >= 0) {
-          atomicAdd(&s_re[run_off + cr], acc[r].x);
-          atomicAdd(&s_im[run_off + cr], acc[r].y);
+        for (int r = 0; r < RPL; ++r) {
+          const int rho = rho0 + r;
+          if (rho < NR) {
+            // offset of row r from this lane's first row
+            int o;
+            if constexpr (DIM == 2) {
+              o = r * row;
+            } else if constexpr (RPL % NS == 0) {
+              o = (r / NS) * plane + (r % NS) * row;
+            } else {
+              o = (rho / NS - rho0 / NS) * plane + (rho % NS - rho0 % NS) * row;
+            }
+            atomicAdd(pr + o, acc[r].x);
+            atomicAdd(pi + o, acc[r].y);
+          }
         }
-        acc[r].x = acc[r].y = (T)0;
       }
+#pragma unroll
+      for (int r = 0; r < RPL; ++r) acc[r].x = acc[r].y = (T)0;
     };
     // software pipeline: coordinates and strength of this lane's point in the
     // current batch (xn, cn) and the point index of the next batch (pn)
@@ -376,21 +431,9 @@ __device__ __forceinline__ void spread_subproblem_runs(const PointArgs<T>& a, co
         const int first = __ffs(starts) - 1;
         for (; j < first; ++j, sp += SLOT) add_slot<T, DIM, NS>(sp, kx, grp, acc);
         if (run_off >= 0) flush_run();
-        for (; j < cnt; ++j, sp += SLOT) {
-          const int pj = __shfl_sync(0xffffffffu, off, j);
-          CT one[RPL];
-#pragma unroll
-          for (int r = 0; r < RPL; ++r) one[r].x = one[r].y = (T)0;
-          add_slot<T, DIM, NS>(sp, kx, grp, one);
-#pragma unroll
-          for (int r = 0; r < RPL; ++r) {
-            const int cr = cell_of(r);
-            if (cr >= 0) {
-              atomicAdd(&s_re[pj + cr], one[r].x);
-              atomicAdd(&s_im[pj + cr], one[r].y);
-            }
-          }
-        }
+        for (; j < cnt; ++j, sp += SLOT)
+          add_slot_direct<T, DIM, NS>(sp, kx, grp, __shfl_sync(0xffffffffu, off, j), s_re, s_im, lane_cell, row,
+                                      plane);
         run_off = __shfl_sync(0xffffffffu, off, cnt - 1);  // accumulators are empty
         j = cnt;
       }
