@@ -804,6 +804,12 @@ __global__ void __launch_bounds__(NW * 32) k_grad(PointArgs<T> a, const cplx_t<T
 #pragma unroll
         for (int i = 0; i <= DIM; ++i) sr[i] = si[i] = (T)0;
         const CT* base = s_tile + (inside ? off : 0);
+        CT wxp[NS], dwxp[NS];  // (w_x, w_x) and (w_x', w_x') pairs, built once per point
+#pragma unroll
+        for (int kx = 0; kx < NS; ++kx) {
+          wxp[kx] = splat2(w[0][kx]);
+          dwxp[kx] = splat2(dw[0][kx]);
+        }
 #pragma unroll 1
         for (int kz = 0; kz < (inside && DIM == 3 ? NS : (inside ? 1 : 0)); ++kz) {
           // per-z accumulators: [0] plain, [1] d/dx, [2] d/dy
@@ -816,8 +822,8 @@ __global__ void __launch_bounds__(NW * 32) k_grad(PointArgs<T> a, const cplx_t<T
 #pragma unroll
             for (int kx = 0; kx < NS; ++kx) {
               const CT v = rp[kx];
-              xa = fma_rc(w[0][kx], v, xa);
-              xa1 = fma_rc(dw[0][kx], v, xa1);
+              xa = fma2(wxp[kx], v, xa);
+              xa1 = fma2(dwxp[kx], v, xa1);
             }
             const T xr = xa.x, xi = xa.y, xr1 = xa1.x, xi1 = xa1.y;
             if (DIM >= 2) {
