@@ -145,6 +145,11 @@ inline size_t spread_smem_bytes(size_t real_bytes, int dim, int ns, const Geom& 
   if (slot > 0) return ((tile + 15) & ~(size_t)15) + (size_t)nw * 32 * slot * real_bytes;  // 16-byte aligned slots
   return tile + ((size_t)dim * ns * (nw * 32 + 1) + (size_t)2 * nw * 32) * real_bytes + (size_t)nw * 32 * sizeof(int);
 }
+// Dynamic shared memory of the plane-owner spread (3D, sparse points): two tile
+// planes plus one slot of 4 ns + 3 reals per staged point.
+inline size_t owner_smem_bytes(size_t real_bytes, int ns, int nw, const Geom& g) {
+  return 2 * real_bytes * (size_t)g.pad[2] * g.pad[1] * g.pitch + (size_t)nw * 32 * (4 * ns + 3) * real_bytes;
+}
 inline size_t tile_smem_bytes(size_t real_bytes, const Geom& g) {
   return 2 * real_bytes * (size_t)g.pad[2] * g.pad[1] * g.pitch;
 }

@@ -588,6 +588,114 @@ __global__ void __launch_bounds__(NW * 32) k_spread(PointArgs<T> a, const cplx_t
   for (int sidx = blockIdx.x; sidx < nsub; sidx += gridDim.x) spread_subproblem<T, DIM, NS, NW>(a, c, fw, sidx, smem_raw);
 }
 
+// Plane-owner spread (3D, points sparser than cells).  The CTA stages up to
+// NW*32 points at a time (every thread folds one point: c * w_x, y and z
+// weights, its tile origin); then warp w adds every staged point into the
+// tile planes z with z % NW == w, each plane's ns x ns cells spread over the
+// lanes, with plain shared-memory read-add-write: a plane belongs to one warp,
+// whose lanes touch distinct cells in each instruction, so no atomics are
+// needed and every cell sums its points in sorted order.  With NW = ns every
+// footprint (ns consecutive planes) gives each warp exactly one plane.
+__host__ __device__ constexpr int owner_slot_reals(int ns) { return 4 * ns + 3; }  // odd: conflict-free stores
+
+template <typename T, int NS, int NW>
+__device__ __forceinline__ void spread_subproblem_owner(const PointArgs<T>& a, const cplx_t<T>* __restrict__ c,
+                                                        cplx_t<T>* __restrict__ fw, int sidx,
+                                                        unsigned char* smem_raw) {
+  using CT = cplx_t<T>;
+  constexpr int SLOT = owner_slot_reals(NS);
+  constexpr int YO = 2 * NS, ZO = 3 * NS, OO = 4 * NS;  // y weights, z weights, origin (offset, z)
+  constexpr int NT = NW * 32;
+  const Geom& g = a.g;
+  const int tile_cells = g.pad[2] * g.pad[1] * g.pitch;
+  T* s_re = reinterpret_cast<T*>(smem_raw);
+  T* s_im = s_re + tile_cells;
+  T* s_st = s_im + tile_cells;  // [NT][SLOT]
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const int row = g.pitch;
+  const int plane = g.pitch * g.pad[1];
+  const int b = a.s.sub_bin[sidx];
+  const int k0 = a.s.sub_start[sidx];
+  const int k1 = min(k0 + a.s.maxsub, a.s.bin_start[b + 1]);
+  int o[3];
+  bin_origin(g, b, o[0], o[1], o[2]);
+  // cells of one footprint plane handled by this lane: column kx = lane % NS,
+  // rows ky0 * IT .. ky0 * IT + IT - 1 with ky0 = lane / NS (LPR row blocks
+  // cover the NS rows; at NS = 8 one instruction touches rows 0, 2, 4, 6)
+  constexpr int LPR = 32 / NS;             // row blocks (lanes per column)
+  constexpr int IT = (NS + LPR - 1) / LPR;  // rows per lane per plane
+  const int kx = lane % NS;
+  const int ky0 = lane / NS;
+  const bool lane_on = ky0 < LPR;
+  for (int t = 0; t < a.n_trans; ++t) {
+    for (int i = threadIdx.x; i < 2 * tile_cells; i += blockDim.x) s_re[i] = (T)0;
+    for (int kb = k0; kb < k1; kb += NT) {
+      const int k = kb + threadIdx.x;
+      if (k < k1) {
+        const int p = a.s.perm[k];
+        T xv[3];
+        load_coords<T, 3>(a, p, xv);
+        int off;
+        T w[3][NS];
+        const bool inside = footprint<T, 3, NS>(a, xv, o, row, plane, off, w);
+        CT cv = c[(int64_t)t * a.M + p];
+        if (!inside) {
+          cv.x = cv.y = (T)0;
+          off = 0;
+        }
+        T* sp = s_st + threadIdx.x * SLOT;
+#pragma unroll
+        for (int q = 0; q < NS; ++q) {
+          sp[2 * q] = cv.x * w[0][q];
+          sp[2 * q + 1] = cv.y * w[0][q];
+          sp[YO + q] = w[1][q];
+          sp[ZO + q] = w[2][q];
+        }
+        sp[OO] = (T)off;
+        sp[OO + 1] = (T)(off / plane);  // z of the footprint origin in the tile
+      }
+      __syncthreads();  // also orders the tile zeroing before the first adds
+      const int cnt = min(NT, k1 - kb);
+      for (int j = 0; j < cnt; ++j) {
+        const T* sp = s_st + j * SLOT;
+        const int off = (int)sp[OO];
+        const int oz = (int)sp[OO + 1];
+        // this warp's planes inside [oz, oz + NS)
+        for (int dz = ((warp - oz) % NW + NW) % NW; dz < NS; dz += NW) {
+          const T wz = sp[ZO + dz];
+          const int base = off + dz * plane + kx;
+          const T cr = sp[2 * kx], ci = sp[2 * kx + 1];
+          if (lane_on) {
+#pragma unroll
+            for (int i = 0; i < IT; ++i) {
+              const int ky = ky0 * IT + i;
+              if (ky < NS) {
+                const T wy = wz * sp[YO + ky];
+                const int addr = base + ky * row;
+                s_re[addr] += wy * cr;
+                s_im[addr] += wy * ci;
+              }
+            }
+          }
+        }
+      }
+      __syncthreads();
+    }
+    flush_tile<T>(g, o, s_re, s_im, fw + (int64_t)t * a.grid_stride);
+    __syncthreads();
+  }
+}
+
+template <typename T, int NS, int NW>
+__global__ void __launch_bounds__(NW * 32) k_spread_owner(PointArgs<T> a, const cplx_t<T>* __restrict__ c,
+                                                          cplx_t<T>* __restrict__ fw) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int nsub = *a.s.nsub;
+  for (int sidx = blockIdx.x; sidx < nsub; sidx += gridDim.x)
+    spread_subproblem_owner<T, NS, NW>(a, c, fw, sidx, smem_raw);
+}
+
 // ---------------------------------------------------------------------------
 // Stage a padded tile of one transform's grid into shared memory (interleaved).
 // ---------------------------------------------------------------------------
@@ -899,8 +1007,19 @@ struct Launch {
   }
 
   static cudaError_t spread(const PointArgs<T>& a, const cplx_t<T>* c, cplx_t<T>* fw, cudaStream_t st) {
-    size_t smem = spread_smem_bytes(sizeof(T), DIM, NS, a.g);
     int grid = 0;
+    if constexpr (DIM == 3 && NS >= 4) {
+      // points sparser than grid cells: runs of same-cell points are rare, and
+      // the plane-owner spread avoids shared-memory atomics altogether
+      if (a.M < (int64_t)a.g.nf[0] * a.g.nf[1] * a.g.nf[2]) {
+        const size_t smem = owner_smem_bytes(sizeof(T), NS, NW, a.g);
+        cudaError_t e = prep(k_spread_owner<T, NS, NW>, smem, grid, a.s.max_subs);
+        if (e != cudaSuccess) return e;
+        k_spread_owner<T, NS, NW><<<grid, NW * 32, smem, st>>>(a, c, fw);
+        return cudaGetLastError();
+      }
+    }
+    size_t smem = spread_smem_bytes(sizeof(T), DIM, NS, a.g);
     cudaError_t e = prep(k_spread<T, DIM, NS, NW>, smem, grid, a.s.max_subs);
     if (e != cudaSuccess) return e;
     k_spread<T, DIM, NS, NW><<<grid, NW * 32, smem, st>>>(a, c, fw);

@@ -95,7 +95,10 @@ def test_sort_empty_and_single():
 # ---------------------------------------------------------------------------
 # Spread / interp components
 # ---------------------------------------------------------------------------
-CASES = [(1, (64,), 700), (1, (1000,), 3000), (2, (48, 40), 2000), (2, (256, 192), 20000), (3, (24, 20, 32), 4000)]
+# The 3D cases cover both 3D spreads: fewer points than grid cells (plane-owner
+# spread) and more (run-merging spread).
+CASES = [(1, (64,), 700), (1, (1000,), 3000), (2, (48, 40), 2000), (2, (256, 192), 20000), (3, (24, 20, 32), 4000),
+         (3, (12, 10, 16), 6000)]
 
 
 @pytest.mark.parametrize("dim,nf,M", CASES)
