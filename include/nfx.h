@@ -155,12 +155,32 @@ int nfx_deconv_pad(int precision, int dim, const int nf[3], const int n_modes[3]
  * In-place batched C2C over the last `dim` axes of n_trans grids.
  * sign = +1: sum_n v[n] e^{+2 pi i k n / nf} (nufftax's ifftn(.) * prod(nf));
  * sign = -1: e^{-...} (fftn).  nufftax/transforms/nufft1.py:81,154,232-235;
- * nufft2.py:317,383,454-457. */
+ * nufft2.py:317,383,454-457.  Calls on different streams may run concurrently,
+ * also with the same plan: the cuFFT work area belongs to the stream (one per
+ * device and stream handle, stream-ordered cudaMallocAsync, grown as needed). */
 int nfx_fft(int precision, int dim, const int nf[3], int n_trans, void* data, int sign, void* stream);
+/* Destroy the cached plans and free the streams' work areas (synchronises the devices). */
 int nfx_fft_cache_clear(void);
 /* Bound the plan cache (default 1024 plans); the least recently used plan is
  * destroyed, after a device synchronisation, when a new one needs room. */
 int nfx_fft_cache_limit(int max_plans);
+
+/* ---- whole transforms in one call -----------------------------------------
+ * The type-1 and type-2 pipelines of nufftax/transforms/nufft1.py:47-90 and
+ * nufft2.py:285-330 as one library call, for callers that want one host call
+ * per transform (serving loops): nfx_nufft1 sorts the points into the
+ * workspace, spreads c into fw (n_trans fine grids), runs the FFT with
+ * fft_sign and deconvolves / reorders into f_out (n_trans x n_modes, CMCL
+ * order); nfx_nufft2 deconvolves / zero-pads f_in into fw, runs the FFT,
+ * sorts and interpolates into c_out.  fac1..fac3 are the per-axis
+ * deconvolution factors (device, precision's real type; unused axes NULL),
+ * n_modes[d] the modes per axis; workspace of nfx_sort_workspace_bytes. */
+int nfx_nufft1(const nfx_opts* opts, const int n_modes[3], const void* x, const void* y, const void* z, int64_t M,
+               const void* c, int n_trans, int fft_sign, const void* fac1, const void* fac2, const void* fac3, void* fw,
+               void* f_out, void* workspace, size_t workspace_bytes, void* stream);
+int nfx_nufft2(const nfx_opts* opts, const int n_modes[3], const void* x, const void* y, const void* z, int64_t M,
+               const void* f_in, int n_trans, int fft_sign, const void* fac1, const void* fac2, const void* fac3,
+               void* fw, void* c_out, void* workspace, size_t workspace_bytes, void* stream);
 
 /* ---- batching: many problems in one launch --------------------------------
  * No counterpart in the reference (nufftax vmaps one problem's strengths).

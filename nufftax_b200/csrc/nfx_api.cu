@@ -764,6 +764,36 @@ static int check_deconv(int precision, int dim, const int nf[3], const int nm[3]
   return NFX_OK;
 }
 
+int nfx_nufft1(const nfx_opts* opts, const int n_modes[3], const void* x, const void* y, const void* z, int64_t M,
+               const void* c, int n_trans, int fft_sign, const void* fac1, const void* fac2, const void* fac3, void* fw,
+               void* f_out, void* ws, size_t ws_bytes, void* stream) {
+  if (opts == nullptr || n_modes == nullptr) {
+    set_error("nfx_nufft1: opts or n_modes is NULL");
+    return NFX_ERR_INVALID;
+  }
+  int st = nfx_sort_points(opts, x, y, z, M, ws, ws_bytes, stream);
+  if (st == NFX_OK) st = nfx_spread_sorted(opts, x, y, z, M, c, n_trans, fw, ws, ws_bytes, stream);
+  if (st == NFX_OK) st = nfx_fft(opts->precision, opts->dim, opts->nf, n_trans, fw, fft_sign, stream);
+  if (st == NFX_OK)
+    st = nfx_deconv_shuffle(opts->precision, opts->dim, opts->nf, n_modes, fac1, fac2, fac3, fw, f_out, n_trans,
+                            stream);
+  return st;
+}
+
+int nfx_nufft2(const nfx_opts* opts, const int n_modes[3], const void* x, const void* y, const void* z, int64_t M,
+               const void* f_in, int n_trans, int fft_sign, const void* fac1, const void* fac2, const void* fac3,
+               void* fw, void* c_out, void* ws, size_t ws_bytes, void* stream) {
+  if (opts == nullptr || n_modes == nullptr) {
+    set_error("nfx_nufft2: opts or n_modes is NULL");
+    return NFX_ERR_INVALID;
+  }
+  int st = nfx_deconv_pad(opts->precision, opts->dim, opts->nf, n_modes, fac1, fac2, fac3, f_in, fw, n_trans, stream);
+  if (st == NFX_OK) st = nfx_fft(opts->precision, opts->dim, opts->nf, n_trans, fw, fft_sign, stream);
+  if (st == NFX_OK) st = nfx_sort_points(opts, x, y, z, M, ws, ws_bytes, stream);
+  if (st == NFX_OK) st = nfx_interp_sorted(opts, x, y, z, M, fw, n_trans, c_out, ws, ws_bytes, stream);
+  return st;
+}
+
 int nfx_deconv_shuffle(int precision, int dim, const int nf[3], const int n_modes[3], const void* fac1,
                        const void* fac2, const void* fac3, const void* fw_hat, void* f_out, int n_trans,
                        void* stream) {

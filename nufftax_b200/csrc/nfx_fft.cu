@@ -1,5 +1,9 @@
 // cuFFT glue: a mutex-guarded, size-limited (least recently used out) cache of
-// batched in-place C2C/Z2Z plans keyed by (device, precision, dims, batch).  Replaces the jnp.fft calls of
+// batched in-place C2C/Z2Z plans keyed by (device, precision, dims, batch).  Plans
+// own no work area: each (device, stream) has one, grown stream-ordered to the
+// largest plan run on it and attached to the plan just before its launch, so the
+// same plan can run concurrently on several streams (a plan's own work area would
+// be shared by them) and cached plans hold no device memory.  Replaces the jnp.fft calls of
 // nufftax/transforms/nufft1.py:81,154,232-235 and nufft2.py:317,383,454-457:
 // sign = +1 is the unnormalised inverse transform (nufftax's ifftn(.) * prod(nf)),
 // sign = -1 the forward transform.
@@ -21,10 +25,19 @@ using PlanKey = std::tuple<int, int, int, int, int, int, int>;  // dev, prec, di
 std::mutex g_plan_mu;
 struct PlanEntry {
   cufftHandle plan;
+  size_t work_bytes;
   uint64_t last_use;
 };
 std::map<PlanKey, PlanEntry>& plans() {
   static std::map<PlanKey, PlanEntry> m;
+  return m;
+}
+struct WorkArea {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+};
+std::map<std::pair<int, cudaStream_t>, WorkArea>& work_areas() {
+  static std::map<std::pair<int, cudaStream_t>, WorkArea> m;
   return m;
 }
 uint64_t g_tick = 0;
@@ -46,6 +59,26 @@ void evict_if_full() {
 int cufft_fail(cufftResult r, const char* where) {
   set_error(std::string(where) + ": cuFFT error " + std::to_string((int)r));
   return NFX_ERR_CUFFT;
+}
+
+// The work area of (dev, stream), at least `bytes` long.  A smaller one is freed
+// in stream order (its last user was a launch on the same stream).
+int stream_work_area(int dev, cudaStream_t s, size_t bytes, void** out) {
+  WorkArea& w = work_areas()[{dev, s}];
+  if (w.bytes < bytes) {
+    if (w.ptr != nullptr) cudaFreeAsync(w.ptr, s);
+    w.ptr = nullptr;
+    w.bytes = 0;
+    cudaError_t e = cudaMallocAsync(&w.ptr, bytes, s);
+    if (e != cudaSuccess) {
+      w.ptr = nullptr;
+      set_error(std::string("cuFFT work area: ") + cudaGetErrorString(e));
+      return NFX_ERR_CUDA;
+    }
+    w.bytes = bytes;
+  }
+  *out = w.ptr;
+  return NFX_OK;
 }
 }  // namespace
 
@@ -77,18 +110,34 @@ int nfx_fft(int precision, int dim, const int nf[3], int n_trans, void* data, in
   std::lock_guard<std::mutex> lk(g_plan_mu);
   cufftHandle plan;
   auto it = plans().find(key);
+  size_t work_bytes = 0;
   if (it == plans().end()) {
     evict_if_full();
-    cufftResult r = cufftPlanMany(&plan, dim, n, nullptr, 1, (int)dist, nullptr, 1, (int)dist,
-                                  precision == NFX_F32 ? CUFFT_C2C : CUFFT_Z2Z, n_trans);
-    if (r != CUFFT_SUCCESS) return cufft_fail(r, "cufftPlanMany");
-    plans()[key] = PlanEntry{plan, ++g_tick};
+    cufftResult r = cufftCreate(&plan);
+    if (r != CUFFT_SUCCESS) return cufft_fail(r, "cufftCreate");
+    r = cufftSetAutoAllocation(plan, 0);
+    if (r == CUFFT_SUCCESS)
+      r = cufftMakePlanMany(plan, dim, n, nullptr, 1, (int)dist, nullptr, 1, (int)dist,
+                            precision == NFX_F32 ? CUFFT_C2C : CUFFT_Z2Z, n_trans, &work_bytes);
+    if (r != CUFFT_SUCCESS) {
+      cufftDestroy(plan);
+      return cufft_fail(r, "cufftMakePlanMany");
+    }
+    plans()[key] = PlanEntry{plan, work_bytes, ++g_tick};
   } else {
     plan = it->second.plan;
+    work_bytes = it->second.work_bytes;
     it->second.last_use = ++g_tick;
   }
   cufftResult r = cufftSetStream(plan, (cudaStream_t)stream);
   if (r != CUFFT_SUCCESS) return cufft_fail(r, "cufftSetStream");
+  if (work_bytes > 0) {
+    void* work = nullptr;
+    int st = stream_work_area(dev, (cudaStream_t)stream, work_bytes, &work);
+    if (st != NFX_OK) return st;
+    r = cufftSetWorkArea(plan, work);
+    if (r != CUFFT_SUCCESS) return cufft_fail(r, "cufftSetWorkArea");
+  }
   const int dir = sign > 0 ? CUFFT_INVERSE : CUFFT_FORWARD;
   if (precision == NFX_F32)
     r = cufftExecC2C(plan, (cufftComplex*)data, (cufftComplex*)data, dir);
@@ -100,9 +149,19 @@ int nfx_fft(int precision, int dim, const int nf[3], int n_trans, void* data, in
 
 int nfx_fft_cache_clear(void) {
   std::lock_guard<std::mutex> lk(g_plan_mu);
-  if (!plans().empty()) cudaDeviceSynchronize();
+  if (!plans().empty() || !work_areas().empty()) cudaDeviceSynchronize();
   for (auto& kv : plans()) cufftDestroy(kv.second.plan);
   plans().clear();
+  int cur = 0;
+  cudaGetDevice(&cur);
+  for (auto& kv : work_areas()) {
+    if (kv.second.ptr == nullptr) continue;
+    cudaSetDevice(kv.first.first);
+    cudaDeviceSynchronize();
+    cudaFree(kv.second.ptr);
+  }
+  cudaSetDevice(cur);
+  work_areas().clear();
   return NFX_OK;
 }
 

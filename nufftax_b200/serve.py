@@ -26,7 +26,11 @@ from typing import Callable, Optional, Sequence
 import numpy as np
 import torch
 
-from ._plan import PointSort, deconv_pad, deconv_shuffle, fft_inplace, precision_of
+from ctypes import byref, c_size_t, c_void_p
+
+from . import _lib
+from ._plan import (PointSort, _facs, complex_dtype, deconv_pad, deconv_shuffle, fft_inplace, make_opts, precision_of,
+                    ptr, real_dtype)
 from .grid import compute_grid_size
 from .kernel import compute_kernel_params
 from .transforms import _fft_sign_type1, _fft_sign_type2, _type3_forward
@@ -87,6 +91,26 @@ class _Slot:
         self.req: Optional[Request] = None
         self.done = torch.cuda.Event()
         self.grids: list = []
+        self.ws: Optional[torch.Tensor] = None  # sort workspace, reused by the slot's next request
+
+    def workspace(self, nbytes: int, device) -> torch.Tensor:
+        if self.ws is None or self.ws.numel() < nbytes:
+            self.ws = None
+            self.ws = torch.empty(max(nbytes, 1 << 20), dtype=torch.uint8, device=device)
+        return self.ws
+
+
+@dataclasses.dataclass
+class _Shape:
+    """Per-shape state of the one-call type 1/2 path: library options, fine grid,
+    deconvolution factors (device) and the FFT sign."""
+
+    opts: _lib.NfxOpts
+    nf: tuple
+    modes: object
+    facs: list
+    fac_ptrs: list
+    sign: int
 
 
 class NufftServer:
@@ -111,6 +135,7 @@ class NufftServer:
         self.points_cache: "collections.OrderedDict[object, tuple[PointSort, torch.cuda.Event]]" = \
             collections.OrderedDict()
         self.keep_points = keep_points
+        self.shapes: dict = {}
         self.lock = threading.Lock()
 
     # -- resident state -----------------------------------------------------------
@@ -152,13 +177,60 @@ class NufftServer:
                 self.points_cache.popitem(last=False)
         return ps
 
+    def _shape(self, req: Request, precision: int) -> _Shape:
+        key = (req.kind, tuple(req.n_modes), req.eps, req.isign, precision)
+        sh = self.shapes.get(key)
+        if sh is None:
+            kp = compute_kernel_params(req.eps)
+            nf = tuple(compute_grid_size(n, 2.0, kp.nspread) for n in req.n_modes)
+            facs = _facs(nf, req.n_modes, kp, precision, self.device)
+            if req.kind == 1:
+                sign = _fft_sign_type1(1 if req.isign is None else req.isign)
+            else:
+                sign = _fft_sign_type2(-1 if req.isign is None else req.isign)
+            sh = _Shape(make_opts(precision, nf, kp, prenorm=True), nf, _lib.int3(req.n_modes), facs,
+                        [ptr(f) for f in facs], sign)
+            self.shapes[key] = sh
+        return sh
+
+    def _run_one_call(self, req: Request, slot: _Slot):
+        """Type 1/2 on unshared points: one library call (sort, spread or interp,
+        FFT, deconvolution) on the slot's pooled workspace and a pooled grid."""
+        c = req.strengths.contiguous()
+        precision = precision_of(c.dtype)
+        xs = [x.contiguous() for x in req.coords]
+        if len(xs) != req.dim or any(x.dtype != real_dtype(precision) or x.shape != (req.M,) for x in xs):
+            raise ValueError(f"coordinates must be {req.dim} tensors of shape ({req.M},), {real_dtype(precision)}")
+        want = (req.M,) if req.kind == 1 else tuple(reversed(req.n_modes))
+        if tuple(c.shape) != want:
+            raise ValueError(f"type-{req.kind} strengths must have shape {want}")
+        sh = self._shape(req, precision)
+        lib = _lib.load()
+        nbytes = c_size_t(0)
+        _lib.check(lib.nfx_sort_workspace_bytes(byref(sh.opts), req.M, byref(nbytes)), "nfx_sort_workspace_bytes")
+        ws = slot.workspace(int(nbytes.value), self.device)
+        fw = self._grid((1,) + sh.nf[::-1], c.dtype, slot)
+        xyz = [ptr(x) for x in xs] + [None] * (3 - len(xs))
+        stream = c_void_p(slot.stream.cuda_stream)
+        if req.kind == 1:
+            out = torch.empty(tuple(reversed(req.n_modes)), dtype=complex_dtype(precision), device=self.device)
+            _lib.check(lib.nfx_nufft1(byref(sh.opts), sh.modes, *xyz, req.M, ptr(c), 1, sh.sign, *sh.fac_ptrs,
+                                      ptr(fw), ptr(out), ptr(ws), ws.numel(), stream), "nfx_nufft1")
+        else:
+            out = torch.empty(req.M, dtype=complex_dtype(precision), device=self.device)
+            _lib.check(lib.nfx_nufft2(byref(sh.opts), sh.modes, *xyz, req.M, ptr(c), 1, sh.sign, *sh.fac_ptrs,
+                                      ptr(fw), ptr(out), ptr(ws), ws.numel(), stream), "nfx_nufft2")
+        req.result = out
+
     # -- execution ------------------------------------------------------------------
     def _run(self, req: Request, slot: _Slot):
         with torch.cuda.device(self.device), torch.cuda.stream(slot.stream):
             if req.make_inputs is not None:
                 req.coords, req.strengths, req.targets = req.make_inputs(self.device)
             kp = compute_kernel_params(req.eps)
-            if req.kind == 1:
+            if req.kind in (1, 2) and req.points_id is None:
+                self._run_one_call(req, slot)
+            elif req.kind == 1:
                 isign = 1 if req.isign is None else req.isign
                 nf = tuple(compute_grid_size(n, 2.0, kp.nspread) for n in req.n_modes)
                 ps = self._sorted(req, req.coords, nf, kp, slot)

@@ -81,3 +81,78 @@ def test_budget_serialises_large_requests():
     assert len(done) == 12 and peak <= budget
     for r in reqs:
         assert rel_l2(r.result.cpu().numpy(), _alone(r).cpu().numpy()) <= 2e-6
+
+
+@pytest.mark.parametrize("dim", [1, 2, 3])
+@pytest.mark.parametrize("dtype", [torch.complex64, torch.complex128])
+def test_one_call_entry_points_match_api(dim, dtype):
+    """nfx_nufft1 / nfx_nufft2 (sort + spread/interp + FFT + deconvolution in one
+    library call, two transforms) equal the public API transform by transform."""
+    from ctypes import byref, c_size_t, c_void_p
+
+    from nufftax_b200 import _lib
+    from nufftax_b200._plan import _facs, make_opts, ptr
+    from nufftax_b200.grid import compute_grid_size
+    from nufftax_b200.kernel import compute_kernel_params
+
+    dev = cuda_device()
+    rng = np.random.default_rng(20 + dim)
+    eps = 1e-6 if dtype == torch.complex64 else 1e-9
+    prec = _lib.NFX_F32 if dtype == torch.complex64 else _lib.NFX_F64
+    rdt = torch.float32 if dtype == torch.complex64 else torch.float64
+    M, nt = 3000, 2
+    nm = (40, 24, 16)[:dim]
+    X = [torch.from_numpy(rng.uniform(-np.pi, np.pi, M)).to(dev, rdt) for _ in range(dim)]
+    c = torch.from_numpy(rng.standard_normal((nt, M)) + 1j * rng.standard_normal((nt, M))).to(dev, dtype)
+    f = torch.from_numpy(rng.standard_normal((nt,) + nm[::-1]) + 1j * rng.standard_normal((nt,) + nm[::-1])).to(
+        dev, dtype)
+    kp = compute_kernel_params(eps)
+    nf = tuple(compute_grid_size(n, 2.0, kp.nspread) for n in nm)
+    o = make_opts(prec, nf, kp, prenorm=True)
+    lib = _lib.load()
+    nb_ = c_size_t(0)
+    assert lib.nfx_sort_workspace_bytes(byref(o), M, byref(nb_)) == 0
+    ws = torch.empty(nb_.value, dtype=torch.uint8, device=dev)
+    fw = torch.empty((nt,) + nf[::-1], dtype=dtype, device=dev)
+    facs = [ptr(t) for t in _facs(nf, nm, kp, prec, dev)]
+    xyz = [ptr(x) for x in X] + [None] * (3 - dim)
+    st = c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    F = torch.empty((nt,) + nm[::-1], dtype=dtype, device=dev)
+    C = torch.empty((nt, M), dtype=dtype, device=dev)
+    # type 1 with isign +1 runs the FFT with sign +1; type 2 with isign -1 with sign -1
+    assert lib.nfx_nufft1(byref(o), _lib.int3(nm), *xyz, M, ptr(c), nt, 1, *facs, ptr(fw), ptr(F), ptr(ws),
+                          ws.numel(), st) == 0, lib.nfx_last_error()
+    assert lib.nfx_nufft2(byref(o), _lib.int3(nm), *xyz, M, ptr(f), nt, -1, *facs, ptr(fw), ptr(C), ptr(ws),
+                          ws.numel(), st) == 0, lib.nfx_last_error()
+    t1 = {1: nb.nufft1d1, 2: nb.nufft2d1, 3: nb.nufft3d1}[dim]
+    t2 = {1: nb.nufft1d2, 2: nb.nufft2d2, 3: nb.nufft3d2}[dim]
+    tol = 2e-6 if dtype == torch.complex64 else 1e-12
+    for k in range(nt):
+        r1 = t1(*X, c[k], nm[0] if dim == 1 else nm, eps=eps, isign=1)
+        r2 = t2(*X, f[k], eps=eps, isign=-1)
+        assert rel_l2(F[k].cpu().numpy(), r1.cpu().numpy()) <= tol
+        assert rel_l2(C[k].cpu().numpy(), r2.cpu().numpy()) <= tol
+
+
+def test_fft_same_plan_concurrent_streams():
+    """One cached cuFFT plan launched on several streams at once: each stream has
+    its own work area, so every grid gets its own forward transform."""
+    from nufftax_b200._plan import fft_inplace
+
+    dev = cuda_device()
+    g = torch.Generator(device=dev)
+    g.manual_seed(3)
+    shape = (1, 90, 150, 150)  # mixed radix: cuFFT needs a work area
+    xs = [torch.complex(torch.randn(shape, device=dev, generator=g), torch.randn(shape, device=dev, generator=g))
+          for _ in range(6)]
+    refs = [torch.fft.fftn(x, dim=(-3, -2, -1)) for x in xs]
+    ys = [x.clone() for x in xs]
+    streams = [torch.cuda.Stream(dev) for _ in range(3)]
+    torch.cuda.synchronize()
+    for i, y in enumerate(ys):
+        s = streams[i % 3]
+        with torch.cuda.stream(s):
+            fft_inplace(y, 3, -1)
+    torch.cuda.synchronize()
+    for y, r in zip(ys, refs):
+        assert rel_l2(y.cpu().numpy(), r.cpu().numpy()) <= 1e-5
