@@ -159,6 +159,13 @@ int nfx_deconv_pad(int precision, int dim, const int nf[3], const int n_modes[3]
  * also with the same plan: the cuFFT work area belongs to the stream (one per
  * device and stream handle, stream-ordered cudaMallocAsync, grown as needed). */
 int nfx_fft(int precision, int dim, const int nf[3], int n_trans, void* data, int sign, void* stream);
+/* The same transform on a caller-owned work area of at least nfx_fft_work_bytes
+ * bytes (NULL when that is 0).  This is the form to capture in a CUDA graph:
+ * nfx_fft refuses a capturing stream, since the graph would keep a work area
+ * that later calls on the same stream handle reuse or replace. */
+int nfx_fft_work_bytes(int precision, int dim, const int nf[3], int n_trans, size_t* bytes);
+int nfx_fft_ws(int precision, int dim, const int nf[3], int n_trans, void* data, int sign, void* work,
+               size_t work_bytes, void* stream);
 /* Destroy the cached plans and free the streams' work areas (synchronises the devices). */
 int nfx_fft_cache_clear(void);
 /* Bound the plan cache (default 1024 plans); the least recently used plan is

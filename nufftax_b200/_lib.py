@@ -99,6 +99,8 @@ _SIGNATURES = {
                            c_int),
     "nfx_deconv_pad": ([c_int, c_int, POINTER(c_int), POINTER(c_int), _vp, _vp, _vp, _vp, _vp, c_int, _vp], c_int),
     "nfx_fft": ([c_int, c_int, POINTER(c_int), c_int, _vp, c_int, _vp], c_int),
+    "nfx_fft_work_bytes": ([c_int, c_int, POINTER(c_int), c_int, POINTER(c_size_t)], c_int),
+    "nfx_fft_ws": ([c_int, c_int, POINTER(c_int), c_int, _vp, c_int, _vp, c_size_t, _vp], c_int),
     "nfx_nufft1": ([POINTER(NfxOpts), POINTER(c_int), _vp, _vp, _vp, c_int64, _vp, c_int, c_int, _vp, _vp, _vp, _vp,
                     _vp, _vp, c_size_t, _vp], c_int),
     "nfx_nufft2": ([POINTER(NfxOpts), POINTER(c_int), _vp, _vp, _vp, c_int64, _vp, c_int, c_int, _vp, _vp, _vp, _vp,

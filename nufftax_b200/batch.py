@@ -19,7 +19,7 @@ are read at every run, so they may be updated in place between runs.
 from __future__ import annotations
 
 import ctypes
-from ctypes import byref, c_int, c_int64, c_void_p
+from ctypes import byref, c_int, c_int64, c_size_t, c_void_p
 from typing import Sequence
 
 import torch
@@ -81,6 +81,14 @@ class BatchPlan:
             self.groups.append((nf, buf))
             for i, p in enumerate(members):
                 self.fw[p] = buf[i]
+        # cuFFT work areas owned by the plan (the captured graph keeps their addresses)
+        self.fft_work = []
+        for nf, buf in self.groups:
+            nbytes = c_size_t(0)
+            with torch.cuda.device(dev):
+                _lib.check(self.lib.nfx_fft_work_bytes(self.precision, self.dim, _lib.int3(nf), int(buf.shape[0]),
+                                                       byref(nbytes)), "nfx_fft_work_bytes")
+            self.fft_work.append(torch.empty(max(int(nbytes.value), 1), dtype=torch.uint8, device=dev))
 
         # sort workspaces and batch problem tables
         self.opts = _lib.NfxOpts()
@@ -201,8 +209,9 @@ class BatchPlan:
         lib = self.lib
         for i, (nf, buf) in enumerate(self.groups):
             sd = self.side[i % self.n_side]
-            _lib.check(lib.nfx_fft(self.precision, self.dim, _lib.int3(nf), int(buf.shape[0]), ptr(buf), sign,
-                                   c_void_p(sd.cuda_stream)), "nfx_fft")
+            work = self.fft_work[i]
+            _lib.check(lib.nfx_fft_ws(self.precision, self.dim, _lib.int3(nf), int(buf.shape[0]), ptr(buf), sign,
+                                      ptr(work), work.numel(), c_void_p(sd.cuda_stream)), "nfx_fft_ws")
 
     def _enqueue(self):
         lib = self.lib

@@ -80,17 +80,11 @@ int stream_work_area(int dev, cudaStream_t s, size_t bytes, void** out) {
   *out = w.ptr;
   return NFX_OK;
 }
-}  // namespace
 
-}  // namespace nfx
-
-using namespace nfx;
-
-extern "C" {
-
-int nfx_fft(int precision, int dim, const int nf[3], int n_trans, void* data, int sign, void* stream) {
-  if ((precision != NFX_F32 && precision != NFX_F64) || dim < 1 || dim > 3 || nf == nullptr || n_trans < 1 ||
-      data == nullptr || (sign != 1 && sign != -1)) {
+// The cached plan of (current device, precision, nf, n_trans) and its work-area size.
+// Call with g_plan_mu held.
+int get_plan(int precision, int dim, const int nf[3], int n_trans, cufftHandle* plan, size_t* work_bytes) {
+  if ((precision != NFX_F32 && precision != NFX_F64) || dim < 1 || dim > 3 || nf == nullptr || n_trans < 1) {
     set_error("invalid nfx_fft arguments");
     return NFX_ERR_INVALID;
   }
@@ -107,34 +101,32 @@ int nfx_fft(int precision, int dim, const int nf[3], int n_trans, void* data, in
   int dev = 0;
   cudaGetDevice(&dev);
   PlanKey key(dev, precision, dim, nf[0], dim > 1 ? nf[1] : 1, dim > 2 ? nf[2] : 1, n_trans);
-  std::lock_guard<std::mutex> lk(g_plan_mu);
-  cufftHandle plan;
   auto it = plans().find(key);
-  size_t work_bytes = 0;
-  if (it == plans().end()) {
-    evict_if_full();
-    cufftResult r = cufftCreate(&plan);
-    if (r != CUFFT_SUCCESS) return cufft_fail(r, "cufftCreate");
-    r = cufftSetAutoAllocation(plan, 0);
-    if (r == CUFFT_SUCCESS)
-      r = cufftMakePlanMany(plan, dim, n, nullptr, 1, (int)dist, nullptr, 1, (int)dist,
-                            precision == NFX_F32 ? CUFFT_C2C : CUFFT_Z2Z, n_trans, &work_bytes);
-    if (r != CUFFT_SUCCESS) {
-      cufftDestroy(plan);
-      return cufft_fail(r, "cufftMakePlanMany");
-    }
-    plans()[key] = PlanEntry{plan, work_bytes, ++g_tick};
-  } else {
-    plan = it->second.plan;
-    work_bytes = it->second.work_bytes;
+  if (it != plans().end()) {
+    *plan = it->second.plan;
+    *work_bytes = it->second.work_bytes;
     it->second.last_use = ++g_tick;
+    return NFX_OK;
   }
-  cufftResult r = cufftSetStream(plan, (cudaStream_t)stream);
+  evict_if_full();
+  cufftResult r = cufftCreate(plan);
+  if (r != CUFFT_SUCCESS) return cufft_fail(r, "cufftCreate");
+  r = cufftSetAutoAllocation(*plan, 0);
+  if (r == CUFFT_SUCCESS)
+    r = cufftMakePlanMany(*plan, dim, n, nullptr, 1, (int)dist, nullptr, 1, (int)dist,
+                          precision == NFX_F32 ? CUFFT_C2C : CUFFT_Z2Z, n_trans, work_bytes);
+  if (r != CUFFT_SUCCESS) {
+    cufftDestroy(*plan);
+    return cufft_fail(r, "cufftMakePlanMany");
+  }
+  plans()[key] = PlanEntry{*plan, *work_bytes, ++g_tick};
+  return NFX_OK;
+}
+
+int exec_plan(cufftHandle plan, int precision, void* data, int sign, void* work, cudaStream_t stream) {
+  cufftResult r = cufftSetStream(plan, stream);
   if (r != CUFFT_SUCCESS) return cufft_fail(r, "cufftSetStream");
-  if (work_bytes > 0) {
-    void* work = nullptr;
-    int st = stream_work_area(dev, (cudaStream_t)stream, work_bytes, &work);
-    if (st != NFX_OK) return st;
+  if (work != nullptr) {
     r = cufftSetWorkArea(plan, work);
     if (r != CUFFT_SUCCESS) return cufft_fail(r, "cufftSetWorkArea");
   }
@@ -145,6 +137,72 @@ int nfx_fft(int precision, int dim, const int nf[3], int n_trans, void* data, in
     r = cufftExecZ2Z(plan, (cufftDoubleComplex*)data, (cufftDoubleComplex*)data, dir);
   if (r != CUFFT_SUCCESS) return cufft_fail(r, "cufftExec");
   return NFX_OK;
+}
+
+int check_exec_args(void* data, int sign) {
+  if (data == nullptr || (sign != 1 && sign != -1)) {
+    set_error("invalid nfx_fft arguments");
+    return NFX_ERR_INVALID;
+  }
+  return NFX_OK;
+}
+}  // namespace
+}  // namespace nfx
+
+using namespace nfx;
+
+extern "C" {
+
+int nfx_fft(int precision, int dim, const int nf[3], int n_trans, void* data, int sign, void* stream) {
+  int st = check_exec_args(data, sign);
+  if (st != NFX_OK) return st;
+  // A captured launch would keep the stream's work area, which later calls on the
+  // same stream handle reuse or replace: captures pass their own (nfx_fft_ws).
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing((cudaStream_t)stream, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone) {
+    set_error("nfx_fft: stream is capturing; use nfx_fft_ws with a work area owned by the graph");
+    return NFX_ERR_INVALID;
+  }
+  std::lock_guard<std::mutex> lk(g_plan_mu);
+  cufftHandle plan;
+  size_t work_bytes = 0;
+  st = get_plan(precision, dim, nf, n_trans, &plan, &work_bytes);
+  if (st != NFX_OK) return st;
+  void* work = nullptr;
+  if (work_bytes > 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    st = stream_work_area(dev, (cudaStream_t)stream, work_bytes, &work);
+    if (st != NFX_OK) return st;
+  }
+  return exec_plan(plan, precision, data, sign, work, (cudaStream_t)stream);
+}
+
+int nfx_fft_work_bytes(int precision, int dim, const int nf[3], int n_trans, size_t* bytes) {
+  if (bytes == nullptr) {
+    set_error("nfx_fft_work_bytes: bytes is NULL");
+    return NFX_ERR_INVALID;
+  }
+  std::lock_guard<std::mutex> lk(g_plan_mu);
+  cufftHandle plan;
+  return get_plan(precision, dim, nf, n_trans, &plan, bytes);
+}
+
+int nfx_fft_ws(int precision, int dim, const int nf[3], int n_trans, void* data, int sign, void* work,
+               size_t work_bytes, void* stream) {
+  int st = check_exec_args(data, sign);
+  if (st != NFX_OK) return st;
+  std::lock_guard<std::mutex> lk(g_plan_mu);
+  cufftHandle plan;
+  size_t need = 0;
+  st = get_plan(precision, dim, nf, n_trans, &plan, &need);
+  if (st != NFX_OK) return st;
+  if (need > 0 && (work == nullptr || work_bytes < need)) {
+    set_error("nfx_fft_ws: work area of " + std::to_string(work_bytes) + " bytes, plan needs " +
+              std::to_string(need));
+    return NFX_ERR_WORKSPACE;
+  }
+  return exec_plan(plan, precision, data, sign, need > 0 ? work : nullptr, (cudaStream_t)stream);
 }
 
 int nfx_fft_cache_clear(void) {

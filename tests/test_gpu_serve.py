@@ -135,14 +135,14 @@ def test_one_call_entry_points_match_api(dim, dtype):
 
 
 def test_fft_same_plan_concurrent_streams():
-    """One cached cuFFT plan launched on several streams at once: each stream has
-    its own work area, so every grid gets its own forward transform."""
+    """One cached cuFFT plan launched on several streams at once (each stream with
+    its own work area) gives every grid its own forward transform."""
     from nufftax_b200._plan import fft_inplace
 
     dev = cuda_device()
     g = torch.Generator(device=dev)
     g.manual_seed(3)
-    shape = (1, 90, 150, 150)  # mixed radix: cuFFT needs a work area
+    shape = (1, 16, 64, 1009)  # a prime axis (Bluestein)
     xs = [torch.complex(torch.randn(shape, device=dev, generator=g), torch.randn(shape, device=dev, generator=g))
           for _ in range(6)]
     refs = [torch.fft.fftn(x, dim=(-3, -2, -1)) for x in xs]
@@ -156,3 +156,55 @@ def test_fft_same_plan_concurrent_streams():
     torch.cuda.synchronize()
     for y, r in zip(ys, refs):
         assert rel_l2(y.cpu().numpy(), r.cpu().numpy()) <= 1e-5
+
+
+def test_fft_caller_work_area_and_capture():
+    """nfx_fft_ws runs on a caller-owned work area (too small: NFX_ERR_WORKSPACE);
+    a captured nfx_fft_ws replays correctly; nfx_fft refuses a capturing stream."""
+    from ctypes import byref, c_size_t, c_void_p
+
+    from nufftax_b200 import _lib
+    from nufftax_b200._plan import fft_inplace, ptr
+
+    dev = cuda_device()
+    lib = _lib.load()
+    nf = (150, 150, 90)
+    nb_ = c_size_t(0)
+    with torch.cuda.device(dev):
+        assert lib.nfx_fft_work_bytes(_lib.NFX_F32, 3, _lib.int3(nf), 1, byref(nb_)) == 0
+    assert nb_.value > 0
+    g = torch.Generator(device=dev)
+    g.manual_seed(4)
+    x = torch.complex(torch.randn((1,) + nf[::-1], device=dev, generator=g),
+                      torch.randn((1,) + nf[::-1], device=dev, generator=g))
+    ref = torch.fft.fftn(x, dim=(-3, -2, -1))
+    work = torch.empty(nb_.value, dtype=torch.uint8, device=dev)
+    y = x.clone()
+    st = torch.cuda.current_stream(dev)
+    assert lib.nfx_fft_ws(_lib.NFX_F32, 3, _lib.int3(nf), 1, ptr(y), -1, ptr(work), nb_.value - 1,
+                          c_void_p(st.cuda_stream)) \
+        == _lib.NFX_ERR_WORKSPACE
+    assert lib.nfx_fft_ws(_lib.NFX_F32, 3, _lib.int3(nf), 1, ptr(y), -1, ptr(work), work.numel(),
+                          c_void_p(st.cuda_stream)) == 0
+    assert rel_l2(y.cpu().numpy(), ref.cpu().numpy()) <= 1e-5
+    # captured: the graph keeps the caller's work area
+    y.copy_(x)
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    refused = None
+    with torch.cuda.graph(graph):
+        cs = torch.cuda.current_stream(dev)
+        refused = lib.nfx_fft(_lib.NFX_F32, 3, _lib.int3(nf), 1, ptr(y), -1, c_void_p(cs.cuda_stream))
+        assert lib.nfx_fft_ws(_lib.NFX_F32, 3, _lib.int3(nf), 1, ptr(y), -1, ptr(work), work.numel(),
+                              c_void_p(cs.cuda_stream)) == 0
+    assert refused == _lib.NFX_ERR_INVALID
+    for _ in range(2):
+        y.copy_(x)
+        graph.replay()
+        torch.cuda.synchronize()
+        assert rel_l2(y.cpu().numpy(), ref.cpu().numpy()) <= 1e-5
+    del graph
+    # the per-stream path is unaffected
+    y.copy_(x)
+    fft_inplace(y, 3, -1)
+    assert rel_l2(y.cpu().numpy(), ref.cpu().numpy()) <= 1e-5
