@@ -719,12 +719,195 @@ __device__ __forceinline__ void stage_tile(const Geom& g, const int o[3], const 
 }
 
 // ---------------------------------------------------------------------------
+// 3D interpolation, one lane group per point.  GL lanes (the power
+// of two >= NS) share a point: lane kx = lane % GL reads footprint column kx of
+// every (ky, kz) row.  The 32 / GL points of one warp instruction are
+// consecutive in cell order, so their rows overlap in shared memory (few
+// wavefronts; thread-per-point reads of 32 scattered footprints conflicted on
+// about half of theirs).  Each lane computes only its own column's weight per
+// axis; the y and z weights reach the other lanes of the group by shuffles, and
+// the group sums its columns with a butterfly of shuffles.
+// ---------------------------------------------------------------------------
+template <int NS>
+__host__ __device__ constexpr int group_lanes() {
+  return NS <= 4 ? 4 : (NS <= 8 ? 8 : 16);
+}
+
+// Weight q of one axis: the same arithmetic as axis_weights for that q (cq =
+// the polynomial coefficients of q when the float polynomial is in use).
+template <typename T, int NS>
+__device__ __forceinline__ T axis_weight_q(const PointArgs<T>& a, const float (&cq)[kPolyEvalDeg + 1], int i0, T xs,
+                                           int q) {
+  if (std::is_same<T, float>::value && a.poly.deg > 0) {
+    const float v = 2.0f * (float)(xs - (T)i0) - (float)(NS - 1);
+    float h = cq[kPolyEvalDeg];
+#pragma unroll
+    for (int d = kPolyEvalDeg - 1; d >= 0; --d) h = fmaf(h, v, cq[d]);
+    return (T)h;
+  }
+  return es_weight(rn_sub((T)(i0 + q), xs), a.beta, a.kc);
+}
+
+// Folded coordinates, left cells and tile offset of point p (false: outside
+// its bin's tile, see footprint).
+template <typename T, int NS>
+__device__ __forceinline__ bool group_point(const PointArgs<T>& a, int p, const int o[3], int row, int plane, int& off,
+                                            T (&xs)[3], int (&i0)[3]) {
+  const Geom& g = a.g;
+  bool inside = true;
+  off = 0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    xs[d] = scaled_coord(coord(a, d, p), g.nf[d], g.prenorm);
+    i0[d] = left_cell<T, NS>(xs[d]);
+    const int l = wrap_index(i0[d], g.nf[d]) - o[d];
+    inside = inside && (unsigned)l < (unsigned)g.tile[d];
+    off += l * (d == 0 ? 1 : (d == 1 ? row : plane));
+  }
+  return inside;
+}
+
+// One round of 32 points for a warp: lane L folds point kb + L (perm gather,
+// coordinates, left cells, tile offset; off = -1 outside the tile), so the
+// gathers of 32 points are in flight together; the lane groups then take the
+// points PPW at a time by shuffles (group_take).
+template <typename T>
+struct WarpPoints {
+  int p, off;
+  T xs[3];
+  int i0[3];
+};
+
+template <typename T, int NS>
+__device__ __forceinline__ WarpPoints<T> warp_points(const PointArgs<T>& a, int kb, int k1, const int o[3], int row,
+                                                     int plane) {
+  WarpPoints<T> w;
+  const int k = kb + (threadIdx.x & 31);
+  w.p = 0;
+  w.off = -1;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    w.xs[d] = (T)0;
+    w.i0[d] = 0;
+  }
+  if (k < k1) {
+    w.p = a.s.perm[k];
+    int off;
+    const bool inside = group_point<T, NS>(a, w.p, o, row, plane, off, w.xs, w.i0);
+    w.off = inside ? off : -1;
+  }
+  return w;
+}
+
+template <typename T>
+__device__ __forceinline__ WarpPoints<T> group_take(const WarpPoints<T>& w, int src) {
+  constexpr unsigned kAll = 0xffffffffu;
+  WarpPoints<T> r;
+  r.p = __shfl_sync(kAll, w.p, src);
+  r.off = __shfl_sync(kAll, w.off, src);
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    r.xs[d] = __shfl_sync(kAll, w.xs[d], src);
+    r.i0[d] = __shfl_sync(kAll, w.i0[d], src);
+  }
+  return r;
+}
+
+template <typename T, int NS, int NW>
+__device__ __forceinline__ void interp3_group(const PointArgs<T>& a, const cplx_t<T>* __restrict__ fw,
+                                              cplx_t<T>* __restrict__ cout, int sidx, unsigned char* smem_raw) {
+  using CT = cplx_t<T>;
+  constexpr int GL = group_lanes<NS>();
+  constexpr int PPW = 32 / GL;
+  constexpr unsigned kAll = 0xffffffffu;
+  CT* s_tile = reinterpret_cast<CT*>(smem_raw);
+  const Geom& g = a.g;
+  const int row = g.pitch;
+  const int plane = g.pitch * g.pad[1];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int kx = lane % GL;
+  const int leader = lane - kx;
+  const bool col_on = kx < NS;
+  float cq[kPolyEvalDeg + 1];  // this lane's coefficients (constant-indexed parameter reads)
+#pragma unroll
+  for (int d = 0; d <= kPolyEvalDeg; ++d) cq[d] = a.poly.a[0][d];
+#pragma unroll
+  for (int q = 1; q < NS; ++q) {
+    if (kx == q) {
+#pragma unroll
+      for (int d = 0; d <= kPolyEvalDeg; ++d) cq[d] = a.poly.a[q][d];
+    }
+  }
+  const int b = a.s.sub_bin[sidx];
+  const int k0 = a.s.sub_start[sidx];
+  const int k1 = min(k0 + a.s.maxsub, a.s.bin_start[b + 1]);
+  int o[3];
+  bin_origin(g, b, o[0], o[1], o[2]);
+  for (int t = 0; t < a.n_trans; ++t) {
+    __syncthreads();
+    stage_tile<T>(g, o, fw + (int64_t)t * a.grid_stride, s_tile);
+    __syncthreads();
+    for (int kb = k0 + warp * 32; kb < k1; kb += NW * 32) {  // warp-uniform
+      const WarpPoints<T> wp = warp_points<T, NS>(a, kb, k1, o, row, plane);
+      const int npts = min(32, k1 - kb);
+      for (int j0 = 0; j0 < npts; j0 += PPW) {
+        const int j = j0 + lane / GL;
+        const bool valid = j < npts;
+        const WarpPoints<T> pt = group_take(wp, valid ? j : 0);
+        const bool on = col_on && pt.off >= 0;
+        const T wx = axis_weight_q<T, NS>(a, cq, pt.i0[0], pt.xs[0], kx);
+        const T wyq = axis_weight_q<T, NS>(a, cq, pt.i0[1], pt.xs[1], kx);
+        const T wzq = axis_weight_q<T, NS>(a, cq, pt.i0[2], pt.xs[2], kx);
+        T wy[NS], wz[NS];
+#pragma unroll
+        for (int q = 0; q < NS; ++q) {
+          wy[q] = __shfl_sync(kAll, wyq, leader + q);
+          wz[q] = __shfl_sync(kAll, wzq, leader + q);
+        }
+        CT s;
+        s.x = s.y = (T)0;
+        if (on) {
+          const CT* base = s_tile + pt.off + kx;
+          // one independent accumulator per z plane: NS chains in flight
+          CT acc[NS];
+#pragma unroll
+          for (int kz = 0; kz < NS; ++kz) acc[kz].x = acc[kz].y = (T)0;
+#pragma unroll
+          for (int ky = 0; ky < NS; ++ky) {
+#pragma unroll
+            for (int kz = 0; kz < NS; ++kz) acc[kz] = fma2(splat2(wy[ky]), base[kz * plane + ky * row], acc[kz]);
+          }
+#pragma unroll
+          for (int kz = 0; kz < NS; ++kz) s = fma2(splat2(wz[kz]), acc[kz], s);
+        }
+        T sr = on ? s.x * wx : (T)0, si = on ? s.y * wx : (T)0;
+#pragma unroll
+        for (int m = GL / 2; m >= 1; m >>= 1) {
+          sr += __shfl_xor_sync(kAll, sr, m);
+          si += __shfl_xor_sync(kAll, si, m);
+        }
+        if (valid && kx == 0) {
+          CT r;
+          r.x = sr;
+          r.y = si;
+          cout[(int64_t)t * a.M + pt.p] = r;
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Interp
 // ---------------------------------------------------------------------------
 template <typename T, int DIM, int NS, int NW>
 __device__ __forceinline__ void interp_subproblem(const PointArgs<T>& a, const cplx_t<T>* __restrict__ fw,
                                                   cplx_t<T>* __restrict__ cout, int sidx, unsigned char* smem_raw) {
   using CT = cplx_t<T>;
+  if constexpr (DIM == 3) {
+    interp3_group<T, NS, NW>(a, fw, cout, sidx, smem_raw);
+    return;
+  }
   CT* s_tile = reinterpret_cast<CT*>(smem_raw);
   const Geom& g = a.g;
   const int row = g.pitch;
