@@ -514,31 +514,46 @@ def run_reference(args):
 
 
 def run_case(args):
-    """One point set, `reps` rounds of sort + type 1 + type 2, no timing: for ncu captures."""
+    """One point set (a 2D set of the bench, or 8M uniform 3D points on 128^3
+    modes), `reps` rounds of sort + type 1 + type 2, no timing: for ncu captures."""
     import torch
 
     import nufftax_b200 as nb
 
     dev = torch.device("cuda", 0)
-    sets = [s for s in workload(seed=1234, scale=args.scale) if s["name"] == args.case]
-    s = sets[0]
-    x, y = torch.from_numpy(s["x"]).to(dev), torch.from_numpy(s["y"]).to(dev)
-    c, f = torch.from_numpy(s["c"]).to(dev), torch.from_numpy(s["f"]).to(dev)
+    if args.case == "uniform3d":
+        # 3D: M = 8e6 uniform points, 128^3 modes (nf 256^3), eps 1e-6, complex64
+        M, N3 = int(8_000_000 * args.scale), (128, 128, 128)
+        rng = np.random.default_rng(4)
+        X = [torch.from_numpy(rng.uniform(-np.pi, np.pi, M).astype(np.float32)).to(dev) for _ in range(3)]
+        c = torch.from_numpy((rng.standard_normal(M) + 1j * rng.standard_normal(M)).astype(np.complex64)).to(dev)
+        f = torch.from_numpy((rng.standard_normal(N3) + 1j * rng.standard_normal(N3)).astype(np.complex64)).to(dev)
+
+        def one():
+            nb.sort_cache.clear()
+            nb.nufft3d1(*X, c, N3, eps=EPS)
+            nb.nufft3d2(*X, f, eps=EPS)
+    else:
+        s = [s for s in workload(seed=1234, scale=args.scale) if s["name"] == args.case][0]
+        M = s["M"]
+        x, y = torch.from_numpy(s["x"]).to(dev), torch.from_numpy(s["y"]).to(dev)
+        c, f = torch.from_numpy(s["c"]).to(dev), torch.from_numpy(s["f"]).to(dev)
+
+        def one():
+            nb.sort_cache.clear()
+            nb.nufft2d1(x, y, c, N_MODES, eps=EPS)
+            nb.nufft2d2(x, y, f, eps=EPS)
     for _ in range(args.reps):
-        nb.sort_cache.clear()
-        nb.nufft2d1(x, y, c, N_MODES, eps=EPS)
-        nb.nufft2d2(x, y, f, eps=EPS)
+        one()
     torch.cuda.synchronize()
-    out = {"case": args.case, "M": s["M"], "reps": args.reps}
+    out = {"case": args.case, "M": M, "reps": args.reps}
     if args.time_calls:
         # per-call device time on one stream (CUDA events around each library call)
         from nufftax_b200 import profiling
 
         with profiling.record() as rec:
             for _ in range(args.reps):
-                nb.sort_cache.clear()
-                nb.nufft2d1(x, y, c, N_MODES, eps=EPS)
-                nb.nufft2d2(x, y, f, eps=EPS)
+                one()
         torch.cuda.synchronize()
         out["us_per_call"] = {k: round(1e3 * v["ms"] / max(v["calls"], 1), 2) for k, v in rec.summary().items()}
     print(json.dumps(out))
@@ -875,7 +890,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="nufftax_b200", choices=["nufftax_b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--case", choices=["radial", "clustered"], help="profile one point set only (no timing)")
+    ap.add_argument("--case", choices=["radial", "clustered", "uniform3d"],
+                    help="profile one point set only (no timing)")
     ap.add_argument("--reps", type=int, default=2)
     ap.add_argument("--time-calls", action="store_true", help="with --case: also print per-call device time")
     ap.add_argument("--scale", type=float, default=1.0)

@@ -748,17 +748,17 @@ __device__ __forceinline__ T axis_weight_q(const PointArgs<T>& a, const float (&
   return es_weight(rn_sub((T)(i0 + q), xs), a.beta, a.kc);
 }
 
-// Folded coordinates, left cells and tile offset of point p (false: outside
-// its bin's tile, see footprint).
+// Folded coordinates, left cells and tile offset of a point with raw
+// coordinates xv (false: outside its bin's tile, see footprint).
 template <typename T, int NS>
-__device__ __forceinline__ bool group_point(const PointArgs<T>& a, int p, const int o[3], int row, int plane, int& off,
-                                            T (&xs)[3], int (&i0)[3]) {
+__device__ __forceinline__ bool group_point(const PointArgs<T>& a, const T (&xv)[3], const int o[3], int row,
+                                            int plane, int& off, T (&xs)[3], int (&i0)[3]) {
   const Geom& g = a.g;
   bool inside = true;
   off = 0;
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    xs[d] = scaled_coord(coord(a, d, p), g.nf[d], g.prenorm);
+    xs[d] = scaled_coord(xv[d], g.nf[d], g.prenorm);
     i0[d] = left_cell<T, NS>(xs[d]);
     const int l = wrap_index(i0[d], g.nf[d]) - o[d];
     inside = inside && (unsigned)l < (unsigned)g.tile[d];
@@ -767,10 +767,11 @@ __device__ __forceinline__ bool group_point(const PointArgs<T>& a, int p, const 
   return inside;
 }
 
-// One round of 32 points for a warp: lane L folds point kb + L (perm gather,
-// coordinates, left cells, tile offset; off = -1 outside the tile), so the
-// gathers of 32 points are in flight together; the lane groups then take the
-// points PPW at a time by shuffles (group_take).
+// One round of 32 points for a warp: lane L folds point kb + L (left cells,
+// tile offset; off = -1 outside the tile); the lane groups then take the
+// points PPW at a time by shuffles (group_take).  The gathers are pipelined
+// across rounds: the permutation entries two rounds ahead and the coordinates
+// one round ahead are in flight while a round is processed.
 template <typename T>
 struct WarpPoints {
   int p, off;
@@ -778,22 +779,31 @@ struct WarpPoints {
   int i0[3];
 };
 
-template <typename T, int NS>
-__device__ __forceinline__ WarpPoints<T> warp_points(const PointArgs<T>& a, int kb, int k1, const int o[3], int row,
-                                                     int plane) {
-  WarpPoints<T> w;
+__device__ __forceinline__ int round_perm(const SortView& s, int kb, int k1) {
   const int k = kb + (threadIdx.x & 31);
-  w.p = 0;
+  return k < k1 ? s.perm[k] : -1;
+}
+
+template <typename T>
+__device__ __forceinline__ void round_coords(const PointArgs<T>& a, int p, T (&xv)[3]) {
+#pragma unroll
+  for (int d = 0; d < 3; ++d) xv[d] = p >= 0 ? coord(a, d, p) : (T)0;
+}
+
+template <typename T, int NS>
+__device__ __forceinline__ WarpPoints<T> warp_points(const PointArgs<T>& a, int p, const T (&xv)[3], const int o[3],
+                                                     int row, int plane) {
+  WarpPoints<T> w;
+  w.p = p >= 0 ? p : 0;
   w.off = -1;
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     w.xs[d] = (T)0;
     w.i0[d] = 0;
   }
-  if (k < k1) {
-    w.p = a.s.perm[k];
+  if (p >= 0) {
     int off;
-    const bool inside = group_point<T, NS>(a, w.p, o, row, plane, off, w.xs, w.i0);
+    const bool inside = group_point<T, NS>(a, xv, o, row, plane, off, w.xs, w.i0);
     w.off = inside ? off : -1;
   }
   return w;
@@ -847,8 +857,20 @@ __device__ __forceinline__ void interp3_group(const PointArgs<T>& a, const cplx_
     __syncthreads();
     stage_tile<T>(g, o, fw + (int64_t)t * a.grid_stride, s_tile);
     __syncthreads();
-    for (int kb = k0 + warp * 32; kb < k1; kb += NW * 32) {  // warp-uniform
-      const WarpPoints<T> wp = warp_points<T, NS>(a, kb, k1, o, row, plane);
+    constexpr int kStep = NW * 32;
+    int p_cur = round_perm(a.s, k0 + warp * 32, k1);
+    int p_next = round_perm(a.s, k0 + warp * 32 + kStep, k1);
+    T x_cur[3];
+    round_coords(a, p_cur, x_cur);
+    for (int kb = k0 + warp * 32; kb < k1; kb += kStep) {  // warp-uniform
+      const int p_after = round_perm(a.s, kb + 2 * kStep, k1);
+      T x_next[3];
+      round_coords(a, p_next, x_next);
+      const WarpPoints<T> wp = warp_points<T, NS>(a, p_cur, x_cur, o, row, plane);
+      p_cur = p_next;
+      p_next = p_after;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) x_cur[d] = x_next[d];
       const int npts = min(32, k1 - kb);
       for (int j0 = 0; j0 < npts; j0 += PPW) {
         const int j = j0 + lane / GL;
