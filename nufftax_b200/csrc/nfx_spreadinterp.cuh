@@ -1091,14 +1091,39 @@ __global__ void __launch_bounds__(NW * 32) k_grad(PointArgs<T> a, const cplx_t<T
       __syncthreads();
       stage_tile<T>(g, o, G + (int64_t)t * a.grid_stride, s_tile);
       __syncthreads();
-      for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
-        const int p = a.s.perm[k];
+      // gathers pipelined across iterations: the permutation two iterations
+      // ahead, coordinates and V one iteration ahead
+      const int kStep = blockDim.x;
+      int k = k0 + threadIdx.x;
+      int p_cur = k < k1 ? a.s.perm[k] : 0;
+      int p_next = k + kStep < k1 ? a.s.perm[k + kStep] : 0;
+      T x_cur[DIM];
+      CT v_cur;
+      v_cur.x = v_cur.y = (T)0;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) x_cur[d] = k < k1 ? coord(a, d, p_cur) : (T)0;
+      if (k < k1) v_cur = V[(int64_t)t * a.M + p_cur];
+      for (; k < k1; k += kStep) {
+        const int p = p_cur;
+        T xv[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) xv[d] = x_cur[d];
+        const CT vv = v_cur;
+        {
+          const bool more = k + kStep < k1;
+          const int p_after = k + 2 * kStep < k1 ? a.s.perm[k + 2 * kStep] : 0;
+#pragma unroll
+          for (int d = 0; d < DIM; ++d) x_cur[d] = more ? coord(a, d, p_next) : (T)0;
+          if (more) v_cur = V[(int64_t)t * a.M + p_next];
+          p_cur = p_next;
+          p_next = p_after;
+        }
         T w[DIM][NS], dw[DIM][NS];
         int off = 0;
         bool inside = true;
 #pragma unroll
         for (int d = 0; d < DIM; ++d) {
-          const T xs = scaled_coord(coord(a, d, p), g.nf[d], g.prenorm);
+          const T xs = scaled_coord(xv[d], g.nf[d], g.prenorm);
           const int i0 = left_cell<T, NS>(xs);
           const int l = wrap_index(i0, g.nf[d]) - o[d];
           inside = inside && (unsigned)l < (unsigned)g.tile[d];
@@ -1155,7 +1180,15 @@ __global__ void __launch_bounds__(NW * 32) k_grad(PointArgs<T> a, const cplx_t<T
             }
           }
           if (DIM == 3) {
-            const T wz = w[DIM - 1][kz], dwz = dw[DIM - 1][kz];
+            // z weights by an unrolled select: a dynamic index would put w / dw in local memory
+            T wz = (T)0, dwz = (T)0;
+#pragma unroll
+            for (int q = 0; q < NS; ++q) {
+              if (q == kz) {
+                wz = w[DIM - 1][q];
+                dwz = dw[DIM - 1][q];
+              }
+            }
             sr[0] += zr0 * wz;
             si[0] += zi0 * wz;
             sr[1] += zr1 * wz;
@@ -1181,7 +1214,6 @@ __global__ void __launch_bounds__(NW * 32) k_grad(PointArgs<T> a, const cplx_t<T
           r.y = si[0];
           out_interp[(int64_t)t * a.M + p] = r;
         }
-        const CT vv = V[(int64_t)t * a.M + p];
 #pragma unroll
         for (int d = 0; d < DIM; ++d) {
           if (douts[d] != nullptr) {
