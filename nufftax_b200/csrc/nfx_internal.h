@@ -147,8 +147,23 @@ inline size_t spread_smem_bytes(size_t real_bytes, int dim, int ns, const Geom& 
 }
 // Dynamic shared memory of the plane-owner spread (3D, sparse points): two tile
 // planes plus one slot of 4 ns + 3 reals per staged point.
+// Staging slot of the plane-owner spread, in reals of real_bytes each: c * w_x
+// pairs (2 ns), w_y and w_z (each padded to whole 16-byte vectors), then the
+// footprint's tile offset and z (padded to a vector).  The slot is a whole, odd
+// number of 16-byte vectors, so 16-byte stores of consecutive slots are
+// conflict-free and every slot starts 16-byte aligned.
+__host__ __device__ constexpr int owner_pad(int n, int m) { return (n + m - 1) / m * m; }
+__host__ __device__ constexpr int owner_slot_raw(int real_bytes, int ns) {
+  return 2 * ns + 2 * owner_pad(ns, 16 / real_bytes) + owner_pad(2, 16 / real_bytes);
+}
+__host__ __device__ constexpr int owner_slot_reals(int real_bytes, int ns) {
+  return (owner_slot_raw(real_bytes, ns) / (16 / real_bytes)) % 2 == 0 ? owner_slot_raw(real_bytes, ns) + 16 / real_bytes
+                                                                        : owner_slot_raw(real_bytes, ns);
+}
 inline size_t owner_smem_bytes(size_t real_bytes, int ns, int nw, const Geom& g) {
-  return 2 * real_bytes * (size_t)g.pad[2] * g.pad[1] * g.pitch + (size_t)nw * 32 * (4 * ns + 3) * real_bytes;
+  const int r16 = 16 / (int)real_bytes;
+  const size_t tile = (size_t)owner_pad(2 * g.pad[2] * g.pad[1] * g.pitch, r16);
+  return real_bytes * (tile + (size_t)nw * 32 * owner_slot_reals((int)real_bytes, ns));
 }
 inline size_t tile_smem_bytes(size_t real_bytes, const Geom& g) {
   return 2 * real_bytes * (size_t)g.pad[2] * g.pad[1] * g.pitch;

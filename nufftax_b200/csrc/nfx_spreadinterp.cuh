@@ -595,22 +595,38 @@ __global__ void __launch_bounds__(NW * 32) k_spread(PointArgs<T> a, const cplx_t
 // lanes, with plain shared-memory read-add-write: a plane belongs to one warp,
 // whose lanes touch distinct cells in each instruction, so no atomics are
 // needed and every cell sums its points in sorted order.  With NW = ns every
-// footprint (ns consecutive planes) gives each warp exactly one plane.
-__host__ __device__ constexpr int owner_slot_reals(int ns) { return 4 * ns + 3; }  // odd: conflict-free stores
+// footprint (ns consecutive planes) gives each warp exactly one plane.  Slots
+// are 16-byte aligned (owner_slot_reals): staged with 16-byte stores, read with
+// 8-byte loads of (c w_x re, im), (offset, z) and pairs of y weights.
+template <typename T>
+struct Vec16;
+template <>
+struct Vec16<float> {
+  using type = float4;
+};
+template <>
+struct Vec16<double> {
+  using type = double2;
+};
 
 template <typename T, int NS, int NW>
 __device__ __forceinline__ void spread_subproblem_owner(const PointArgs<T>& a, const cplx_t<T>* __restrict__ c,
                                                         cplx_t<T>* __restrict__ fw, int sidx,
                                                         unsigned char* smem_raw) {
   using CT = cplx_t<T>;
-  constexpr int SLOT = owner_slot_reals(NS);
-  constexpr int YO = 2 * NS, ZO = 3 * NS, OO = 4 * NS;  // y weights, z weights, origin (offset, z)
+  using V16 = typename Vec16<T>::type;
+  constexpr int R = 16 / (int)sizeof(T);  // reals per 16-byte vector
+  static_assert((2 * NS) % R == 0, "c * w_x pairs fill whole vectors");
+  constexpr int SLOT = owner_slot_reals((int)sizeof(T), NS);
+  constexpr int YO = 2 * NS;                 // y weights
+  constexpr int ZO = YO + owner_pad(NS, R);  // z weights
+  constexpr int OO = ZO + owner_pad(NS, R);  // origin (offset, z)
   constexpr int NT = NW * 32;
   const Geom& g = a.g;
   const int tile_cells = g.pad[2] * g.pad[1] * g.pitch;
   T* s_re = reinterpret_cast<T*>(smem_raw);
   T* s_im = s_re + tile_cells;
-  T* s_st = s_im + tile_cells;  // [NT][SLOT]
+  T* s_st = s_re + owner_pad(2 * tile_cells, R);  // [NT][SLOT], 16-byte aligned
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   const int row = g.pitch;
@@ -644,37 +660,64 @@ __device__ __forceinline__ void spread_subproblem_owner(const PointArgs<T>& a, c
           cv.x = cv.y = (T)0;
           off = 0;
         }
-        T* sp = s_st + threadIdx.x * SLOT;
+        T v[SLOT];
+#pragma unroll
+        for (int i = 0; i < SLOT; ++i) v[i] = (T)0;
 #pragma unroll
         for (int q = 0; q < NS; ++q) {
-          sp[2 * q] = cv.x * w[0][q];
-          sp[2 * q + 1] = cv.y * w[0][q];
-          sp[YO + q] = w[1][q];
-          sp[ZO + q] = w[2][q];
+          v[2 * q] = cv.x * w[0][q];
+          v[2 * q + 1] = cv.y * w[0][q];
+          v[YO + q] = w[1][q];
+          v[ZO + q] = w[2][q];
         }
-        sp[OO] = (T)off;
-        sp[OO + 1] = (T)(off / plane);  // z of the footprint origin in the tile
+        v[OO] = (T)off;
+        v[OO + 1] = (T)(off / plane);  // z of the footprint origin in the tile
+        V16* sp = reinterpret_cast<V16*>(s_st + threadIdx.x * SLOT);
+#pragma unroll
+        for (int i = 0; i < SLOT / R; ++i) {
+          V16 u;
+          if constexpr (R == 4) {
+            u.x = v[4 * i];
+            u.y = v[4 * i + 1];
+            u.z = v[4 * i + 2];
+            u.w = v[4 * i + 3];
+          } else {
+            u.x = v[2 * i];
+            u.y = v[2 * i + 1];
+          }
+          sp[i] = u;
+        }
       }
       __syncthreads();  // also orders the tile zeroing before the first adds
       const int cnt = min(NT, k1 - kb);
       for (int j = 0; j < cnt; ++j) {
         const T* sp = s_st + j * SLOT;
-        const int off = (int)sp[OO];
-        const int oz = (int)sp[OO + 1];
+        const CT org = *reinterpret_cast<const CT*>(sp + OO);  // (offset, z)
+        const int off = (int)org.x;
+        const int oz = (int)org.y;
         // this warp's planes inside [oz, oz + NS)
         for (int dz = ((warp - oz) % NW + NW) % NW; dz < NS; dz += NW) {
           const T wz = sp[ZO + dz];
           const int base = off + dz * plane + kx;
-          const T cr = sp[2 * kx], ci = sp[2 * kx + 1];
+          const CT cx = *reinterpret_cast<const CT*>(sp + 2 * kx);  // c * w_x[kx]
           if (lane_on) {
+            T wyr[IT];
+            if constexpr (IT == 2) {
+              const CT pr = *reinterpret_cast<const CT*>(sp + YO + 2 * ky0);
+              wyr[0] = pr.x;
+              wyr[1] = pr.y;
+            } else {
+#pragma unroll
+              for (int i = 0; i < IT; ++i) wyr[i] = sp[YO + ky0 * IT + i];
+            }
 #pragma unroll
             for (int i = 0; i < IT; ++i) {
               const int ky = ky0 * IT + i;
               if (ky < NS) {
-                const T wy = wz * sp[YO + ky];
+                const T wy = wz * wyr[i];
                 const int addr = base + ky * row;
-                s_re[addr] += wy * cr;
-                s_im[addr] += wy * ci;
+                s_re[addr] += wy * cx.x;
+                s_im[addr] += wy * cx.y;
               }
             }
           }
