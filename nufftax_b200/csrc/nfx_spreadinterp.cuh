@@ -987,14 +987,34 @@ __device__ __forceinline__ void interp_subproblem(const PointArgs<T>& a, const c
       __syncthreads();
       stage_tile<T>(g, o, fw + (int64_t)t * a.grid_stride, s_tile);
       __syncthreads();
-      for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
-        const int p = a.s.perm[k];
+      // gathers pipelined across iterations: the permutation two iterations
+      // ahead, the coordinates one iteration ahead
+      const int kStep = blockDim.x;
+      int k = k0 + threadIdx.x;
+      int p_cur = k < k1 ? a.s.perm[k] : 0;
+      int p_next = k + kStep < k1 ? a.s.perm[k + kStep] : 0;
+      T x_cur[DIM];
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) x_cur[d] = k < k1 ? coord(a, d, p_cur) : (T)0;
+      for (; k < k1; k += kStep) {
+        const int p = p_cur;
+        T xv[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) xv[d] = x_cur[d];
+        {
+          const bool more = k + kStep < k1;
+          const int p_after = k + 2 * kStep < k1 ? a.s.perm[k + 2 * kStep] : 0;
+#pragma unroll
+          for (int d = 0; d < DIM; ++d) x_cur[d] = more ? coord(a, d, p_next) : (T)0;
+          p_cur = p_next;
+          p_next = p_after;
+        }
         T w[DIM][NS];
         int off = 0;
         bool inside = true;
 #pragma unroll
         for (int d = 0; d < DIM; ++d) {
-          const T xs = scaled_coord(coord(a, d, p), g.nf[d], g.prenorm);
+          const T xs = scaled_coord(xv[d], g.nf[d], g.prenorm);
           const int i0 = left_cell<T, NS>(xs);
           const int l = wrap_index(i0, g.nf[d]) - o[d];
           inside = inside && (unsigned)l < (unsigned)g.tile[d];
