@@ -181,7 +181,10 @@ int nfx_fft_cache_limit(int max_plans);
  * order); nfx_nufft2 deconvolves / zero-pads f_in into fw, runs the FFT,
  * sorts and interpolates into c_out.  fac1..fac3 are the per-axis
  * deconvolution factors (device, precision's real type; unused axes NULL),
- * n_modes[d] the modes per axis; workspace of nfx_sort_workspace_bytes. */
+ * n_modes[d] the modes per axis; workspace of nfx_sort_workspace_bytes.  The
+ * FFT step uses the stream's cuFFT work area (nfx_fft), so these two refuse a
+ * capturing stream (NFX_ERR_INVALID); capture the step-by-step calls with
+ * nfx_fft_ws instead. */
 int nfx_nufft1(const nfx_opts* opts, const int n_modes[3], const void* x, const void* y, const void* z, int64_t M,
                const void* c, int n_trans, int fft_sign, const void* fac1, const void* fac2, const void* fac3, void* fw,
                void* f_out, void* workspace, size_t workspace_bytes, void* stream);
