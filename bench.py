@@ -859,8 +859,14 @@ def run_serve(args):
         server.serve([copy.copy(r) for r in reqs[:20]])
         torch.cuda.synchronize()
         server.completed = []
+        retries0 = torch.cuda.memory_stats(dev).get("num_alloc_retries", 0)
+        torch.cuda.reset_peak_memory_stats(dev)
         done = server.serve(batch, list(arrivals))
         st = server.stats(done)
+        mem = torch.cuda.memory_stats(dev)
+        # allocator retries free the cache and synchronise the device: a stall
+        st["alloc_retries"] = int(mem.get("num_alloc_retries", 0) - retries0)
+        st["peak_reserved_gb"] = round(mem.get("reserved_bytes.all.peak", 0) / 1e9, 1)
         st["offered_load"] = load
         st["offered_requests_per_s"] = rate
         out["loads"].append(st)
