@@ -40,7 +40,14 @@ def complex_dtype(precision: int) -> torch.dtype:
     return _CPLX[precision]
 
 
+_raw_stream = getattr(torch._C, "_cuda_getCurrentRawStream", None)
+
+
 def stream_of(device: torch.device) -> int:
+    """Handle of the current stream of `device` (the raw query when torch has it:
+    no Stream object per call)."""
+    if _raw_stream is not None:
+        return _raw_stream(device.index if device.index is not None else torch.cuda.current_device())
     return torch.cuda.current_stream(device).cuda_stream
 
 
@@ -53,8 +60,29 @@ def require_cuda(t: torch.Tensor, what: str) -> None:
         raise ValueError(f"{what} must be a CUDA tensor")
 
 
+_opts_cache: dict = {}
+_opts_lock = threading.Lock()
+
+
 def make_opts(precision: int, nf: Sequence[int], kp: KernelParams, prenorm: bool, tile=None,
               max_subproblem: int = 0) -> _lib.NfxOpts:
+    """Library options with default tiles filled in; a private copy of a cached
+    struct per (precision, grid, kernel, tiling) key."""
+    key = (precision, tuple(int(n) for n in nf), int(kp.nspread), float(kp.beta), float(kp.c), bool(prenorm),
+           None if tile is None else tuple(int(t) for t in tile), int(max_subproblem))
+    with _opts_lock:
+        o = _opts_cache.get(key)
+    if o is None:
+        o = _make_opts(precision, nf, kp, prenorm, tile, max_subproblem)
+        with _opts_lock:
+            if len(_opts_cache) >= 4096:
+                _opts_cache.clear()
+            _opts_cache[key] = o
+    return _lib.NfxOpts.from_buffer_copy(o)
+
+
+def _make_opts(precision: int, nf: Sequence[int], kp: KernelParams, prenorm: bool, tile,
+               max_subproblem: int) -> _lib.NfxOpts:
     o = _lib.NfxOpts()
     o.precision = precision
     o.dim = len(nf)

@@ -48,18 +48,29 @@ def record():
         _state.rec = prev
 
 
-@contextlib.contextmanager
-def span(name: str, device, launches: int | None = None):
-    rec = getattr(_state, "rec", None)
-    if rec is None:
-        yield
-        return
-    stream = torch.cuda.current_stream(device)
-    a = torch.cuda.Event(enable_timing=True)
-    b = torch.cuda.Event(enable_timing=True)
-    a.record(stream)
-    try:
-        yield
-    finally:
-        b.record(stream)
-        rec.events.append((name, a, b, LAUNCHES.get(name, 1) if launches is None else launches))
+class span:
+    """Brackets one library call with CUDA events while a `record()` is active
+    on this thread; otherwise does nothing (a plain object, no generator, so
+    the common case costs a thread-local read)."""
+
+    __slots__ = ("rec", "name", "stream", "launches", "a")
+
+    def __init__(self, name: str, device, launches: int | None = None):
+        self.rec = getattr(_state, "rec", None)
+        if self.rec is not None:
+            self.name = name
+            self.stream = torch.cuda.current_stream(device)
+            self.launches = LAUNCHES.get(name, 1) if launches is None else launches
+
+    def __enter__(self):
+        if self.rec is not None:
+            self.a = torch.cuda.Event(enable_timing=True)
+            self.a.record(self.stream)
+        return self
+
+    def __exit__(self, *exc):
+        if self.rec is not None:
+            b = torch.cuda.Event(enable_timing=True)
+            b.record(self.stream)
+            self.rec.events.append((self.name, self.a, b, self.launches))
+        return False

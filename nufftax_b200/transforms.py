@@ -104,6 +104,20 @@ def _fft_sign_type2(isign: int) -> int:
     return -1 if isign < 0 else 1
 
 
+class _NoGradCtx:
+    """Stands in for the autograd context when no input needs a gradient: the
+    forward pass then runs without autograd's bookkeeping."""
+
+    needs_input_grad = ()
+
+    def save_for_backward(self, *tensors):
+        pass
+
+
+def _needs_grad(*tensors) -> bool:
+    return torch.is_grad_enabled() and any(t.requires_grad for t in tensors)
+
+
 # ---------------------------------------------------------------------------
 # Type 1
 # ---------------------------------------------------------------------------
@@ -152,7 +166,8 @@ def _type1(coords, c, n_modes: Sequence[int], eps, isign, upsampfac):
     if c2.shape[-1] != M:
         raise ValueError("c must have M entries along its last axis")
     uf, uf_t = _split_upsampfac(upsampfac)
-    f = _Type1.apply(c2, tuple(int(n) for n in n_modes), float(eps), int(isign), uf, uf_t, *xs)
+    args = (c2, tuple(int(n) for n in n_modes), float(eps), int(isign), uf, uf_t, *xs)
+    f = _Type1.apply(*args) if _needs_grad(c2, *xs) else _Type1.forward(_NoGradCtx(), *args)
     return bd.back(f if batched else f[0])
 
 
@@ -222,7 +237,8 @@ def _type2(coords, f, eps, isign, upsampfac):
     batched = fd.ndim == dim + 1
     f2 = (fd if batched else fd.unsqueeze(0)).contiguous()
     uf, uf_t = _split_upsampfac(upsampfac)
-    c = _Type2.apply(f2, float(eps), int(isign), uf, uf_t, *xs)
+    args = (f2, float(eps), int(isign), uf, uf_t, *xs)
+    c = _Type2.apply(*args) if _needs_grad(f2, *xs) else _Type2.forward(_NoGradCtx(), *args)
     return bd.back(c if batched else c[0])
 
 
