@@ -250,6 +250,18 @@ def run_gpu(args):
         torch.cuda.synchronize()
         n_w += 1
 
+    # One more warm-up step with CUDA events around every library call: the
+    # per-call breakdown, the kernel launches of a step and the dominant single
+    # kernel (the events cost host time, so the timed loop records only that one).
+    with profiling.record() as rec0:
+        step(devsets)
+    torch.cuda.synchronize()
+    per_call = rec0.summary()
+    launches = sum(v["launches"] for v in per_call.values()) * args.steps
+    ours = {k: v for k, v in per_call.items() if k in ALG_BYTES and k != "nfx_sort_points"}
+    dom = max(ours, key=lambda k: ours[k]["ms"])
+    breakdown = {k: {"calls": v["calls"], "ms_per_step": v["ms"]} for k, v in per_call.items()}
+
     # ---- timed region: device-resident inputs ---------------------------------
     stream = torch.cuda.current_stream(dev)
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
@@ -257,7 +269,7 @@ def run_gpu(args):
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
-    with profiling.record() as rec:
+    with profiling.record(only=[dom]) as rec:
         for i in range(args.steps):
             flush.fill_(float(i))
             starts[i].record(stream)
@@ -266,22 +278,18 @@ def run_gpu(args):
     torch.cuda.synchronize()
     step_ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
     total_ms = float(sum(step_ms))
-    per_call = rec.summary()
-    launches = sum(v["launches"] for v in per_call.values())
     total_ms, value = aggregate_ranks(total_ms, points_per_step(sets) * args.steps, world, dev)
     pts = points_per_step(sets) * args.steps * world
 
-    # roofline of the dominant single kernel (the sort is eleven launches)
+    # roofline of the dominant single kernel, its launches timed live in the loop
     peak, peak_kind = measured_peaks()
-    ours = {k: v for k, v in per_call.items() if k in ALG_BYTES and k != "nfx_sort_points"}
-    dom = max(ours, key=lambda k: ours[k]["ms"])
+    live = rec.summary()[dom]
     # every step launches the dominant kernel once per point set
     alg_total = args.steps * sum(ALG_BYTES[dom](s["M"], nf, N_MODES) for s in sets)
-    n_dom = ours[dom]["calls"]
+    n_dom = live["calls"]
     alg_per_launch = alg_total / max(n_dom, 1)
-    avg_ms = ours[dom]["ms"] / max(n_dom, 1)
-    achieved = alg_total / (ours[dom]["ms"] / 1e3) / 1e9
-    breakdown = {k: {"calls": v["calls"], "ms_per_step": v["ms"] / args.steps} for k, v in per_call.items()}
+    avg_ms = live["ms"] / max(n_dom, 1)
+    achieved = alg_total / (live["ms"] / 1e3) / 1e9
 
     # ---- e2e: public API with pinned host buffers -------------------------------
     out_host = []

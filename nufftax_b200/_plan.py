@@ -248,6 +248,10 @@ class _SortCache:
     def get(self, coords, nf, kp, prenorm) -> PointSort:
         key = tuple((id(c), c.data_ptr(), c._version, c.dtype, c.shape[0]) for c in coords) + (
             tuple(nf), kp.nspread, float(kp.beta), float(kp.c), bool(prenorm))
+        if torch.cuda.is_current_stream_capturing():
+            # a sort made during capture has only been captured, not run: it
+            # belongs to the graph and never enters the cache
+            return PointSort(coords, nf, kp, prenorm)
         if self.enabled:
             with self._lock:
                 hit = self._d.get(key)
@@ -303,8 +307,17 @@ def fft_inplace(fw: torch.Tensor, dim: int, sign: int) -> torch.Tensor:
     nf = tuple(reversed(fw.shape[-dim:]))
     lib = _lib.load()
     with torch.cuda.device(fw.device), span("nfx_fft", fw.device, 0):
-        _lib.check(lib.nfx_fft(precision, dim, _lib.int3(nf), int(fw.shape[0]), ptr(fw), int(sign),
-                               c_void_p(stream_of(fw.device))), "nfx_fft")
+        if torch.cuda.is_current_stream_capturing():
+            # a captured FFT keeps its work area: take one from the graph's pool
+            nbytes = c_size_t(0)
+            _lib.check(lib.nfx_fft_work_bytes(precision, dim, _lib.int3(nf), int(fw.shape[0]), byref(nbytes)),
+                       "nfx_fft_work_bytes")
+            work = torch.empty(max(int(nbytes.value), 1), dtype=torch.uint8, device=fw.device)
+            _lib.check(lib.nfx_fft_ws(precision, dim, _lib.int3(nf), int(fw.shape[0]), ptr(fw), int(sign), ptr(work),
+                                      work.numel(), c_void_p(stream_of(fw.device))), "nfx_fft_ws")
+        else:
+            _lib.check(lib.nfx_fft(precision, dim, _lib.int3(nf), int(fw.shape[0]), ptr(fw), int(sign),
+                                   c_void_p(stream_of(fw.device))), "nfx_fft")
     return fw
 
 

@@ -25,6 +25,7 @@ LAUNCHES = {"nfx_sort_points": 8, "nfx_spread_sorted": 1, "nfx_interp_sorted": 1
 class Recorder:
     def __init__(self):
         self.events = []
+        self.only = None
 
     def summary(self):
         torch.cuda.synchronize()
@@ -38,8 +39,11 @@ class Recorder:
 
 
 @contextlib.contextmanager
-def record():
+def record(only=None):
+    """Record the library calls of this thread (only those named in `only`, if
+    given: fewer events on the host)."""
     rec = Recorder()
+    rec.only = None if only is None else frozenset(only)
     prev = getattr(_state, "rec", None)
     _state.rec = rec
     try:
@@ -57,6 +61,8 @@ class span:
 
     def __init__(self, name: str, device, launches: int | None = None):
         self.rec = getattr(_state, "rec", None)
+        if self.rec is not None and self.rec.only is not None and name not in self.rec.only:
+            self.rec = None
         if self.rec is not None:
             self.name = name
             self.stream = torch.cuda.current_stream(device)
