@@ -18,6 +18,9 @@ overlap: all uploads are queued first in the order the work needs them (x, y, f
 of each set, then c), the type 2 runs first and its result downloads while c
 uploads; consecutive steps are pipelined (a step's uploads run while the
 previous step computes), and the timed region spans all K steps.
+Inside the timed loop only the dominant kernel's library calls are bracketed
+with CUDA events (its live launch time for `roofline`); the per-call breakdown
+and the launch count come from one recorded warm-up step.
 `--impl reference` times the CPU restatement of nufftax's
 pure-JAX path (oracle/) on all host cores on a bounded sample.
 Multi-GPU runs are independent replicas (weak scaling), timed as the max over ranks.
