@@ -170,3 +170,33 @@ def test_es_polynomial_refused_for_narrow_kernel():
     deg = ctypes.c_int()
     assert lib.nfx_es_poly(kp.nspread, kp.beta, kp.c, None, byref(deg), None) == 0
     assert deg.value == 0
+
+
+def test_make_opts_cache_returns_private_copies():
+    """make_opts caches the filled struct per key but hands out copies: changing
+    one caller's options leaves the cache and other callers untouched."""
+    from nufftax_b200._plan import make_opts
+
+    kp = nb.compute_kernel_params(1e-6)
+    a = make_opts(0, (1024, 1024), kp, True)
+    b = make_opts(0, (1024, 1024), kp, True)
+    assert a is not b and bytes(a) == bytes(b)
+    a.max_subproblem = 77
+    a.tile[0] = 5
+    c = make_opts(0, (1024, 1024), kp, True)
+    assert bytes(c) == bytes(b) and c.max_subproblem == 0 and c.tile[0] == 32
+    d = make_opts(0, (1024, 1024), kp, True, tile=(16, 16))
+    assert list(d.tile)[:2] == [16, 16]
+    bad = nb.compute_kernel_params(1e-6)._replace(nspread=18)
+    for _ in range(2):  # a failed fill is not cached
+        with pytest.raises(NotImplementedError):
+            make_opts(0, (1024, 1024), bad, True)
+
+
+def test_profiling_span_is_inert_without_recorder():
+    """Outside profiling.record() a span touches no CUDA state (this runs without a GPU)."""
+    from nufftax_b200 import profiling
+
+    with profiling.span("nfx_spread_sorted", None) as s:
+        assert s.rec is None
+    assert profiling.LAUNCHES["nfx_sort_points"] >= 1
