@@ -44,7 +44,10 @@ uint64_t g_tick = 0;
 size_t g_plan_limit = 1024;
 
 // Keep at most g_plan_limit plans; the least recently used one is destroyed
-// after the device is idle (an in-flight transform may still use its work area).
+// after the device is idle (an in-flight transform may still use the plan).
+// Only calls on a stream that is not capturing evict (the synchronisation would
+// end a capture): nfx_fft_work_bytes and captured nfx_fft_ws calls let the cache
+// run over its limit until the next such call.
 void evict_if_full() {
   while (plans().size() >= g_plan_limit && !plans().empty()) {
     auto victim = plans().begin();
@@ -83,7 +86,8 @@ int stream_work_area(int dev, cudaStream_t s, size_t bytes, void** out) {
 
 // The cached plan of (current device, precision, nf, n_trans) and its work-area size.
 // Call with g_plan_mu held.
-int get_plan(int precision, int dim, const int nf[3], int n_trans, cufftHandle* plan, size_t* work_bytes) {
+int get_plan(int precision, int dim, const int nf[3], int n_trans, bool may_evict, cufftHandle* plan,
+             size_t* work_bytes) {
   if ((precision != NFX_F32 && precision != NFX_F64) || dim < 1 || dim > 3 || nf == nullptr || n_trans < 1) {
     set_error("invalid nfx_fft arguments");
     return NFX_ERR_INVALID;
@@ -108,7 +112,7 @@ int get_plan(int precision, int dim, const int nf[3], int n_trans, cufftHandle* 
     it->second.last_use = ++g_tick;
     return NFX_OK;
   }
-  evict_if_full();
+  if (may_evict) evict_if_full();
   cufftResult r = cufftCreate(plan);
   if (r != CUFFT_SUCCESS) return cufft_fail(r, "cufftCreate");
   r = cufftSetAutoAllocation(*plan, 0);
@@ -166,7 +170,7 @@ int nfx_fft(int precision, int dim, const int nf[3], int n_trans, void* data, in
   std::lock_guard<std::mutex> lk(g_plan_mu);
   cufftHandle plan;
   size_t work_bytes = 0;
-  st = get_plan(precision, dim, nf, n_trans, &plan, &work_bytes);
+  st = get_plan(precision, dim, nf, n_trans, true, &plan, &work_bytes);
   if (st != NFX_OK) return st;
   void* work = nullptr;
   if (work_bytes > 0) {
@@ -185,17 +189,20 @@ int nfx_fft_work_bytes(int precision, int dim, const int nf[3], int n_trans, siz
   }
   std::lock_guard<std::mutex> lk(g_plan_mu);
   cufftHandle plan;
-  return get_plan(precision, dim, nf, n_trans, &plan, bytes);
+  return get_plan(precision, dim, nf, n_trans, false, &plan, bytes);
 }
 
 int nfx_fft_ws(int precision, int dim, const int nf[3], int n_trans, void* data, int sign, void* work,
                size_t work_bytes, void* stream) {
   int st = check_exec_args(data, sign);
   if (st != NFX_OK) return st;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  const bool capturing =
+      cudaStreamIsCapturing((cudaStream_t)stream, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone;
   std::lock_guard<std::mutex> lk(g_plan_mu);
   cufftHandle plan;
   size_t need = 0;
-  st = get_plan(precision, dim, nf, n_trans, &plan, &need);
+  st = get_plan(precision, dim, nf, n_trans, !capturing, &plan, &need);
   if (st != NFX_OK) return st;
   if (need > 0 && (work == nullptr || work_bytes < need)) {
     set_error("nfx_fft_ws: work area of " + std::to_string(work_bytes) + " bytes, plan needs " +
