@@ -48,12 +48,6 @@ __device__ __forceinline__ unsigned peer_mask(int key, int nbits) {
   return m;
 }
 
-__host__ __device__ inline int key_bits(int nkeys) {
-  int b = 0;
-  while ((1 << b) < nkeys + 1) ++b;
-  return b;
-}
-
 // Bin of the tile holding the footprint's left cell, and that cell's index
 // inside the tile (both x-fastest), from the point's coordinates.
 template <typename T, int DIM>
