@@ -125,6 +125,20 @@ def test_spread_interp_vs_oracle(dim, nf, M, eps, prec):
 
 
 @pytest.mark.parametrize("ns_eps", [1e-1, 1e-3, 1e-5, 1e-7, 1e-9, 1e-11, 1e-13, 1e-15])
+def test_every_kernel_width_3d_float_owner(ns_eps):
+    """3D complex64 spread with fewer points than cells (the plane-owner kernel and
+    its 16-byte staging slots) at every even nspread, against the oracle; float
+    weights and sums bound the error near 1e-6 whatever the width."""
+    rng = np.random.default_rng(5)
+    kp = nb.compute_kernel_params(ns_eps)
+    nf, M = (36, 34, 40), 1500
+    X = [rng.uniform(-np.pi, np.pi, M).astype(np.float32) for _ in range(3)]
+    c = rand_c(rng, M, np.complex64)
+    fw = spread_3d(*[to_dev(x) for x in X], to_dev(c), *nf, kp).cpu().numpy()
+    assert rel_l2(fw, O.spread(X, c, nf, kp)) < 1e-5
+
+
+@pytest.mark.parametrize("ns_eps", [1e-1, 1e-3, 1e-5, 1e-7, 1e-9, 1e-11, 1e-13, 1e-15])
 def test_every_kernel_width(ns_eps):
     """Every even nspread 2..16 compiles, launches and matches (complex128)."""
     rng = np.random.default_rng(3)
