@@ -169,3 +169,18 @@ def int3(vals) -> ctypes.Array:
     for i, v in enumerate(vals):
         arr[i] = int(v)
     return arr
+
+
+_int3_cache: dict = {}
+
+
+def int3c(vals) -> ctypes.Array:
+    """int3 for read-only arguments (`const int[3]`), shared per value: the hot
+    paths pass the same grid sizes on every call."""
+    key = tuple(int(v) for v in vals)
+    arr = _int3_cache.get(key)
+    if arr is None:
+        if len(_int3_cache) >= 4096:
+            _int3_cache.clear()
+        arr = _int3_cache[key] = int3(key)
+    return arr

@@ -140,7 +140,8 @@ class PointSort:
         _lib.check(lib.nfx_sort_workspace_bytes(byref(self.opts), self.M, byref(nbytes)), "nfx_sort_workspace_bytes")
         self.ws_bytes = int(nbytes.value)
         self.ws = torch.empty(max(self.ws_bytes, 1), dtype=torch.uint8, device=self.device)
-        with torch.cuda.device(self.device), span("nfx_sort_points", self.device, sort_launches(self.opts, self.M)):
+        launches = lambda: sort_launches(self.opts, self.M)  # noqa: E731 (evaluated only when recording)
+        with torch.cuda.device(self.device), span("nfx_sort_points", self.device, launches):
             _lib.check(lib.nfx_sort_points(byref(self.opts), *self._xyz(), self.M, ptr(self.ws), self.ws_bytes,
                                            c_void_p(stream_of(self.device))), "nfx_sort_points")
 
@@ -310,13 +311,13 @@ def fft_inplace(fw: torch.Tensor, dim: int, sign: int) -> torch.Tensor:
         if torch.cuda.is_current_stream_capturing():
             # a captured FFT keeps its work area: take one from the graph's pool
             nbytes = c_size_t(0)
-            _lib.check(lib.nfx_fft_work_bytes(precision, dim, _lib.int3(nf), int(fw.shape[0]), byref(nbytes)),
+            _lib.check(lib.nfx_fft_work_bytes(precision, dim, _lib.int3c(nf), int(fw.shape[0]), byref(nbytes)),
                        "nfx_fft_work_bytes")
             work = torch.empty(max(int(nbytes.value), 1), dtype=torch.uint8, device=fw.device)
-            _lib.check(lib.nfx_fft_ws(precision, dim, _lib.int3(nf), int(fw.shape[0]), ptr(fw), int(sign), ptr(work),
+            _lib.check(lib.nfx_fft_ws(precision, dim, _lib.int3c(nf), int(fw.shape[0]), ptr(fw), int(sign), ptr(work),
                                       work.numel(), c_void_p(stream_of(fw.device))), "nfx_fft_ws")
         else:
-            _lib.check(lib.nfx_fft(precision, dim, _lib.int3(nf), int(fw.shape[0]), ptr(fw), int(sign),
+            _lib.check(lib.nfx_fft(precision, dim, _lib.int3c(nf), int(fw.shape[0]), ptr(fw), int(sign),
                                    c_void_p(stream_of(fw.device))), "nfx_fft")
     return fw
 
@@ -335,7 +336,7 @@ def deconv_shuffle(fw_hat: torch.Tensor, n_modes: Sequence[int], kp: KernelParam
     out = torch.empty((fw_hat.shape[0],) + tuple(reversed(n_modes)), dtype=fw_hat.dtype, device=fw_hat.device)
     lib = _lib.load()
     with torch.cuda.device(fw_hat.device), span("nfx_deconv_shuffle", fw_hat.device):
-        _lib.check(lib.nfx_deconv_shuffle(precision, dim, _lib.int3(nf), _lib.int3(n_modes), ptr(fs[0]), ptr(fs[1]),
+        _lib.check(lib.nfx_deconv_shuffle(precision, dim, _lib.int3c(nf), _lib.int3c(n_modes), ptr(fs[0]), ptr(fs[1]),
                                           ptr(fs[2]), ptr(fw_hat), ptr(out), int(fw_hat.shape[0]),
                                           c_void_p(stream_of(fw_hat.device))), "nfx_deconv_shuffle")
     return out
@@ -352,7 +353,7 @@ def deconv_pad(f: torch.Tensor, nf: Sequence[int], kp: KernelParams, out: torch.
         out = torch.empty((f.shape[0],) + tuple(reversed(nf)), dtype=f.dtype, device=f.device)
     lib = _lib.load()
     with torch.cuda.device(f.device), span("nfx_deconv_pad", f.device):
-        _lib.check(lib.nfx_deconv_pad(precision, dim, _lib.int3(nf), _lib.int3(n_modes), ptr(fs[0]), ptr(fs[1]),
+        _lib.check(lib.nfx_deconv_pad(precision, dim, _lib.int3c(nf), _lib.int3c(n_modes), ptr(fs[0]), ptr(fs[1]),
                                       ptr(fs[2]), ptr(f), ptr(out), int(f.shape[0]), c_void_p(stream_of(f.device))),
                    "nfx_deconv_pad")
     return out

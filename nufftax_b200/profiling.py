@@ -55,7 +55,8 @@ def record(only=None):
 class span:
     """Brackets one library call with CUDA events while a `record()` is active
     on this thread; otherwise does nothing (a plain object, no generator, so
-    the common case costs a thread-local read)."""
+    the common case costs a thread-local read).  `launches` (kernels the call
+    launches) may be a callable, evaluated only when recording."""
 
     __slots__ = ("rec", "name", "stream", "launches", "a")
 
@@ -66,6 +67,8 @@ class span:
         if self.rec is not None:
             self.name = name
             self.stream = torch.cuda.current_stream(device)
+            if callable(launches):  # computed only when recording
+                launches = launches()
             self.launches = LAUNCHES.get(name, 1) if launches is None else launches
 
     def __enter__(self):

@@ -58,6 +58,7 @@ class Request:
     arrival: float = 0.0
     # filled by the server
     result: Optional[torch.Tensor] = None
+    error: Optional[str] = None  # set when the request could not run (it fails alone)
     admitted: float = 0.0
     finished: float = 0.0
     nbytes: int = 0
@@ -273,7 +274,14 @@ class NufftServer:
                     slot.req = req
                     self.in_use += req.nbytes
                     req.admitted = time.perf_counter()
-                    self._run(req, slot)
+                    try:
+                        self._run(req, slot)
+                    except (ValueError, TypeError, RuntimeError, NotImplementedError) as e:
+                        # a malformed request fails alone; its slot is released by
+                        # the normal completion path once its stream is idle
+                        req.error = f"{type(e).__name__}: {e}"
+                        req.result = None
+                        slot.done.record(slot.stream)
                 else:
                     i += 1
 
@@ -324,7 +332,8 @@ class NufftServer:
         return self.completed
 
     def stats(self, reqs: Sequence[Request] | None = None) -> dict:
-        reqs = list(reqs if reqs is not None else self.completed)
+        """p50 / p99 / mean latency and throughput over the requests that ran."""
+        reqs = [r for r in (reqs if reqs is not None else self.completed) if r.error is None]
         lat = np.array([r.finished - r.arrival for r in reqs]) * 1e3
         pts = sum(r.points() for r in reqs)
         span = max(r.finished for r in reqs) - min(r.arrival for r in reqs)

@@ -240,3 +240,22 @@ def test_public_api_under_graph_capture():
     # eager on the same coordinates after capture sorts afresh
     assert rel_l2(nb.nufft2d1(xg, yg, c, nm).cpu().numpy(), ref1) <= 1e-6
     del g
+
+
+def test_malformed_request_fails_alone():
+    """A request whose inputs do not match its description gets `error` set and no
+    result; the requests around it complete correctly and the budget is released."""
+    dev = cuda_device()
+    rng = np.random.default_rng(12)
+    reqs = _mix(rng, dev, n=8)
+    bad = Request(kind=1, dim=2, n_modes=(16, 16), M=100,
+                  coords=[torch.zeros(100, device=dev), torch.zeros(99, device=dev)],
+                  strengths=torch.zeros(100, dtype=torch.complex64, device=dev))
+    server = NufftServer(dev, slots=4, hbm_budget=2e9)
+    done = server.serve(reqs[:4] + [bad] + reqs[4:])
+    assert len(done) == 9 and server.in_use == 0
+    assert bad.error is not None and bad.result is None
+    for r in reqs:
+        assert r.error is None
+        assert rel_l2(r.result.cpu().numpy(), _alone(r).cpu().numpy()) <= 2e-6
+    assert server.stats(done)["requests"] == 8
