@@ -200,3 +200,23 @@ def test_profiling_span_is_inert_without_recorder():
     with profiling.span("nfx_spread_sorted", None) as s:
         assert s.rec is None
     assert profiling.LAUNCHES["nfx_sort_points"] >= 1
+
+
+def test_autotune_cache_round_trip(tmp_path, monkeypatch):
+    """The tuner's JSON cache (NUFFTAX_B200_TUNE_CACHE) loads what it saved and
+    ignores a malformed file."""
+    from nufftax_b200 import autotune
+
+    path = tmp_path / "tune.json"
+    monkeypatch.setenv("NUFFTAX_B200_TUNE_CACHE", str(path))
+    monkeypatch.setattr(autotune, "_cache", {})
+    monkeypatch.setattr(autotune, "_loaded", True)
+    autotune._cache["d2-uf2-ns8-f32-rho2-clu"] = ((32, 32), 2048)
+    autotune._save()
+    monkeypatch.setattr(autotune, "_cache", {})
+    monkeypatch.setattr(autotune, "_loaded", False)
+    assert autotune.cached() == {"d2-uf2-ns8-f32-rho2-clu": ((32, 32), 2048)}
+    path.write_text("{not json")
+    monkeypatch.setattr(autotune, "_cache", {})
+    monkeypatch.setattr(autotune, "_loaded", False)
+    assert autotune.cached() == {}
