@@ -95,6 +95,14 @@ def test_invalid_arguments_rejected_without_gpu():
     assert lib.nfx_fft(0, 2, _lib.int3((8, 8)), 1, ctypes.c_void_p(8), 0, None) == _lib.NFX_ERR_INVALID
     assert lib.nfx_deconv_pad(0, 1, _lib.int3((8,)), _lib.int3((9,)), ctypes.c_void_p(8), None, None,
                               ctypes.c_void_p(8), ctypes.c_void_p(8), 1, None) == _lib.NFX_ERR_INVALID
+    # one-call transforms without options; FFT entries with a bad sign / no size pointer
+    assert lib.nfx_nufft1(None, _lib.int3((8, 8)), None, None, None, 0, None, 1, 1, None, None, None, None, None,
+                          None, 0, None) == _lib.NFX_ERR_INVALID
+    assert lib.nfx_nufft2(None, _lib.int3((8, 8)), None, None, None, 0, None, 1, -1, None, None, None, None, None,
+                          None, 0, None) == _lib.NFX_ERR_INVALID
+    assert lib.nfx_fft_ws(0, 2, _lib.int3((8, 8)), 1, ctypes.c_void_p(8), 2, None, 0, None) == _lib.NFX_ERR_INVALID
+    assert lib.nfx_fft_ws(0, 2, _lib.int3((8, 8)), 1, None, 1, None, 0, None) == _lib.NFX_ERR_INVALID
+    assert lib.nfx_fft_work_bytes(0, 2, _lib.int3((8, 8)), 1, None) == _lib.NFX_ERR_INVALID
     with pytest.raises(ValueError):
         _lib.check(_lib.NFX_ERR_INVALID, "probe")
 
