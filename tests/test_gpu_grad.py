@@ -170,3 +170,35 @@ def test_type1_3d_grad_matches_spectral_reference_formula():
         ref = np.real(np.conj(c) * t2)
         assert rel_l2(Xt[d].grad.cpu().numpy(), ref) < 1e-7
     assert rel_l2(ct.grad.cpu().numpy(), O.nufft_type2(X, G, eps=eps, isign=-1)) < 1e-9
+
+
+def test_cg_least_squares_recovers_modes():
+    """The linear-solve use of the reference (nufftax tests/test_linear_solve.py):
+    conjugate gradients on the normal equations A^H A f = A^H c, with A the 2D
+    type 2 (modes -> points, isign -1) and A^H the type 1 (isign +1), recovers
+    the modes behind exact samples; the pair must be adjoint for CG to converge."""
+    dev = cuda_device()
+    rng = np.random.default_rng(17)
+    M, n = 4000, (24, 20)
+    x = torch.from_numpy(rng.uniform(-np.pi, np.pi, M)).to(dev)
+    y = torch.from_numpy(rng.uniform(-np.pi, np.pi, M)).to(dev)
+    f_true = torch.from_numpy(rng.standard_normal(n[::-1]) + 1j * rng.standard_normal(n[::-1])).to(dev)
+    eps = 1e-12
+    A = lambda f: nb.nufft2d2(x, y, f, eps=eps, isign=-1)  # noqa: E731
+    AH = lambda c: nb.nufft2d1(x, y, c, n, eps=eps, isign=1)  # noqa: E731
+    b = AH(A(f_true))
+    f = torch.zeros_like(f_true)
+    r = b.clone()
+    p = r.clone()
+    rr = torch.vdot(r.flatten(), r.flatten()).real
+    for _ in range(60):
+        Ap = AH(A(p))
+        alpha = rr / torch.vdot(p.flatten(), Ap.flatten()).real
+        f = f + alpha * p
+        r = r - alpha * Ap
+        rr_new = torch.vdot(r.flatten(), r.flatten()).real
+        if float(rr_new.sqrt() / b.norm()) < 1e-11:
+            break
+        p = r + (rr_new / rr) * p
+        rr = rr_new
+    assert rel_l2(f.cpu().numpy(), f_true.cpu().numpy()) < 1e-8

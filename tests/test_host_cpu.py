@@ -228,3 +228,21 @@ def test_autotune_cache_round_trip(tmp_path, monkeypatch):
     monkeypatch.setattr(autotune, "_cache", {})
     monkeypatch.setattr(autotune, "_loaded", False)
     assert autotune.cached() == {}
+
+
+@pytest.mark.parametrize("eps", [1e-3, 1e-6, 1e-12])
+def test_deconv_factors_positive_symmetric_growing(eps):
+    """Properties the reference's kernel tests check on phi-hat
+    (nufftax tests/test_kernel.py): the Fourier series is positive and decays
+    away from k = 0, so the per-mode factors 1 / phi-hat are positive, symmetric
+    in k and grow with |k|."""
+    kp = nb.compute_kernel_params(eps)
+    n = 64
+    nf = nb.compute_grid_size(n, 2.0, kp.nspread)
+    fac = np.abs(deconv_factors(nf, n, kp))  # CMCL order k = -n/2 .. n/2 - 1, sign (-1)^k
+    assert np.all(fac > 0)
+    k = np.arange(-n // 2, n // 2)
+    mag = {int(kk): f for kk, f in zip(k, fac)}
+    for kk in range(1, n // 2):
+        assert np.isclose(mag[kk], mag[-kk], rtol=1e-12)
+        assert mag[kk] >= mag[kk - 1]
