@@ -8,7 +8,6 @@ memory and the current stream; all arithmetic happens in the CUDA library.
 from __future__ import annotations
 
 import collections
-import ctypes
 import threading
 from ctypes import byref, c_int, c_size_t, c_void_p
 from typing import Sequence

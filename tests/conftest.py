@@ -4,7 +4,6 @@ Markers: `gpu` tests need a CUDA device and the built libnfx_b200.so; the rest
 run on the CPU.  The oracle under oracle/ is the checker for every parity test.
 """
 
-import os
 import sys
 from pathlib import Path
 
