@@ -286,6 +286,8 @@ def factors(nf: int, n_modes: int, kp: KernelParams, precision: int, device: tor
         arr = deconv_factors(nf, n_modes, kp)
         t = torch.from_numpy(arr.astype(np.float32 if precision == _lib.NFX_F32 else np.float64)).to(device)
         with _fac_lock:
+            # never evicted while the process runs: an enqueued deconvolution may
+            # still read a factor tensor after its call returns (a few KB a shape)
             _fac_cache[key] = t
     return t
 

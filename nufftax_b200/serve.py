@@ -136,7 +136,10 @@ class NufftServer:
         self.points_cache: "collections.OrderedDict[object, tuple[PointSort, torch.cuda.Event]]" = \
             collections.OrderedDict()
         self.keep_points = keep_points
-        self.shapes: dict = {}
+        self.shapes: "collections.OrderedDict[tuple, _Shape]" = collections.OrderedDict()
+        # per-shape library options kept (least recently used out); the device
+        # factors they point at stay alive in the library-wide factor cache
+        self.keep_shapes = 4096
         self.lock = threading.Lock()
 
     # -- resident state -----------------------------------------------------------
@@ -181,7 +184,9 @@ class NufftServer:
     def _shape(self, req: Request, precision: int) -> _Shape:
         key = (req.kind, tuple(req.n_modes), req.eps, req.isign, precision)
         sh = self.shapes.get(key)
-        if sh is None:
+        if sh is not None:
+            self.shapes.move_to_end(key)
+        else:
             kp = compute_kernel_params(req.eps)
             nf = tuple(compute_grid_size(n, 2.0, kp.nspread) for n in req.n_modes)
             facs = _facs(nf, req.n_modes, kp, precision, self.device)
@@ -192,6 +197,8 @@ class NufftServer:
             sh = _Shape(make_opts(precision, nf, kp, prenorm=True), nf, _lib.int3(req.n_modes), facs,
                         [ptr(f) for f in facs], sign)
             self.shapes[key] = sh
+            while len(self.shapes) > self.keep_shapes:
+                self.shapes.popitem(last=False)
         return sh
 
     def _run_one_call(self, req: Request, slot: _Slot):

@@ -121,3 +121,28 @@ def test_failure_isolated_and_excluded_from_stats(server_factory):
     assert srv.in_use == 0 and len(srv.completed) == 2
     st = srv.stats()
     assert st["requests"] == 1 and st["points"] == good.points()
+
+
+def test_shape_state_is_bounded(monkeypatch):
+    """Per-shape options of the one-call path are kept least recently used out
+    (host structs only; runs without a GPU on the CPU device)."""
+    monkeypatch.setattr(serve, "_Slot", _FakeSlot)
+    srv = serve.NufftServer("cpu", slots=1)
+    srv.keep_shapes = 3
+    reqs = [serve.Request(kind=1, dim=2, n_modes=(16 + 2 * i, 16), M=10) for i in range(5)]
+    for r in reqs[:3]:
+        srv._shape(r, 0)
+    srv._shape(reqs[0], 0)  # touch: most recently used
+    srv._shape(reqs[3], 0)
+    srv._shape(reqs[4], 0)
+    kept = {k[1] for k in srv.shapes}
+    assert len(srv.shapes) == 3 and (16, 16) in kept and (18, 16) not in kept
+    sh = srv._shape(reqs[4], 0)
+    assert sh.nf == tuple(nb_grid(n) for n in (24, 16)) and sh.sign == 1
+
+
+def nb_grid(n):
+    from nufftax_b200.grid import compute_grid_size
+    from nufftax_b200.kernel import compute_kernel_params
+
+    return compute_grid_size(n, 2.0, compute_kernel_params(1e-6).nspread)
