@@ -206,3 +206,21 @@ def test_type1_type2_adjoint():
     a = np.vdot(f, O.nufft_type1([x, y], c, (16, 12), isign=1, eps=1e-9))
     b = np.vdot(O.nufft_type2([x, y], f, isign=-1, eps=1e-9), c)
     assert abs(a - b) / abs(a) < 1e-8
+
+
+@pytest.mark.parametrize("eps,bound", [(1e-3, 2e-2), (1e-6, 1e-4), (1e-9, 1e-5)])
+def test_upsampfac_125_works_but_coarse(eps, bound):
+    """nufftax tests/test_upsampfac.py: upsampfac 1.25 runs with the same kernel
+    width and is coarser than 2.0 but still converges with eps (types 1 and 2
+    against the direct sums)."""
+    rng = np.random.default_rng(3)
+    x = rng.uniform(-np.pi, np.pi, 3000)
+    c = rng.standard_normal(3000) + 1j * rng.standard_normal(3000)
+    fm = rng.standard_normal(256) + 1j * rng.standard_normal(256)
+    d1 = O.direct_type1([x], c, (256,))
+    d2 = O.direct_type2([x], fm, O.flat_mode_list((256,)))
+    e1 = {uf: rel_l2(O.nufft_type1([x], c, (256,), eps=eps, upsampfac=uf), d1) for uf in (2.0, 1.25)}
+    e2 = {uf: rel_l2(O.nufft_type2([x], fm, eps=eps, upsampfac=uf), d2) for uf in (2.0, 1.25)}
+    assert O.compute_kernel_params(eps, 1.25).nspread == O.compute_kernel_params(eps, 2.0).nspread
+    for e in (e1, e2):
+        assert e[2.0] < 2 * eps and e[1.25] < bound and e[1.25] > e[2.0]
