@@ -246,3 +246,43 @@ def test_deconv_factors_positive_symmetric_growing(eps):
     for kk in range(1, n // 2):
         assert np.isclose(mag[kk], mag[-kk], rtol=1e-12)
         assert mag[kk] >= mag[kk - 1]
+
+
+def test_host_only_sizes_and_limits():
+    """Entry points that size buffers or set limits answer without a GPU: the
+    no-alloc scratch (64 MiB), type-3 parameter / scratch sizes, the batched
+    deconvolution table (growing with the problem count), the FFT plan-cache limit
+    (at least one plan) and the SM count (a default without a device)."""
+    lib = _lib.load()
+    assert lib.nfx_noalloc_scratch_bytes() == 64 << 20
+    assert lib.nfx_t3_params_bytes() > 0
+    assert lib.nfx_t3_scratch_bytes(0, 1000, 2000) > 0 and lib.nfx_t3_scratch_bytes(1, 1000, 2000) > 0
+    sizes = [lib.nfx_batch_deconv_table_bytes(0, n) for n in (1, 2, 8, 64)]
+    assert sizes[0] > 0 and all(a <= b for a, b in zip(sizes, sizes[1:])) and sizes[-1] > sizes[0]
+    assert lib.nfx_fft_cache_limit(0) == _lib.NFX_ERR_INVALID
+    assert lib.nfx_fft_cache_limit(1024) == 0
+    assert lib.nfx_num_sms() >= 1
+
+
+def test_batch_info_host_side():
+    """nfx_batch_info_get sizes the device table, the shared memory and the
+    work-queue bound of a batched launch from the problem descriptors alone."""
+    lib = _lib.load()
+    kp = nb.compute_kernel_params(1e-6)
+    common = _lib.NfxOpts()
+    common.precision, common.dim, common.nspread, common.prenorm = 0, 2, int(kp.nspread), 1
+    common.beta, common.kc = float(kp.beta), float(kp.c)
+
+    def info_for(specs):
+        probs = (_lib.NfxBatchProblem * len(specs))()
+        for i, (M, nf) in enumerate(specs):
+            probs[i].M = M
+            probs[i].nf = _lib.int3(nf)
+        info = _lib.NfxBatchInfo()
+        assert lib.nfx_batch_info_get(byref(common), 1, probs, len(specs), byref(info)) == 0, lib.nfx_last_error()
+        return info
+
+    a = info_for([(1000, (64, 64))])
+    b = info_for([(1000, (64, 64)), (50_000, (256, 192))])
+    assert a.table_bytes > 0 and a.smem_bytes > 0 and a.max_subs >= 1
+    assert b.table_bytes > a.table_bytes and b.max_subs > a.max_subs
