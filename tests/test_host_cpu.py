@@ -208,6 +208,12 @@ def test_profiling_span_is_inert_without_recorder():
     with profiling.span("nfx_spread_sorted", None) as s:
         assert s.rec is None
     assert profiling.LAUNCHES["nfx_sort_points"] >= 1
+    # a recorder limited to some calls leaves the others inert, and a lazily
+    # given launch count is never evaluated for them
+    with profiling.record(only=["nfx_spread_sorted"]) as rec:
+        with profiling.span("nfx_interp_sorted", None, lambda: 1 / 0) as s:
+            assert s.rec is None
+    assert rec.events == []
 
 
 def test_autotune_cache_round_trip(tmp_path, monkeypatch):
