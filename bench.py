@@ -3,7 +3,7 @@
 
 Workload (one step = one type-1 and one type-2 transform of each point set):
   (a) radial: 512 spokes x 1024 samples (M = 524,288), golden-angle spoke angles
-      theta_s = s * pi (sqrt(5) - 1) / 2 mod pi, 1024 evenly spaced radii in [-pi, pi);
+      theta_s = s * pi (sqrt(5) - 1) / 2 mod pi, every radius uniform in [-pi, pi);
   (b) clustered: M = 4,000,000 points, x, y ~ N(0, 0.3^2) wrapped to [-pi, pi);
   strengths c and modes f iid complex N(0, 1); seeded synthetic data.
 Metric: NU points per second, counting M once per transform (2 * (Ma + Mb) per step).
@@ -21,8 +21,10 @@ previous step computes), and the timed region spans all K steps.
 Inside the timed loop only the dominant kernel's library calls are bracketed
 with CUDA events (its live launch time for `roofline`); the per-call breakdown
 and the launch count come from one recorded warm-up step.
-`--impl reference` times the CPU restatement of nufftax's
-pure-JAX path (oracle/) on all host cores on a bounded sample.
+`cpu_baseline` times the CPU restatement of nufftax's pure-JAX path (oracle/)
+on one core over one full step, and `accuracy` checks that step's GPU outputs
+against it and against the FP64 direct sum on a subsample.  `--impl reference`
+times the same restatement on all host cores on a bounded sample of each step.
 Multi-GPU runs are independent replicas (weak scaling), timed as the max over ranks.
 """
 
@@ -49,12 +51,14 @@ METRIC = "type-1/2 NU points/s at eps 1e-6 (2D, 512^2 modes, complex64)"
 # ---------------------------------------------------------------------------
 # Workload
 # ---------------------------------------------------------------------------
-def radial_points(n_spokes=512, n_samples=1024):
+def radial_points(rng, n_spokes=512, n_samples=1024):
+    """Radial trajectory: golden-angle spoke angles theta_s = s pi (sqrt(5) - 1) / 2
+    mod pi, every sample's signed radius drawn uniform in [-pi, pi)."""
     ga = np.pi * (np.sqrt(5.0) - 1.0) / 2.0
     theta = np.mod(np.arange(n_spokes) * ga, np.pi)
-    r = -np.pi + 2.0 * np.pi * np.arange(n_samples) / n_samples
-    x = (r[None, :] * np.cos(theta)[:, None]).ravel()
-    y = (r[None, :] * np.sin(theta)[:, None]).ravel()
+    r = rng.uniform(-np.pi, np.pi, (n_spokes, n_samples))
+    x = (r * np.cos(theta)[:, None]).ravel()
+    y = (r * np.sin(theta)[:, None]).ravel()
     return x.astype(np.float32), y.astype(np.float32)
 
 
@@ -66,7 +70,7 @@ def clustered_points(M, rng, sigma=0.3):
 
 def workload(seed=1234, scale=1.0):
     rng = np.random.default_rng(seed)
-    xa, ya = radial_points(max(1, int(512 * scale)), 1024)
+    xa, ya = radial_points(rng, max(1, int(512 * scale)), 1024)
     Mb = max(1, int(4_000_000 * scale))
     xb, yb = clustered_points(Mb, rng)
     sets = []
@@ -77,6 +81,19 @@ def workload(seed=1234, scale=1.0):
             (N_MODES[1], N_MODES[0]))).astype(np.complex64)
         sets.append({"name": name, "x": x, "y": y, "c": c, "f": f, "M": M})
     return sets
+
+
+DATA = ("synthetic (seeded): radial 512 golden-angle spokes x 1024 samples, radius uniform in [-pi, pi); "
+        "4M points clustered N(0, 0.3^2) wrapped to [-pi, pi); c, f iid complex N(0, 1)")
+
+
+def bench_config(world: int, sets) -> dict:
+    """The workload the headline line (and the reference arm) is quoted on."""
+    return {"workload": "2D type-1 + type-2, 512x512 modes, nf 1024x1024, eps 1e-6, ns 8: radial M=524288 and "
+                        "clustered M=4000000 per step",
+            "global_batch": points_per_step(sets) * world, "parallelism": f"replicas x{world}",
+            "l2": "flushed between steps (256 MB write)",
+            "sort": "every step: one sort per point set, shared by its type 1 and type 2"}
 
 
 def points_per_step(sets):
@@ -405,10 +422,8 @@ def run_gpu(args):
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "c64",
-        "data": "synthetic (seeded): radial 512x1024 golden-angle + 4M clustered N(0,0.3^2)",
-        "config": {"workload": "2D type-1 + type-2, 512x512 modes, nf 1024x1024, eps 1e-6, ns 8: radial "
-                               "M=524288 and clustered M=4000000 per step", "global_batch": points_per_step(sets) * world,
-                   "parallelism": f"replicas x{world}", "l2": "flushed between steps (256 MB write)"},
+        "data": DATA,
+        "config": bench_config(world, sets),
         "e2e": {"value": e2e_value, "unit": "NU points/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "steps_pipelined": True,
                 "pcie_gbs": round((h2d + d2h) * args.steps / (e_ms / 1e3) / 1e9, 1)},
@@ -422,7 +437,16 @@ def run_gpu(args):
         "breakdown": breakdown,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline_sample()
+        # GPU results of one step at full size (the compute path of the timed
+        # steps), checked in the CPU leg below against the oracle and the FP64
+        # direct sum
+        gpu_out = []
+        for s in devsets:
+            nb.sort_cache.clear()
+            f1 = nb.nufft2d1(s["x"], s["y"], s["c"], N_MODES, eps=EPS)
+            c2 = nb.nufft2d2(s["x"], s["y"], s["f"], eps=EPS)
+            gpu_out.append((f1.cpu().numpy(), c2.cpu().numpy()))
+        line["cpu_baseline"], line["accuracy"] = cpu_leg(sets, gpu_out)
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
@@ -440,22 +464,42 @@ def _oracle():
     return O
 
 
-def cpu_baseline_sample():
-    """Single-core oracle timing on a bounded sample (about 10-30 s of CPU work)."""
+def cpu_leg(sets, gpu_out):
+    """The CPU leg of the headline run (rank 0, one GPU): the oracle (NumPy
+    restatement of nufftax's pure-JAX path) runs one full step of the workload
+    on one core, which is timed as `cpu_baseline`; its outputs, and the FP64
+    direct sum on a subsample, then check the GPU's outputs of the same step
+    (`accuracy`).  The oracle is the checker here, never the thing measured."""
     O = _oracle()
-    sets = workload(seed=99, scale=1.0)
-    sample = []
-    for s in sets:
-        m = 65536 if s["name"] == "radial" else 131072
-        sample.append({**s, "x": s["x"][:m], "y": s["y"][:m], "c": s["c"][:m], "M": m})
     t0 = time.perf_counter()
-    for s in sample:
-        O.nufft_type1([s["x"], s["y"]], s["c"], N_MODES, eps=EPS)
-        O.nufft_type2([s["x"], s["y"]], s["f"], eps=EPS)
+    ref = []
+    for s in sets:
+        ref.append((O.nufft_type1([s["x"], s["y"]], s["c"], N_MODES, eps=EPS),
+                    O.nufft_type2([s["x"], s["y"]], s["f"], eps=EPS)))
     dt = time.perf_counter() - t0
-    return {"value": points_per_step(sample) / dt, "unit": "NU points/s", "cores": 1, "kind": "port",
-            "sample": f"radial first {sample[0]['M']} points + clustered first {sample[1]['M']} points, "
-                      f"one type 1 + one type 2 each, {dt:.1f} s"}
+    base = {"value": points_per_step(sets) / dt, "unit": "NU points/s", "cores": 1, "kind": "port",
+            "sample": f"one full step (radial M={sets[0]['M']}, clustered M={sets[1]['M']}: one type 1 + one "
+                      f"type 2 each), {dt:.1f} s"}
+    rng = np.random.default_rng(2024)
+    acc = {"eps": EPS, "dtype": "c64",
+           "bound_vs_oracle": 2 * EPS,
+           "bound_vs_direct": 10 * EPS + 2 * max(N_MODES) * 2.0 ** -24,
+           "bound_note": "direct-sum bound = 10 eps + 2 N 2^-24: coordinates are folded in float32, as "
+                         "nufftax does for complex64 inputs",
+           "direct_sample": "type 1: 256 modes (16 x 16 product set, all points); type 2: 256 random "
+                            "targets (all modes)"}
+    for s, (f1, c2), (r1, r2) in zip(sets, gpu_out, ref):
+        ax = [np.sort(rng.choice(np.arange(-(n // 2), (n - 1) // 2 + 1), 16, replace=False)) for n in N_MODES]
+        d1 = O.direct_type1_product([s["x"], s["y"]], s["c"], ax, isign=1)
+        sub1 = f1[np.ix_(ax[1] + N_MODES[1] // 2, ax[0] + N_MODES[0] // 2)]
+        rows = np.sort(rng.choice(s["M"], 256, replace=False))
+        d2 = O.direct_type2_points([s["x"][rows], s["y"][rows]], s["f"], isign=-1)
+        acc[s["name"]] = {"type1_vs_oracle": O.rel_l2(f1, r1), "type2_vs_oracle": O.rel_l2(c2, r2),
+                          "type1_vs_direct": O.rel_l2(sub1, d1), "type2_vs_direct": O.rel_l2(c2[rows], d2),
+                          "oracle_type1_vs_direct": O.rel_l2(r1[np.ix_(ax[1] + N_MODES[1] // 2,
+                                                                      ax[0] + N_MODES[0] // 2)], d1),
+                          "oracle_type2_vs_direct": O.rel_l2(r2[rows], d2)}
+    return base, acc
 
 
 def _spread_chunk(args):
@@ -513,12 +557,13 @@ def run_reference(args):
     line = {
         "metric": METRIC, "value": value, "unit": "NU points/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "c64", "data": "synthetic (seeded), bounded sample of the GPU workload",
-        "config": {"workload": "2D type-1 + type-2, 512x512 modes, nf 1024x1024, eps 1e-6, ns 8: radial "
-                               f"M={sample[0]['M']} and clustered M={sample[1]['M']} per step (sample)"},
+        "vs_baseline": None, "dtype": "c64", "data": DATA,
+        "config": bench_config(world, sets),
         "impl": "reference",
         "cpu_baseline": {"value": value, "unit": "NU points/s", "cores": cores, "kind": "port",
-                         "sample": f"radial first {sample[0]['M']} + clustered first {sample[1]['M']} points"},
+                         "sample": f"each step: radial first {sample[0]['M']} + clustered first {sample[1]['M']} "
+                                   "points of the workload, one type 1 + one type 2 each (points/s counts the "
+                                   "sample's points)"},
         "e2e": {"value": value, "unit": "NU points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)

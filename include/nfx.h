@@ -115,7 +115,8 @@ int nfx_interp_sorted(const nfx_opts* opts, const void* x, const void* y, const 
  * of nfx_noalloc_scratch_bytes() (64 MiB) that the library holds on every GPU
  * that loads it.  Requests needing more scratch fail with NFX_ERR_UNSUPPORTED.
  * The first call on a device looks up the array's address (make it before any
- * stream capture); calls that overlap on the GPU race on the shared array. */
+ * stream capture) and keeps it for the process: it does not survive a
+ * cudaDeviceReset.  Calls that overlap on the GPU race on the shared array. */
 size_t nfx_noalloc_scratch_bytes(void);
 int nfx_spread_noalloc(const nfx_opts* opts, const void* x, const void* y, const void* z, int64_t M, const void* c,
                        int n_trans, void* fw, void* stream);
@@ -242,7 +243,9 @@ int nfx_batch_deconv(int precision, int pad, const void* dev_table, int nprob, i
  * nfx_t3_prepare: from source coordinates (dim arrays of M) and target
  *   frequencies (dim arrays of K) computes, on the device and without a host
  *   round trip, the centres C, D, half-widths S and scales gamma, h per axis
- *   (nufft3.py:268-281) into `params` (a device buffer of nfx_t3_params_bytes()),
+ *   (nufft3.py:268-281) into `params` (a device buffer of nfx_t3_params_bytes();
+ *   computed in the working precision in the reference's order, so that
+ *   complex64 inputs get the reference's float32 rescaled coordinates),
  *   then writes the rescaled folded sources xn_d = mod((x_d - C_d)/gamma_d + pi,
  *   2 pi) - pi, the pre-phased strengths c' = c e^{i isign sum_d D_d x_d}
  *   (n_trans x M), the rescaled folded targets sn_d = mod(h_d gamma_d (s_d - D_d)

@@ -100,8 +100,9 @@ def _make_opts(precision: int, nf: Sequence[int], kp: KernelParams, prenorm: boo
 def sort_launches(opts, M: int) -> int:
     """Kernels one nfx_sort_points call launches: keys (with the first digit's
     counts), per radix pass a column scan and a scatter (plus a count for the
-    passes after the first), bin bounds and subproblems.  The composite key is
-    bin << cell_bits | cell; digits have at most 11 bits."""
+    passes after the first), the sorted folded coordinates, bin bounds and
+    subproblems.  The composite key is bin << cell_bits | cell; digits have at
+    most 11 bits."""
     if M == 0:
         return 2
     nbins = ncell = 1
@@ -111,7 +112,7 @@ def sort_launches(opts, M: int) -> int:
         ncell *= t
     bits = max(1, (ncell - 1).bit_length() + (nbins - 1).bit_length())
     npass = 1 if bits <= 11 else (2 if bits <= 22 else 3)
-    return 3 * npass + 2
+    return 3 * npass + 3
 
 
 class PointSort:
@@ -139,6 +140,8 @@ class PointSort:
         _lib.check(lib.nfx_sort_workspace_bytes(byref(self.opts), self.M, byref(nbytes)), "nfx_sort_workspace_bytes")
         self.ws_bytes = int(nbytes.value)
         self.ws = torch.empty(max(self.ws_bytes, 1), dtype=torch.uint8, device=self.device)
+        self.stream = stream_of(self.device)  # the stream the sort ran on (and the workspace belongs to)
+        self._src = None
         launches = lambda: sort_launches(self.opts, self.M)  # noqa: E731 (evaluated only when recording)
         with torch.cuda.device(self.device), span("nfx_sort_points", self.device, launches):
             _lib.check(lib.nfx_sort_points(byref(self.opts), *self._xyz(), self.M, ptr(self.ws), self.ws_bytes,
@@ -237,7 +240,17 @@ class PointSort:
 class _SortCache:
     """LRU of PointSorts.  Entries hold strong references to their coordinate
     tensors, so a key (tensor identity, data pointer, version counter) can only
-    match the same, unmodified tensors."""
+    match the same tensors unmodified through torch.
+
+    A write that bypasses torch's version counter (a raw kernel, a ctypes or
+    DLPack writer from another framework into the same memory) cannot be seen
+    here: after one, call `invalidate(tensor)` (or `clear()`), or the next
+    transform on those coordinates reuses the old sort and drops every point
+    that left its tile.
+
+    A cached sort may be used from another stream than the one that made it;
+    its workspace is then recorded on that stream, so an eviction cannot hand
+    the memory to new work while the other stream's kernels still read it."""
 
     def __init__(self, size: int = 4):
         self.size = size
@@ -255,9 +268,15 @@ class _SortCache:
         if self.enabled:
             with self._lock:
                 hit = self._d.get(key)
-                if hit is not None and all(a is b for a, b in zip(hit._src, coords)):
+                if hit is not None and not all(a is b for a, b in zip(hit._src, coords)):
+                    hit = None
+                if hit is not None:
                     self._d.move_to_end(key)
-                    return hit
+            if hit is not None:
+                s = stream_of(hit.device)
+                if s != hit.stream:
+                    hit.ws.record_stream(torch.cuda.ExternalStream(s, device=hit.device))
+                return hit
         ps = PointSort(coords, nf, kp, prenorm)
         ps._src = list(coords)
         if self.enabled:
@@ -266,6 +285,16 @@ class _SortCache:
                 while len(self._d) > self.size:
                     self._d.popitem(last=False)
         return ps
+
+    def invalidate(self, *tensors: torch.Tensor) -> int:
+        """Drop every cached sort made from any of `tensors` (coordinates whose
+        memory was written outside torch); returns the number dropped."""
+        ptrs = {t.data_ptr() for t in tensors}
+        with self._lock:
+            dead = [k for k, ps in self._d.items() if any(c.data_ptr() in ptrs for c in ps._src)]
+            for k in dead:
+                del self._d[k]
+        return len(dead)
 
     def clear(self):
         with self._lock:
@@ -293,9 +322,16 @@ def factors(nf: int, n_modes: int, kp: KernelParams, precision: int, device: tor
 
 
 def clear_caches() -> None:
-    """Drop cached point sorts, deconvolution factors and cuFFT plans."""
+    """Drop cached point sorts, deconvolution factors and cuFFT plans.
+
+    Enqueued deconvolutions (a server's requests in flight, work on any stream)
+    may still read the factor tensors, so every device that holds one is
+    synchronised before they are dropped."""
     sort_cache.clear()
     with _fac_lock:
+        devs = {t.device for t in _fac_cache.values()}
+        for d in devs:
+            torch.cuda.synchronize(d)
         _fac_cache.clear()
     _lib.load().nfx_fft_cache_clear()
 

@@ -338,6 +338,7 @@ static void make_layout(const nfx_opts& o, const Geom& g, int64_t M, SortLayout&
   L.off_sub_bin = take((size_t)L.max_subs * 4);
   L.off_sub_start = take((size_t)L.max_subs * 4);
   L.off_nsub = take(4);
+  for (int d = 0; d < 3; ++d) L.off_coord[d] = d < o.dim ? take((size_t)M * real_bytes(o.precision)) : 0;
   L.total = off;
 }
 
@@ -362,12 +363,14 @@ static SortPtrs carve(const SortLayout& L, void* ws) {
   P.sub_bin = (int*)(b + L.off_sub_bin);
   P.sub_start = (int*)(b + L.off_sub_start);
   P.nsub = (int*)(b + L.off_nsub);
+  for (int d = 0; d < 3; ++d) P.coord[d] = L.off_coord[d] != 0 ? (void*)(b + L.off_coord[d]) : nullptr;
   return P;
 }
 
 static SortView view(const SortLayout& L, const void* ws) {
   SortPtrs P = carve(L, const_cast<void*>(ws));
   SortView v;
+  for (int d = 0; d < 3; ++d) v.coord[d] = P.coord[d];
   v.perm = P.perm;
   v.bin_start = P.bin_start;
   v.sub_bin = P.sub_bin;
@@ -505,7 +508,7 @@ static void attach_poly(PointArgs<T>& a, int ns, double beta, double kc) {
 template <typename T>
 static cudaError_t spread_dim(const Prepared& P, const void* x, const void* y, const void* z, int64_t M, const void* c,
                               int n_trans, void* fw, const void* ws, cudaStream_t st) {
-  PointArgs<T> a = make_args<T>(P.g, P.o.beta, P.o.kc, x, y, z, M, n_trans, view(P.L, ws));
+  PointArgs<T> a = make_args<T>(P.g, P.o.beta, P.o.kc, M, n_trans, view(P.L, ws));
   attach_poly(a, P.o.nspread, P.o.beta, P.o.kc);
   switch (P.o.dim) {
     case 1:
@@ -520,7 +523,7 @@ static cudaError_t spread_dim(const Prepared& P, const void* x, const void* y, c
 template <typename T>
 static cudaError_t interp_dim(const Prepared& P, const void* x, const void* y, const void* z, int64_t M,
                               const void* fw, int n_trans, void* out, const void* ws, cudaStream_t st) {
-  PointArgs<T> a = make_args<T>(P.g, P.o.beta, P.o.kc, x, y, z, M, n_trans, view(P.L, ws));
+  PointArgs<T> a = make_args<T>(P.g, P.o.beta, P.o.kc, M, n_trans, view(P.L, ws));
   attach_poly(a, P.o.nspread, P.o.beta, P.o.kc);
   switch (P.o.dim) {
     case 1:
@@ -536,7 +539,7 @@ template <typename T>
 static cudaError_t grad_dim(const Prepared& P, const void* x, const void* y, const void* z, int64_t M, const void* G,
                             const void* V, int n_trans, void* oi, void* dx, void* dy, void* dz, const void* ws,
                             cudaStream_t st) {
-  PointArgs<T> a = make_args<T>(P.g, P.o.beta, P.o.kc, x, y, z, M, n_trans, view(P.L, ws));
+  PointArgs<T> a = make_args<T>(P.g, P.o.beta, P.o.kc, M, n_trans, view(P.L, ws));
   switch (P.o.dim) {
     case 1:
       return dispatch_grad<T, 1>(P.o.nspread, a, G, V, oi, dx, nullptr, nullptr, st);
@@ -877,15 +880,13 @@ int nfx_batch_upload(const nfx_opts* common, int spread, const nfx_batch_problem
     }
     if (common->precision == NFX_F32) {
       BatchItem<float>* it = (BatchItem<float>*)host.data() + p;
-      it->a = make_args<float>(P.g, P.o.beta, P.o.kc, probs[p].x, probs[p].y, probs[p].z, probs[p].M, 1,
-                               view(P.L, probs[p].workspace));
+      it->a = make_args<float>(P.g, P.o.beta, P.o.kc, probs[p].M, 1, view(P.L, probs[p].workspace));
       attach_poly(it->a, P.o.nspread, P.o.beta, P.o.kc);
       it->src = probs[p].src;
       it->dst = probs[p].dst;
     } else {
       BatchItem<double>* it = (BatchItem<double>*)host.data() + p;
-      it->a = make_args<double>(P.g, P.o.beta, P.o.kc, probs[p].x, probs[p].y, probs[p].z, probs[p].M, 1,
-                                view(P.L, probs[p].workspace));
+      it->a = make_args<double>(P.g, P.o.beta, P.o.kc, probs[p].M, 1, view(P.L, probs[p].workspace));
       it->src = probs[p].src;
       it->dst = probs[p].dst;
     }

@@ -26,6 +26,7 @@ struct SortLayout {
   int64_t max_subs; // upper bound on the number of subproblems
   size_t off_keys, off_keys_tmp, off_vals_tmp, off_keys_sorted, off_perm, off_counts, off_totals, off_bin_start,
       off_sub_bin, off_sub_start, off_nsub;
+  size_t off_coord[3];  // folded coordinates in sorted order, one array per axis (0 = unused axis)
   size_t total;
 };
 
@@ -41,10 +42,15 @@ struct SortPtrs {
   int* sub_bin;
   int* sub_start;
   int* nsub;
+  void* coord[3];  // sorted folded coordinates (working precision), nullptr for unused axes
 };
 
 // Pointers a spread / interp / gradient launch needs from a finished sort.
+// coord[d][k] is the folded, rescaled coordinate fold(x_d[perm[k]]) in [0, nf_d]
+// of the k-th sorted point (working precision), written by the sort so that the
+// passes read coordinates in sorted order instead of gathering them.
 struct SortView {
+  const void* coord[3];
   const int* perm;
   const int* bin_start;
   const int* sub_bin;

@@ -14,7 +14,8 @@
 // * Set-up: the first call on a device, with that device current, looks up the
 //   array's device address with cudaGetSymbolAddress (host code cannot use the
 //   array's name as a device pointer); make that first call before any stream
-//   capture.
+//   capture.  The address is kept for the life of the process: it does not
+//   survive a cudaDeviceReset, after which this entry point must not be called.
 // * Sharing: every call on a device uses the same array and leaves its
 //   contents behind.  Nothing in it needs to start at zero: the sort writes every
 //   entry it later reads.  Calls that overlap on the GPU (different streams,
@@ -58,9 +59,14 @@ int nfx_spread_noalloc(const nfx_opts* opts, const void* x, const void* y, const
   }
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess || dev < 0 || dev >= 64) {
+  if (e != cudaSuccess) {
     set_error(std::string("nfx_spread_noalloc: cudaGetDevice: ") + cudaGetErrorString(e));
     return NFX_ERR_CUDA;
+  }
+  if (dev < 0 || dev >= 64) {
+    set_error("nfx_spread_noalloc: device index " + std::to_string(dev) +
+              " is beyond the 64 devices whose scratch address the library keeps");
+    return NFX_ERR_UNSUPPORTED;
   }
   void* scratch = nullptr;
   {

@@ -21,12 +21,14 @@
 //     per digit bit inside each 32-element round, per-warp running counts
 //     across rounds), stages the chunk in shared memory in digit order and
 //     writes it out as contiguous runs per digit;
-// (3) k_bin_bounds reads the bin starts off the sorted keys, and
-//     k_subproblems splits bins larger than max_subproblem points into
-//     subproblems so clustered inputs spread evenly over the SMs.  Points of
-//     a subproblem are ordered by cell, which lets spreading merge runs of
-//     points that share a cell and gives interpolation near-identical
-//     addresses per warp.
+// (3) k_sorted_coords writes every point's folded coordinates in sorted order
+//     (the spread / interp / gradient passes then stream them instead of
+//     gathering through the permutation), k_bin_bounds reads the bin starts
+//     off the sorted keys, and k_subproblems splits bins larger than
+//     max_subproblem points into subproblems so clustered inputs spread evenly
+//     over the SMs.  Points of a subproblem are ordered by cell, which lets
+//     spreading merge runs of points that share a cell and gives interpolation
+//     near-identical addresses per warp.
 // No CTA waits for another: every dependency is a kernel boundary.
 #include <algorithm>
 
@@ -444,6 +446,62 @@ __global__ void k_subproblems(const int* __restrict__ bin_start, int nbins, int 
   }
 }
 
+__device__ __forceinline__ void store_quad(float* o, const float (&r)[4]) {
+  *reinterpret_cast<float4*>(o) = make_float4(r[0], r[1], r[2], r[3]);
+}
+__device__ __forceinline__ void store_quad(double* o, const double (&r)[4]) {
+  reinterpret_cast<double2*>(o)[0] = make_double2(r[0], r[1]);
+  reinterpret_cast<double2*>(o)[1] = make_double2(r[2], r[3]);
+}
+
+// ---- (3a) folded coordinates in sorted order ----------------------------------
+// coord_d[k] = fold(x_d[perm[k]]) for every axis: the same float operations as
+// the keys (so the spread / interp passes see exactly the coordinates the sort
+// binned), written once in sorted order.  Each thread takes 4 consecutive
+// positions: one vector load of the permutation, all gathers in flight together,
+// one vector store per axis.
+template <typename T, int DIM>
+__global__ void __launch_bounds__(256) k_sorted_coords(const T* __restrict__ x, const T* __restrict__ y,
+                                                       const T* __restrict__ z, const int* __restrict__ perm, int M,
+                                                       Geom g, T* __restrict__ o0, T* __restrict__ o1,
+                                                       T* __restrict__ o2) {
+  const T* cs[3] = {x, y, z};
+  T* os[3] = {o0, o1, o2};
+  const int nq = (M + 3) / 4;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nq; t += gridDim.x * blockDim.x) {
+    const int i0 = 4 * t;
+    int p[4];
+    if (i0 + 3 < M) {
+      const int4 v = *reinterpret_cast<const int4*>(perm + i0);
+      p[0] = v.x;
+      p[1] = v.y;
+      p[2] = v.z;
+      p[3] = v.w;
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) p[j] = i0 + j < M ? perm[i0 + j] : -1;
+    }
+    T v[DIM][4];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) v[d][j] = p[j] >= 0 ? cs[d][p[j]] : (T)0;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      T r[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) r[j] = scaled_coord(v[d][j], g.nf[d], g.prenorm);
+      if (i0 + 3 < M) {
+        store_quad(os[d] + i0, r);  // 16-byte aligned: 256-aligned arrays, i0 % 4 == 0
+      } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          if (p[j] >= 0) os[d][i0 + j] = r[j];
+      }
+    }
+  }
+}
+
 __global__ void k_keys_to_bins(const int* __restrict__ K, int64_t M, int cbits, int* __restrict__ out) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < M; i += (int64_t)gridDim.x * blockDim.x)
     out[i] = K[i] >> cbits;
@@ -509,6 +567,11 @@ cudaError_t launch_sort(const SortLayout& L, const Geom& g, int ns, const void* 
     if (e != cudaSuccess) return e;
   }
   const int bgrid = (int)std::max<int64_t>(1, std::min<int64_t>((M / 4 + 256) / 256, (int64_t)num_sms() * 8));
+  if (M > 0) {
+    auto sc = g.dim == 1 ? k_sorted_coords<T, 1> : (g.dim == 2 ? k_sorted_coords<T, 2> : k_sorted_coords<T, 3>);
+    sc<<<bgrid, 256, 0, st>>>((const T*)x, (const T*)y, (const T*)z, P.perm, (int)M, g, (T*)P.coord[0],
+                              (T*)P.coord[1], (T*)P.coord[2]);
+  }
   k_bin_bounds<<<bgrid, 256, 0, st>>>(P.keys_sorted, (int)M, L.cbits, g.nbins, P.bin_start);
   const int max_subs = (int)std::min<int64_t>(L.max_subs, INT32_MAX);
   const size_t sub_smem = g.nbins <= kSubSmemBins ? (size_t)(g.nbins + 1) * sizeof(int) : 0;

@@ -41,9 +41,7 @@ struct Pow<NS, 0> {
 
 template <typename T>
 struct PointArgs {
-  const T* x;
-  const T* y;
-  const T* z;
+  const T* sc[3];  // folded coordinates in sorted order (SortView::coord); unused axes nullptr
   int64_t M;
   int n_trans;
   int64_t grid_stride;  // complex elements per transform of the fine grid
@@ -94,9 +92,10 @@ __device__ __forceinline__ int wrap_up(int i, int n) {
   return i;
 }
 
+// Folded coordinate of axis d of the k-th sorted point (a coalesced read).
 template <typename T>
-__device__ __forceinline__ T coord(const PointArgs<T>& a, int d, int p) {
-  return d == 0 ? a.x[p] : (d == 1 ? a.y[p] : a.z[p]);
+__device__ __forceinline__ T sorted_coord(const PointArgs<T>& a, int d, int k) {
+  return a.sc[d][k];
 }
 
 // ---------------------------------------------------------------------------
@@ -133,19 +132,19 @@ __device__ __forceinline__ void flush_tile(const Geom& g, const int o[3], const 
   }
 }
 
-// Folds a point's coordinates xv, computes its tile offset and per-axis
-// weights.  Returns false for a point outside its bin's tile (possible only
-// when coordinates changed after the sort: such a point is dropped instead of
-// indexing out of the tile).
+// From a point's folded coordinates xf (in [0, nf]), computes its tile offset
+// and per-axis weights.  Returns false for a point outside its bin's tile (the
+// folded coordinates come from the same sort as the bins, so this does not
+// happen; the check keeps a corrupted workspace from indexing out of the tile).
 template <typename T, int DIM, int NS>
-__device__ __forceinline__ bool footprint(const PointArgs<T>& a, const T (&xv)[DIM], const int o[3], int row,
+__device__ __forceinline__ bool footprint(const PointArgs<T>& a, const T (&xf)[DIM], const int o[3], int row,
                                           int plane, int& off, T (&w)[DIM][NS]) {
   const Geom& g = a.g;
   bool inside = true;
   off = 0;
 #pragma unroll
   for (int d = 0; d < DIM; ++d) {
-    const T xs = scaled_coord(xv[d], g.nf[d], g.prenorm);
+    const T xs = xf[d];
     const int i0 = left_cell<T, NS>(xs);
     const int l = wrap_index(i0, g.nf[d]) - o[d];
     inside = inside && (unsigned)l < (unsigned)g.tile[d];
@@ -156,17 +155,17 @@ __device__ __forceinline__ bool footprint(const PointArgs<T>& a, const T (&xv)[D
 }
 
 template <typename T, int DIM>
-__device__ __forceinline__ void load_coords(const PointArgs<T>& a, int p, T (&xv)[DIM]) {
+__device__ __forceinline__ void load_sorted(const PointArgs<T>& a, int k, T (&xf)[DIM]) {
 #pragma unroll
-  for (int d = 0; d < DIM; ++d) xv[d] = coord(a, d, p);
+  for (int d = 0; d < DIM; ++d) xf[d] = sorted_coord(a, d, k);
 }
 
 template <typename T, int DIM, int NS>
-__device__ __forceinline__ bool point_footprint(const PointArgs<T>& a, int p, const int o[3], int row, int plane,
+__device__ __forceinline__ bool point_footprint(const PointArgs<T>& a, int k, const int o[3], int row, int plane,
                                                 int& off, T (&w)[DIM][NS]) {
-  T xv[DIM];
-  load_coords<T, DIM>(a, p, xv);
-  return footprint<T, DIM, NS>(a, xv, o, row, plane, off, w);
+  T xf[DIM];
+  load_sorted<T, DIM>(a, k, xf);
+  return footprint<T, DIM, NS>(a, xf, o, row, plane, off, w);
 }
 
 // Slot helpers of the run-merging spread: 16-byte chunks of four floats or two
@@ -383,8 +382,8 @@ __device__ __forceinline__ void spread_subproblem_runs(const PointArgs<T>& a, co
 #pragma unroll
       for (int r = 0; r < RPL; ++r) acc[r].x = acc[r].y = (T)0;
     };
-    // software pipeline: coordinates and strength of this lane's point in the
-    // current batch (xn, cn) and the point index of the next batch (pn)
+    // software pipeline: folded coordinates and strength of this lane's point
+    // in the current batch (xn, cn) and the point index of the next batch (pn)
     T xn[DIM];
     CT cn;
     cn.x = cn.y = (T)0;
@@ -392,7 +391,7 @@ __device__ __forceinline__ void spread_subproblem_runs(const PointArgs<T>& a, co
     for (int d = 0; d < DIM; ++d) xn[d] = (T)0;
     int pn = w0 + lane < w1 ? a.s.perm[w0 + lane] : -1;
     if (pn >= 0) {
-      load_coords<T, DIM>(a, pn, xn);
+      load_sorted<T, DIM>(a, w0 + lane, xn);
       cn = ct[pn];
     }
     pn = w0 + 32 + lane < w1 ? a.s.perm[w0 + 32 + lane] : -1;
@@ -402,8 +401,8 @@ __device__ __forceinline__ void spread_subproblem_runs(const PointArgs<T>& a, co
 #pragma unroll
       for (int d = 0; d < DIM; ++d) xv[d] = xn[d];
       CT cv = cn;
-      if (pn >= 0) {  // next batch
-        load_coords<T, DIM>(a, pn, xn);
+      if (pn >= 0) {  // next batch (pn >= 0 exactly when kb + 32 + lane < w1)
+        load_sorted<T, DIM>(a, kb + 32 + lane, xn);
         cn = ct[pn];
       }
       pn = kb + 64 + lane < w1 ? a.s.perm[kb + 64 + lane] : -1;
@@ -502,7 +501,7 @@ __device__ __forceinline__ void spread_subproblem_cells(const PointArgs<T>& a, c
         const int p = a.s.perm[k];
         int off;
         T w[DIM][NS];
-        const bool inside = point_footprint<T, DIM, NS>(a, p, o, row, plane, off, w);
+        const bool inside = point_footprint<T, DIM, NS>(a, k, o, row, plane, off, w);
 #pragma unroll
         for (int d = 0; d < DIM; ++d)
 #pragma unroll
@@ -651,7 +650,7 @@ __device__ __forceinline__ void spread_subproblem_owner(const PointArgs<T>& a, c
       if (k < k1) {
         const int p = a.s.perm[k];
         T xv[3];
-        load_coords<T, 3>(a, p, xv);
+        load_sorted<T, 3>(a, k, xv);
         int off;
         T w[3][NS];
         const bool inside = footprint<T, 3, NS>(a, xv, o, row, plane, off, w);
@@ -791,8 +790,8 @@ __device__ __forceinline__ T axis_weight_q(const PointArgs<T>& a, const float (&
   return es_weight(rn_sub((T)(i0 + q), xs), a.beta, a.kc);
 }
 
-// Folded coordinates, left cells and tile offset of a point with raw
-// coordinates xv (false: outside its bin's tile, see footprint).
+// Left cells and tile offset of a point with folded coordinates xv (false:
+// outside its bin's tile, see footprint).
 template <typename T, int NS>
 __device__ __forceinline__ bool group_point(const PointArgs<T>& a, const T (&xv)[3], const int o[3], int row,
                                             int plane, int& off, T (&xs)[3], int (&i0)[3]) {
@@ -801,7 +800,7 @@ __device__ __forceinline__ bool group_point(const PointArgs<T>& a, const T (&xv)
   off = 0;
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    xs[d] = scaled_coord(xv[d], g.nf[d], g.prenorm);
+    xs[d] = xv[d];
     i0[d] = left_cell<T, NS>(xs[d]);
     const int l = wrap_index(i0[d], g.nf[d]) - o[d];
     inside = inside && (unsigned)l < (unsigned)g.tile[d];
@@ -810,11 +809,11 @@ __device__ __forceinline__ bool group_point(const PointArgs<T>& a, const T (&xv)
   return inside;
 }
 
-// One round of 32 points for a warp: lane L folds point kb + L (left cells,
+// One round of 32 points for a warp: lane L takes point kb + L (left cells,
 // tile offset; off = -1 outside the tile); the lane groups then take the
-// points PPW at a time by shuffles (group_take).  The gathers are pipelined
-// across rounds: the permutation entries two rounds ahead and the coordinates
-// one round ahead are in flight while a round is processed.
+// points PPW at a time by shuffles (group_take).  The loads are pipelined
+// across rounds: the next round's permutation entries and folded coordinates
+// (both read in sorted order) are in flight while a round is processed.
 template <typename T>
 struct WarpPoints {
   int p, off;
@@ -828,9 +827,10 @@ __device__ __forceinline__ int round_perm(const SortView& s, int kb, int k1) {
 }
 
 template <typename T>
-__device__ __forceinline__ void round_coords(const PointArgs<T>& a, int p, T (&xv)[3]) {
+__device__ __forceinline__ void round_coords(const PointArgs<T>& a, int kb, int k1, T (&xv)[3]) {
+  const int k = kb + (threadIdx.x & 31);
 #pragma unroll
-  for (int d = 0; d < 3; ++d) xv[d] = p >= 0 ? coord(a, d, p) : (T)0;
+  for (int d = 0; d < 3; ++d) xv[d] = k < k1 ? sorted_coord(a, d, k) : (T)0;
 }
 
 template <typename T, int NS>
@@ -902,16 +902,14 @@ __device__ __forceinline__ void interp3_group(const PointArgs<T>& a, const cplx_
     __syncthreads();
     constexpr int kStep = NW * 32;
     int p_cur = round_perm(a.s, k0 + warp * 32, k1);
-    int p_next = round_perm(a.s, k0 + warp * 32 + kStep, k1);
     T x_cur[3];
-    round_coords(a, p_cur, x_cur);
+    round_coords(a, k0 + warp * 32, k1, x_cur);
     for (int kb = k0 + warp * 32; kb < k1; kb += kStep) {  // warp-uniform
-      const int p_after = round_perm(a.s, kb + 2 * kStep, k1);
+      const int p_next = round_perm(a.s, kb + kStep, k1);
       T x_next[3];
-      round_coords(a, p_next, x_next);
+      round_coords(a, kb + kStep, k1, x_next);
       const WarpPoints<T> wp = warp_points<T, NS>(a, p_cur, x_cur, o, row, plane);
       p_cur = p_next;
-      p_next = p_after;
 #pragma unroll
       for (int d = 0; d < 3; ++d) x_cur[d] = x_next[d];
       const int npts = min(32, k1 - kb);
@@ -987,15 +985,14 @@ __device__ __forceinline__ void interp_subproblem(const PointArgs<T>& a, const c
       __syncthreads();
       stage_tile<T>(g, o, fw + (int64_t)t * a.grid_stride, s_tile);
       __syncthreads();
-      // gathers pipelined across iterations: the permutation two iterations
-      // ahead, the coordinates one iteration ahead
+      // loads pipelined across iterations: the next iteration's permutation
+      // entry and folded coordinates (both in sorted order)
       const int kStep = blockDim.x;
       int k = k0 + threadIdx.x;
       int p_cur = k < k1 ? a.s.perm[k] : 0;
-      int p_next = k + kStep < k1 ? a.s.perm[k + kStep] : 0;
       T x_cur[DIM];
 #pragma unroll
-      for (int d = 0; d < DIM; ++d) x_cur[d] = k < k1 ? coord(a, d, p_cur) : (T)0;
+      for (int d = 0; d < DIM; ++d) x_cur[d] = k < k1 ? sorted_coord(a, d, k) : (T)0;
       for (; k < k1; k += kStep) {
         const int p = p_cur;
         T xv[DIM];
@@ -1003,18 +1000,16 @@ __device__ __forceinline__ void interp_subproblem(const PointArgs<T>& a, const c
         for (int d = 0; d < DIM; ++d) xv[d] = x_cur[d];
         {
           const bool more = k + kStep < k1;
-          const int p_after = k + 2 * kStep < k1 ? a.s.perm[k + 2 * kStep] : 0;
+          p_cur = more ? a.s.perm[k + kStep] : 0;
 #pragma unroll
-          for (int d = 0; d < DIM; ++d) x_cur[d] = more ? coord(a, d, p_next) : (T)0;
-          p_cur = p_next;
-          p_next = p_after;
+          for (int d = 0; d < DIM; ++d) x_cur[d] = more ? sorted_coord(a, d, k + kStep) : (T)0;
         }
         T w[DIM][NS];
         int off = 0;
         bool inside = true;
 #pragma unroll
         for (int d = 0; d < DIM; ++d) {
-          const T xs = scaled_coord(xv[d], g.nf[d], g.prenorm);
+          const T xs = xv[d];
           const int i0 = left_cell<T, NS>(xs);
           const int l = wrap_index(i0, g.nf[d]) - o[d];
           inside = inside && (unsigned)l < (unsigned)g.tile[d];
@@ -1154,8 +1149,8 @@ __global__ void __launch_bounds__(NW * 32) k_grad(PointArgs<T> a, const cplx_t<T
       __syncthreads();
       stage_tile<T>(g, o, G + (int64_t)t * a.grid_stride, s_tile);
       __syncthreads();
-      // gathers pipelined across iterations: the permutation two iterations
-      // ahead, coordinates and V one iteration ahead
+      // loads pipelined across iterations: the permutation two iterations
+      // ahead, folded coordinates (sorted order) and V one iteration ahead
       const int kStep = blockDim.x;
       int k = k0 + threadIdx.x;
       int p_cur = k < k1 ? a.s.perm[k] : 0;
@@ -1164,7 +1159,7 @@ __global__ void __launch_bounds__(NW * 32) k_grad(PointArgs<T> a, const cplx_t<T
       CT v_cur;
       v_cur.x = v_cur.y = (T)0;
 #pragma unroll
-      for (int d = 0; d < DIM; ++d) x_cur[d] = k < k1 ? coord(a, d, p_cur) : (T)0;
+      for (int d = 0; d < DIM; ++d) x_cur[d] = k < k1 ? sorted_coord(a, d, k) : (T)0;
       if (k < k1) v_cur = V[(int64_t)t * a.M + p_cur];
       for (; k < k1; k += kStep) {
         const int p = p_cur;
@@ -1176,7 +1171,7 @@ __global__ void __launch_bounds__(NW * 32) k_grad(PointArgs<T> a, const cplx_t<T
           const bool more = k + kStep < k1;
           const int p_after = k + 2 * kStep < k1 ? a.s.perm[k + 2 * kStep] : 0;
 #pragma unroll
-          for (int d = 0; d < DIM; ++d) x_cur[d] = more ? coord(a, d, p_next) : (T)0;
+          for (int d = 0; d < DIM; ++d) x_cur[d] = more ? sorted_coord(a, d, k + kStep) : (T)0;
           if (more) v_cur = V[(int64_t)t * a.M + p_next];
           p_cur = p_next;
           p_next = p_after;
@@ -1186,7 +1181,7 @@ __global__ void __launch_bounds__(NW * 32) k_grad(PointArgs<T> a, const cplx_t<T
         bool inside = true;
 #pragma unroll
         for (int d = 0; d < DIM; ++d) {
-          const T xs = scaled_coord(xv[d], g.nf[d], g.prenorm);
+          const T xs = xv[d];
           const int i0 = left_cell<T, NS>(xs);
           const int l = wrap_index(i0, g.nf[d]) - o[d];
           inside = inside && (unsigned)l < (unsigned)g.tile[d];
@@ -1426,12 +1421,9 @@ cudaError_t dispatch_grad(int ns, const PointArgs<T>& a, const void* G, const vo
 }
 
 template <typename T>
-PointArgs<T> make_args(const Geom& g, double beta, double kc, const void* x, const void* y, const void* z, int64_t M,
-                       int n_trans, const SortView& s) {
+PointArgs<T> make_args(const Geom& g, double beta, double kc, int64_t M, int n_trans, const SortView& s) {
   PointArgs<T> a;
-  a.x = (const T*)x;
-  a.y = (const T*)y;
-  a.z = (const T*)z;
+  for (int d = 0; d < 3; ++d) a.sc[d] = (const T*)s.coord[d];
   a.M = M;
   a.n_trans = n_trans;
   a.grid_stride = (int64_t)g.nf[0] * g.nf[1] * g.nf[2];

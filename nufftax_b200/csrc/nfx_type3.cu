@@ -52,12 +52,19 @@ __global__ void k_minmax(const T* __restrict__ a, int64_t n, double* __restrict_
 }
 
 // partial: [2*dim arrays][kT3Blocks][2]; arrays 0..dim-1 sources, dim..2dim-1 targets.
+// The scalars are computed in the working type T in the reference's order
+// (nufft3.py:258-268, 354-362), with the Python constants rounded to T first
+// as JAX's weak typing does: C = (min + max) / 2, S = max((max - min) / 2,
+// 1e-10), gamma = nf / ((2 upsampfac) S); h = 2 pi / nf stays a double (it is a
+// Python float there) and is rounded to T where it meets a T array.  The mins
+// and maxes are values of T, so every result is exactly the reference's.
+template <typename T>
 __global__ void k_t3_params(const double* __restrict__ partial, int dim, int nf0, int nf1, int nf2,
                             double upsampfac, T3Params* __restrict__ p) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   const int nf[3] = {nf0, nf1, nf2};
   for (int d = 0; d < dim; ++d) {
-    double mn[2], mx[2];
+    T mn[2], mx[2];
     for (int s = 0; s < 2; ++s) {
       const double* q = partial + (size_t)(s * dim + d) * kT3Blocks * 2;
       double a = 1e300, b = -1e300;
@@ -65,14 +72,18 @@ __global__ void k_t3_params(const double* __restrict__ partial, int dim, int nf0
         a = fmin(a, q[2 * i]);
         b = fmax(b, q[2 * i + 1]);
       }
-      mn[s] = a;
-      mx[s] = b;
+      mn[s] = (T)a;
+      mx[s] = (T)b;
     }
-    p->C[d] = (mn[0] + mx[0]) / 2.0;
-    p->D[d] = (mn[1] + mx[1]) / 2.0;
-    p->S[d] = fmax((mx[1] - mn[1]) / 2.0, 1e-10);
+    const T C = rn_add(mn[0], mx[0]) / (T)2.0;
+    const T D = rn_add(mn[1], mx[1]) / (T)2.0;
+    const T half = rn_sub(mx[1], mn[1]) / (T)2.0;
+    const T S = half > (T)1e-10 ? half : (T)1e-10;
+    p->C[d] = (double)C;
+    p->D[d] = (double)D;
+    p->S[d] = (double)S;
     p->h[d] = 2.0 * kPi / nf[d];
-    p->gamma[d] = nf[d] / (2.0 * upsampfac * p->S[d]);
+    p->gamma[d] = (double)((T)nf[d] / rn_mul((T)(2.0 * upsampfac), S));
   }
 }
 
@@ -87,7 +98,8 @@ __global__ void k_t3_sources(int dim, const T* __restrict__ x0, const T* __restr
     double phase = 0.0;
     for (int d = 0; d < dim; ++d) {
       const T x = xs[d][j];
-      const T r = (x - (T)p->C[d]) / (T)p->gamma[d];
+      // x' = (x - C) / gamma in T (nufft3.py:271, 365-366)
+      const T r = rn_sub(x, (T)p->C[d]) / (T)p->gamma[d];
       os[d][j] = premod(r);
       phase += p->D[d] * (double)x;
     }
@@ -119,9 +131,10 @@ __global__ void k_t3_targets(int dim, const T* __restrict__ s0, const T* __restr
     double phase = 0.0, phi_prod = 1.0;
     for (int d = 0; d < dim; ++d) {
       const T s = ss[d][k];
-      const T r = (T)(p->h[d] * p->gamma[d]) * (s - (T)p->D[d]);
+      // s' = (h gamma) (s - D) in T, in the reference's order (nufft3.py:287, 381-382)
+      const T r = rn_mul(rn_mul((T)p->h[d], (T)p->gamma[d]), rn_sub(s, (T)p->D[d]));
       os[d][k] = premod(r);
-      const double sr = p->h[d] * p->gamma[d] * ((double)s - p->D[d]);
+      const double sr = (double)r;
       double acc = 0.0;
       for (int q = 0; q < nq; ++q) {
         const double z = -j2 + q * dz;
@@ -172,8 +185,8 @@ static cudaError_t t3_prepare(int dim, const int nf[3], int nspread, double beta
     k_minmax<T><<<kT3Blocks, 256, 0, st>>>((const T*)src[d], M, partial + (size_t)d * kT3Blocks * 2);
     k_minmax<T><<<kT3Blocks, 256, 0, st>>>((const T*)tgt[d], K, partial + (size_t)(dim + d) * kT3Blocks * 2);
   }
-  k_t3_params<<<1, 32, 0, st>>>(partial, dim, nf[0], dim > 1 ? nf[1] : 1, dim > 2 ? nf[2] : 1, upsampfac,
-                                (T3Params*)params);
+  k_t3_params<T><<<1, 32, 0, st>>>(partial, dim, nf[0], dim > 1 ? nf[1] : 1, dim > 2 ? nf[2] : 1, upsampfac,
+                                   (T3Params*)params);
   const T* s3[3] = {nullptr, nullptr, nullptr};
   const T* t3[3] = {nullptr, nullptr, nullptr};
   T* so[3] = {nullptr, nullptr, nullptr};

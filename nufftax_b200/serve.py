@@ -73,12 +73,12 @@ def estimate_bytes(req: Request) -> int:
     kp = compute_kernel_params(req.eps)
     pts = req.M
     inputs = pts * (4 * req.dim + 8)
-    sort_ws = pts * 22 + 4 * 1024 * 1024
+    sort_ws = pts * (22 + 4 * req.dim) + 4 * 1024 * 1024  # sort tables + sorted folded coordinates
     if req.kind == 3:
         nf = [compute_grid_size(n, 2.0, kp.nspread) for n in req.n_modes]
         grid = 8 * math.prod(req.n_modes) + 2 * 8 * math.prod(nf)
         out = req.K * (8 + 4 * req.dim) * 2
-        sort_ws += req.K * 22
+        sort_ws += req.K * (22 + 4 * req.dim)
     else:
         nf = [compute_grid_size(n, 2.0, kp.nspread) for n in req.n_modes]
         grid = 2 * 8 * math.prod(nf)
@@ -92,6 +92,10 @@ class _Slot:
         self.req: Optional[Request] = None
         self.done = torch.cuda.Event()
         self.grids: list = []
+        # sorted point sets the request in flight reads: kept alive until the
+        # slot's completion event, so an eviction from the points cache cannot
+        # free a workspace that this slot's stream still reads
+        self.held: list = []
         self.ws: Optional[torch.Tensor] = None  # sort workspace, reused by the slot's next request
 
     def workspace(self, nbytes: int, device) -> torch.Tensor:
@@ -171,8 +175,10 @@ class NufftServer:
             ps, ev = self.points_cache[key]
             self.points_cache.move_to_end(key)
             slot.stream.wait_event(ev)
+            slot.held.append(ps)
             return ps
         ps = PointSort(list(coords), nf, kp, prenorm=True)
+        slot.held.append(ps)
         if key is not None:
             ev = torch.cuda.Event()
             ev.record(slot.stream)
@@ -301,6 +307,7 @@ class NufftServer:
                 for key, g in s.grids:
                     self._return_grid(key, g)
                 s.grids = []
+                s.held = []
                 s.req = None
                 if req.make_inputs is not None:  # inputs were generated here: release them
                     req.coords = req.strengths = req.targets = None

@@ -12,14 +12,27 @@ current CUDA device and back).  Every numerical step runs in libnfx_b200:
   type 3 (nufftax/transforms/nufft3.py:216-515): on-device centring/scaling and
          pre-phase -> spread -> inner type 2 -> phihat(s') and phase correction.
 
-Autograd (torch convention G = dL/dRe + i dL/dIm) replaces the JAX primitives'
-JVP/transpose rules (nufftax/transforms/primitives.py):
-  type 1: dc = type-2 adjoint pipeline of G; dx from the ES-derivative adjoint
-          kernel on the same grid (one fused pass for dc, dx, dy, dz);
-  type 2: df = type-1 adjoint pipeline of G; dx from the ES-derivative
-          interpolation of the forward fine grid;
-  type 3: dc, dx, ds through type-3 transforms of weighted cotangents
-          (primitives.py:534-659).
+The three transforms are torch.autograd.Functions that take the place of the
+JAX primitives of nufftax/transforms/primitives.py, with the same three rules:
+
+  reverse mode (torch convention G = dL/dRe + i dL/dIm; the transpose rules):
+    type 1: dc = type-2 adjoint pipeline of G; dx from the ES-derivative adjoint
+            kernel on the same grid (one fused pass for dc, dx, dy, dz);
+    type 2: df = type-1 adjoint pipeline of G; dx from the ES-derivative
+            interpolation of the forward fine grid;
+    type 3: dc, dx, ds through type-3 transforms of weighted cotangents
+            (primitives.py:534-659);
+  forward mode (torch.func.jvp, torch.autograd.forward_ad; the JVP rules of
+    primitives.py:271-284, 443-465, 606-633): the tangent is the transform of
+    dc (df) plus k-weighted transforms for the coordinate tangents, all of them
+    stacked along n_trans into ONE call, so they share one sort and one launch
+    of each kernel;
+  batching (torch.func.vmap; the batcher of primitives.py:28-48): a batch of
+    strengths / modes over shared coordinates becomes the n_trans axis of one
+    call; batched coordinates run one call per batch element.
+
+The `*_jvp` names are the same functions, as in nufftax (autodiff.py:150-161):
+forward and reverse mode flow through the same Functions.
 """
 
 from __future__ import annotations
@@ -29,6 +42,7 @@ from typing import Sequence
 
 import numpy as np
 import torch
+import torch.autograd.forward_ad as _fwad
 
 from . import _lib
 from ._plan import (PointSort, complex_dtype, deconv_pad, deconv_shuffle, fft_inplace, precision_of, ptr,
@@ -104,36 +118,65 @@ def _fft_sign_type2(isign: int) -> int:
     return -1 if isign < 0 else 1
 
 
-class _NoGradCtx:
-    """Stands in for the autograd context when no input needs a gradient: the
-    forward pass then runs without autograd's bookkeeping."""
-
-    needs_input_grad = ()
-
-    def save_for_backward(self, *tensors):
-        pass
+_is_wrapped = torch._C._functorch.is_functorch_wrapped_tensor
 
 
-def _needs_grad(*tensors) -> bool:
-    return torch.is_grad_enabled() and any(t.requires_grad for t in tensors)
+def _tracked(*tensors) -> bool:
+    """Whether the call must go through the autograd Function: an input needs a
+    gradient, forward-mode AD is active, or a torch.func transform (vmap, jvp,
+    grad) wraps an input.  Otherwise the forward runs directly, without
+    autograd's bookkeeping."""
+    if _fwad._current_level >= 0:
+        return True
+    grad = torch.is_grad_enabled()
+    for t in tensors:
+        if (grad and t.requires_grad) or _is_wrapped(t):
+            return True
+    return False
+
+
+def _modes_axis(n: int, d: int, dim: int, device, dtype) -> torch.Tensor:
+    """CMCL integer modes of axis d (k = -n/2 .. (n-1)/2) shaped to broadcast
+    against a (n_trans, n_dim, ..., n_1) array."""
+    k = torch.arange(-(n // 2), (n + 1) // 2, device=device, dtype=dtype)
+    shape = [1] * (dim + 1)
+    shape[dim - d] = n
+    return k.reshape(shape)
+
+
+def _bdim_front(t, bdim, B):
+    """Batch axis moved to the front (an unbatched input is expanded)."""
+    if bdim is None:
+        return t.unsqueeze(0).expand((B,) + tuple(t.shape))
+    return t.movedim(bdim, 0)
 
 
 # ---------------------------------------------------------------------------
 # Type 1
 # ---------------------------------------------------------------------------
+def _type1_forward(c2, n_modes, eps, isign, uf, coords):
+    dim = len(coords)
+    kp = compute_kernel_params(eps, uf)
+    nf = tuple(compute_grid_size(n, uf, kp.nspread) for n in n_modes)
+    ps = sort_cache.get(list(coords), nf, kp, prenorm=True)
+    fw = ps.spread(c2)
+    fft_inplace(fw, dim, _fft_sign_type1(isign))
+    return deconv_shuffle(fw, n_modes, kp)
+
+
 class _Type1(torch.autograd.Function):
+    """f = type 1 (c2 at coords), c2: (n_trans, M) -> (n_trans, N_d..N_1)."""
+
     @staticmethod
-    def forward(ctx, c2, n_modes, eps, isign, uf, uf_t, *coords):
-        dim = len(coords)
-        kp = compute_kernel_params(eps, uf)
-        nf = tuple(compute_grid_size(n, uf, kp.nspread) for n in n_modes)
-        ps = sort_cache.get(list(coords), nf, kp, prenorm=True)
-        fw = ps.spread(c2)
-        fft_inplace(fw, dim, _fft_sign_type1(isign))
-        f = deconv_shuffle(fw, n_modes, kp)
+    def forward(c2, n_modes, eps, isign, uf, uf_t, *coords):
+        return _type1_forward(c2, n_modes, eps, isign, uf, coords)
+
+    @staticmethod
+    def setup_context(ctx, inputs, output):
+        c2, n_modes, eps, isign, uf, uf_t, *coords = inputs
         ctx.meta = (n_modes, eps, isign, uf, uf_t)
         ctx.save_for_backward(c2, *coords)
-        return f
+        ctx.save_for_forward(c2, *coords)
 
     @staticmethod
     def backward(ctx, G):
@@ -154,6 +197,46 @@ class _Type1(torch.autograd.Function):
             dc = ps.interp(H)
         return (dc, None, None, None, None, None, *dxs)
 
+    @staticmethod
+    def jvp(ctx, dc, _n, _e, _i, _u, _ut, *dxs):
+        # df = T1(dc) + sum_d (i isign k_d) T1(c dx_d)   (primitives.py:271-284, 443-465)
+        c2, *coords = ctx.saved_tensors
+        n_modes, eps, isign, uf, uf_t = ctx.meta
+        dim = len(coords)
+        nt = c2.shape[0]
+        parts = ([dc] if dc is not None else []) + [c2 * dx.to(c2.dtype)[None, :] for dx in dxs if dx is not None]
+        if not parts:
+            return None
+        F = _type1_forward(torch.cat(parts, 0).contiguous(), n_modes, eps, isign, uf, coords)
+        i = 0
+        out = None
+        if dc is not None:
+            out = F[:nt]
+            i = nt
+        for d, dx in enumerate(dxs):
+            if dx is None:
+                continue
+            k = _modes_axis(n_modes[d], d, dim, F.device, F.real.dtype)
+            term = (1j * isign) * k * F[i:i + nt]
+            out = term if out is None else out + term
+            i += nt
+        return out
+
+    @staticmethod
+    def vmap(info, in_dims, c2, n_modes, eps, isign, uf, uf_t, *coords):
+        cdim, xdims = in_dims[0], in_dims[6:]
+        B = info.batch_size
+        if all(d is None for d in xdims):
+            # shared points: the batch becomes part of n_trans (one call)
+            cb = _bdim_front(c2, cdim, B)
+            nt = cb.shape[1]
+            f = _Type1.apply(cb.reshape((B * nt,) + tuple(cb.shape[2:])), n_modes, eps, isign, uf, uf_t, *coords)
+            return f.reshape((B, nt) + tuple(f.shape[1:])), 0
+        cb = _bdim_front(c2, cdim, B)
+        xb = [_bdim_front(x, d, B) for x, d in zip(coords, xdims)]
+        outs = [_Type1.apply(cb[b], n_modes, eps, isign, uf, uf_t, *[x[b] for x in xb]) for b in range(B)]
+        return torch.stack(outs, 0), 0
+
 
 def _type1(coords, c, n_modes: Sequence[int], eps, isign, upsampfac):
     bd = _Boundary(c, *coords)
@@ -167,7 +250,7 @@ def _type1(coords, c, n_modes: Sequence[int], eps, isign, upsampfac):
         raise ValueError("c must have M entries along its last axis")
     uf, uf_t = _split_upsampfac(upsampfac)
     args = (c2, tuple(int(n) for n in n_modes), float(eps), int(isign), uf, uf_t, *xs)
-    f = _Type1.apply(*args) if _needs_grad(c2, *xs) else _Type1.forward(_NoGradCtx(), *args)
+    f = _Type1.apply(*args) if _tracked(c2, *xs) else _Type1.forward(*args)
     return bd.back(f if batched else f[0])
 
 
@@ -191,26 +274,38 @@ def nufft3d1(x, y, z, c, n_modes, eps: float = 1e-6, isign: int = 1, upsampfac=2
 # ---------------------------------------------------------------------------
 # Type 2
 # ---------------------------------------------------------------------------
+def _type2_grid(f2, n_modes, eps, isign, uf, dim):
+    kp = compute_kernel_params(eps, uf)
+    nf = tuple(compute_grid_size(n, uf, kp.nspread) for n in n_modes)
+    fw = deconv_pad(f2, nf, kp)
+    fft_inplace(fw, dim, _fft_sign_type2(isign))
+    return fw, nf, kp
+
+
+def _type2_forward(f2, eps, isign, uf, coords):
+    dim = len(coords)
+    n_modes = tuple(int(v) for v in reversed(f2.shape[1:]))
+    fw, nf, kp = _type2_grid(f2, n_modes, eps, isign, uf, dim)
+    return sort_cache.get(list(coords), nf, kp, prenorm=True).interp(fw)
+
+
 class _Type2(torch.autograd.Function):
+    """c = type 2 (f2 at coords), f2: (n_trans, N_d..N_1) -> (n_trans, M)."""
+
     @staticmethod
-    def forward(ctx, f2, eps, isign, uf, uf_t, *coords):
-        dim = len(coords)
-        n_modes = tuple(int(v) for v in reversed(f2.shape[1:]))
-        kp = compute_kernel_params(eps, uf)
-        nf = tuple(compute_grid_size(n, uf, kp.nspread) for n in n_modes)
-        fw = deconv_pad(f2, nf, kp)
-        fft_inplace(fw, dim, _fft_sign_type2(isign))
-        ps = sort_cache.get(list(coords), nf, kp, prenorm=True)
-        c = ps.interp(fw)
-        ctx.meta = (n_modes, eps, isign, uf, uf_t)
-        ctx.ps = ps
-        need_x = any(ctx.needs_input_grad[5:])
-        ctx.save_for_backward(*coords, fw if need_x else None)
-        return c
+    def forward(f2, eps, isign, uf, uf_t, *coords):
+        return _type2_forward(f2, eps, isign, uf, coords)
+
+    @staticmethod
+    def setup_context(ctx, inputs, output):
+        f2, eps, isign, uf, uf_t, *coords = inputs
+        ctx.meta = (tuple(int(v) for v in reversed(f2.shape[1:])), eps, isign, uf, uf_t)
+        ctx.save_for_backward(f2, *coords)
+        ctx.save_for_forward(f2, *coords)
 
     @staticmethod
     def backward(ctx, G):
-        *coords, fw = ctx.saved_tensors
+        f2, *coords = ctx.saved_tensors
         n_modes, eps, isign, uf, uf_t = ctx.meta
         dim = len(coords)
         need_f = ctx.needs_input_grad[0]
@@ -224,8 +319,53 @@ class _Type2(torch.autograd.Function):
             gw = ps_t.spread(G)
             fft_inplace(gw, dim, -_fft_sign_type2(isign))
             df = deconv_shuffle(gw, n_modes, kp)
-        dxs = ctx.ps.interp_grad(fw, G, need_x) if any(need_x) else [None] * dim
+        dxs = [None] * dim
+        if any(need_x):
+            # the forward fine grid again (deconvolve + FFT), then the
+            # ES-derivative interpolation on it
+            fw, nf, kp = _type2_grid(f2.contiguous(), n_modes, eps, isign, uf, dim)
+            dxs = sort_cache.get(list(coords), nf, kp, prenorm=True).interp_grad(fw, G, need_x)
         return (df, None, None, None, None, *dxs)
+
+    @staticmethod
+    def jvp(ctx, df, _e, _i, _u, _ut, *dxs):
+        # dc = T2(df) + sum_d dx_d T2(i isign k_d f)   (primitives.py:211-231)
+        f2, *coords = ctx.saved_tensors
+        n_modes, eps, isign, uf, uf_t = ctx.meta
+        dim = len(coords)
+        nt = f2.shape[0]
+        parts = [df] if df is not None else []
+        for d, dx in enumerate(dxs):
+            if dx is not None:
+                parts.append((1j * isign) * _modes_axis(n_modes[d], d, dim, f2.device, f2.real.dtype) * f2)
+        if not parts:
+            return None
+        C = _type2_forward(torch.cat(parts, 0).contiguous(), eps, isign, uf, coords)
+        i = 0
+        out = None
+        if df is not None:
+            out = C[:nt]
+            i = nt
+        for dx in dxs:
+            if dx is None:
+                continue
+            term = dx.to(C.dtype)[None, :] * C[i:i + nt]
+            out = term if out is None else out + term
+            i += nt
+        return out
+
+    @staticmethod
+    def vmap(info, in_dims, f2, eps, isign, uf, uf_t, *coords):
+        fdim, xdims = in_dims[0], in_dims[5:]
+        B = info.batch_size
+        fb = _bdim_front(f2, fdim, B)
+        if all(d is None for d in xdims):
+            nt = fb.shape[1]
+            c = _Type2.apply(fb.reshape((B * nt,) + tuple(fb.shape[2:])), eps, isign, uf, uf_t, *coords)
+            return c.reshape((B, nt) + tuple(c.shape[1:])), 0
+        xb = [_bdim_front(x, d, B) for x, d in zip(coords, xdims)]
+        outs = [_Type2.apply(fb[b], eps, isign, uf, uf_t, *[x[b] for x in xb]) for b in range(B)]
+        return torch.stack(outs, 0), 0
 
 
 def _type2(coords, f, eps, isign, upsampfac):
@@ -238,7 +378,7 @@ def _type2(coords, f, eps, isign, upsampfac):
     f2 = (fd if batched else fd.unsqueeze(0)).contiguous()
     uf, uf_t = _split_upsampfac(upsampfac)
     args = (f2, float(eps), int(isign), uf, uf_t, *xs)
-    c = _Type2.apply(*args) if _needs_grad(f2, *xs) else _Type2.forward(_NoGradCtx(), *args)
+    c = _Type2.apply(*args) if _tracked(f2, *xs) else _Type2.forward(*args)
     return bd.back(c if batched else c[0])
 
 
@@ -306,12 +446,18 @@ def _type3_forward(src: list[torch.Tensor], c2: torch.Tensor, tgt: list[torch.Te
 
 
 class _Type3(torch.autograd.Function):
+    """f = type 3 (c2 at sources -> targets), c2: (n_trans, M) -> (n_trans, K)."""
+
     @staticmethod
-    def forward(ctx, c2, nf, eps, isign, uf, dim, *pts):
-        src, tgt = list(pts[:dim]), list(pts[dim:])
+    def forward(c2, nf, eps, isign, uf, dim, *pts):
+        return _type3_forward(list(pts[:dim]), c2, list(pts[dim:]), nf, eps, isign, uf)
+
+    @staticmethod
+    def setup_context(ctx, inputs, output):
+        c2, nf, eps, isign, uf, dim, *pts = inputs
         ctx.meta = (nf, eps, isign, uf, dim)
         ctx.save_for_backward(c2, *pts)
-        return _type3_forward(src, c2, tgt, nf, eps, isign, uf)
+        ctx.save_for_forward(c2, *pts)
 
     @staticmethod
     def backward(ctx, G):
@@ -342,6 +488,51 @@ class _Type3(torch.autograd.Function):
                 grads.append(None)
         return (dc, None, None, None, None, None, *grads)
 
+    @staticmethod
+    def jvp(ctx, dc, _nf, _e, _i, _u, _d, *dpts):
+        # df = T3(dc) + sum_d (i isign s_d) T3(c dx_d) + sum_d (i isign ds_d) T3(x_d c)
+        # (primitives.py:606-633), all strengths stacked into one call
+        c2, *pts = ctx.saved_tensors
+        nf, eps, isign, uf, dim = ctx.meta
+        src, tgt = pts[:dim], pts[dim:]
+        nt = c2.shape[0]
+        dxs, dss = dpts[:dim], dpts[dim:]
+        parts = [dc] if dc is not None else []
+        parts += [c2 * dx.to(c2.dtype)[None, :] for dx in dxs if dx is not None]
+        parts += [src[d].to(c2.dtype)[None, :] * c2 for d in range(dim) if dss[d] is not None]
+        if not parts:
+            return None
+        F = _type3_forward(list(src), torch.cat(parts, 0).contiguous(), list(tgt), nf, eps, isign, uf)
+        i = 0
+        out = None
+        if dc is not None:
+            out = F[:nt]
+            i = nt
+        for d, dx in enumerate(dxs):
+            if dx is not None:
+                term = (1j * isign) * tgt[d].to(F.dtype)[None, :] * F[i:i + nt]
+                out = term if out is None else out + term
+                i += nt
+        for d, ds in enumerate(dss):
+            if ds is not None:
+                term = (1j * isign) * ds.to(F.dtype)[None, :] * F[i:i + nt]
+                out = term if out is None else out + term
+                i += nt
+        return out
+
+    @staticmethod
+    def vmap(info, in_dims, c2, nf, eps, isign, uf, dim, *pts):
+        cdim, pdims = in_dims[0], in_dims[6:]
+        B = info.batch_size
+        cb = _bdim_front(c2, cdim, B)
+        if all(d is None for d in pdims):
+            nt = cb.shape[1]
+            f = _Type3.apply(cb.reshape((B * nt,) + tuple(cb.shape[2:])), nf, eps, isign, uf, dim, *pts)
+            return f.reshape((B, nt) + tuple(f.shape[1:])), 0
+        pb = [_bdim_front(p, d, B) for p, d in zip(pts, pdims)]
+        outs = [_Type3.apply(cb[b], nf, eps, isign, uf, dim, *[p[b] for p in pb]) for b in range(B)]
+        return torch.stack(outs, 0), 0
+
 
 def _type3(src, c, tgt, n_modes, eps, isign, upsampfac):
     dim = len(src)
@@ -355,7 +546,8 @@ def _type3(src, c, tgt, n_modes, eps, isign, upsampfac):
     nf = (int(n_modes),) if dim == 1 and np.isscalar(n_modes) else tuple(int(v) for v in n_modes)
     if len(nf) != dim:
         raise ValueError(f"n_modes must have {dim} entries")
-    f = _Type3.apply(c2, nf, float(eps), int(isign), float(upsampfac), dim, *xs, *ss)
+    args = (c2, nf, float(eps), int(isign), float(upsampfac), dim, *xs, *ss)
+    f = _Type3.apply(*args) if _tracked(c2, *xs, *ss) else _Type3.forward(*args)
     return bd.back(f if batched else f[0])
 
 
@@ -374,7 +566,8 @@ def nufft3d3(x, y, z, c, s, t, u, n_modes, eps: float = 1e-6, isign: int = 1, up
     return _type3([x, y, z], c, [s, t, u], n_modes, eps, isign, upsampfac)
 
 
-# Aliases kept by nufftax for backward compatibility (autodiff.py:153-161).
+# The *_jvp names of nufftax (autodiff.py:150-161): the same functions, whose
+# autograd Functions carry the forward-mode (jvp) and batching (vmap) rules.
 nufft1d1_jvp = nufft1d1
 nufft1d2_jvp = nufft1d2
 nufft2d1_jvp = nufft2d1

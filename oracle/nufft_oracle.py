@@ -260,6 +260,17 @@ def _flat_index_and_weights(coords, nf, kp):
     return idx.reshape(M, -1), w.reshape(M, -1)
 
 
+# Points per chunk of the spread / interp sums: the (M, ns^d) index and weight
+# tables of one chunk stay near 2^25 entries, so million-point inputs fit in
+# memory.  Chunking changes only the order of the float64 sums.
+_CHUNK_ENTRIES = 1 << 25
+
+
+def _chunks(M: int, nspread: int, dim: int):
+    step = max(1, _CHUNK_ENTRIES // (nspread ** dim))
+    return [(s, min(s + step, M)) for s in range(0, M, step)]
+
+
 def spread(coords: Sequence[np.ndarray], c: np.ndarray, nf: Sequence[int], kp: KernelParams) -> np.ndarray:
     """spread_{1,2,3}d_impl (nufftax/core/spread.py:285-339, 435-494, 596-658).
 
@@ -267,13 +278,15 @@ def spread(coords: Sequence[np.ndarray], c: np.ndarray, nf: Sequence[int], kp: K
     c: (M,) or (n_trans, M) complex.  Returns grid (n_trans?, nf_d..., nf_1), complex128.
     """
     c2 = c[None, :] if c.ndim == 1 else c
-    idx, w = _flat_index_and_weights(coords, nf, kp)
     ntot = int(np.prod(nf))
-    out = np.empty((c2.shape[0], ntot), dtype=np.complex128)
-    fi = idx.ravel()
-    for t in range(c2.shape[0]):
-        wc = (c2[t].astype(np.complex128)[:, None] * w).ravel()
-        out[t] = np.bincount(fi, weights=wc.real, minlength=ntot) + 1j * np.bincount(fi, weights=wc.imag, minlength=ntot)
+    out = np.zeros((c2.shape[0], ntot), dtype=np.complex128)
+    for a, b in _chunks(coords[0].shape[0], kp.nspread, len(coords)):
+        idx, w = _flat_index_and_weights([x[a:b] for x in coords], nf, kp)
+        fi = idx.ravel()
+        for t in range(c2.shape[0]):
+            wc = (c2[t, a:b].astype(np.complex128)[:, None] * w).ravel()
+            out[t] += np.bincount(fi, weights=wc.real, minlength=ntot) + 1j * np.bincount(
+                fi, weights=wc.imag, minlength=ntot)
     out = out.reshape((c2.shape[0],) + tuple(reversed(nf)))
     return out[0] if c.ndim == 1 else out
 
@@ -284,8 +297,12 @@ def interp(coords: Sequence[np.ndarray], fw: np.ndarray, kp: KernelParams) -> np
     nf = tuple(reversed(fw.shape[-dim:]))
     batched = fw.ndim == dim + 1
     f2 = fw.reshape((-1, int(np.prod(nf)))).astype(np.complex128)
-    idx, w = _flat_index_and_weights(coords, nf, kp)
-    out = np.stack([(f2[t][idx] * w).sum(axis=1) for t in range(f2.shape[0])])
+    M = coords[0].shape[0]
+    out = np.empty((f2.shape[0], M), dtype=np.complex128)
+    for a, b in _chunks(M, kp.nspread, dim):
+        idx, w = _flat_index_and_weights([x[a:b] for x in coords], nf, kp)
+        for t in range(f2.shape[0]):
+            out[t, a:b] = (f2[t][idx] * w).sum(axis=1)
     return out if batched else out[0]
 
 
@@ -461,28 +478,41 @@ def nufft_type2(coords: Sequence[np.ndarray], f: np.ndarray, eps: float = 1e-6, 
 
 def nufft_type3(src: Sequence[np.ndarray], c: np.ndarray, tgt: Sequence[np.ndarray], n_modes: Sequence[int],
                 eps: float = 1e-6, isign: int = 1, upsampfac: float = 2.0) -> np.ndarray:
-    """nufft{1,2,3}d3 (nufftax/transforms/nufft3.py:216-515), float64 host scalars."""
+    """nufft{1,2,3}d3 (nufftax/transforms/nufft3.py:216-515).
+
+    Dtype-faithful like the fold: the centres, half-widths and scales
+    (nufft3.py:258-268, 354-362) and the rescaled sources and targets
+    (nufft3.py:271-272, 287-288, 365-366, 381-384) are computed in the
+    coordinates' dtype in the reference's order, with Python constants rounded
+    to that dtype first (JAX weak typing): C = (min + max) / 2,
+    S = max((max - min) / 2, 1e-10), gamma = nf / ((2 upsampfac) S),
+    x' = (x - C) / gamma, s' = (h gamma) (s - D) with h = 2 pi / nf.  The
+    phases, phi-hat and the accumulations run in float64."""
     dim = len(src)
     kp = compute_kernel_params(eps, upsampfac)
     c2 = (c[None, :] if c.ndim == 1 else c).astype(np.complex128)
-    src = [np.asarray(a, dtype=np.float64) for a in src]
-    tgt = [np.asarray(a, dtype=np.float64) for a in tgt]
-    C = [(a.min() + a.max()) / 2.0 for a in src]
-    D = [(a.min() + a.max()) / 2.0 for a in tgt]
-    S = [max((a.max() - a.min()) / 2.0, 1e-10) for a in tgt]
+    dt = np.result_type(*[np.asarray(a).dtype for a in list(src) + list(tgt)])
+    dt = np.dtype(np.float32) if dt == np.float32 else np.dtype(np.float64)
+    t = dt.type
+    src = [np.asarray(a, dtype=dt) for a in src]
+    tgt = [np.asarray(a, dtype=dt) for a in tgt]
+    C = [(a.min() + a.max()) / t(2.0) for a in src]
+    D = [(a.min() + a.max()) / t(2.0) for a in tgt]
+    S = [max((a.max() - a.min()) / t(2.0), t(1e-10)) for a in tgt]
     nf = list(n_modes)
     h = [2.0 * np.pi / n for n in nf]
-    gam = [nf[d] / (2.0 * upsampfac * S[d]) for d in range(dim)]
+    gam = [t(nf[d]) / (t(2.0 * upsampfac) * S[d]) for d in range(dim)]
     xn = [premod((src[d] - C[d]) / gam[d]) for d in range(dim)]
-    phase_in = np.exp(1j * isign * sum(D[d] * src[d] for d in range(dim)))
+    phase_in = np.exp(1j * isign * sum(np.float64(D[d]) * src[d].astype(np.float64) for d in range(dim)))
     fw = spread(xn, c2 * phase_in[None, :], nf, kp)
-    s_resc = [h[d] * gam[d] * (tgt[d] - D[d]) for d in range(dim)]
+    s_resc = [(t(h[d]) * gam[d]) * (tgt[d] - D[d]) for d in range(dim)]
     sn = [premod(a) for a in s_resc]
     f = nufft_type2(sn, fw, eps=eps, isign=isign, upsampfac=upsampfac)
     phi = np.ones(tgt[0].shape[0])
     for d in range(dim):
-        phi = phi * kernel_ft_at_point(s_resc[d], kp.nspread, kp.beta, kp.c)
-    ph = np.exp(1j * isign * sum((tgt[d] - D[d]) * C[d] for d in range(dim)))
+        phi = phi * kernel_ft_at_point(s_resc[d].astype(np.float64), kp.nspread, kp.beta, kp.c)
+    ph = np.exp(1j * isign * sum((tgt[d].astype(np.float64) - np.float64(D[d])) * np.float64(C[d])
+                                 for d in range(dim)))
     f = f * (ph / phi)[None, :]
     return f[0] if c.ndim == 1 else f
 
@@ -547,6 +577,50 @@ def direct_type3(src, c, tgt, isign=1):
     c2 = (c[None, :] if c.ndim == 1 else c).astype(np.complex128)
     out = c2 @ np.exp(1j * isign * (X @ S.T))
     return out[0] if c.ndim == 1 else out
+
+
+def direct_type1_product(coords, c, mode_axes, isign=1, chunk=1 << 18):
+    """The direct sum of tests/conftest.py:154-175 at the product set of integer
+    modes mode_axes = (k1 values, k2 values[, k3 values]), evaluated separably:
+    exp(i isign k.x) = prod_d exp(i isign k_d x_d), so M points cost M * sum(len(k_d))
+    exponentials and one matrix product per chunk of points,
+    f[.., k2, k1] = sum_j (prod_{d>=2} E_d[j, k_d]) (c_j E_1[j, k1]).  Returns
+    (len(k_d), ..., len(k_1)) complex128 (slowest axis first, as the transforms)."""
+    dim = len(coords)
+    M = coords[0].shape[0]
+    ks = [np.asarray(k, dtype=np.float64) for k in mode_axes]
+    sizes = [k.size for k in ks]
+    out = np.zeros((int(np.prod(sizes[1:])), sizes[0]), dtype=np.complex128)
+    c1 = np.asarray(c).astype(np.complex128)
+
+    def expi(x, k):
+        th = isign * np.outer(np.asarray(x, dtype=np.float64), k)
+        return np.cos(th) + 1j * np.sin(th)
+
+    for a in range(0, M, chunk):
+        b = min(a + chunk, M)
+        A = expi(coords[0][a:b], ks[0]) * c1[a:b, None]  # (m, n1)
+        B = np.ones((b - a, 1), dtype=np.complex128)
+        for d in range(1, dim):  # axis d becomes the new slowest axis of B
+            B = (expi(coords[d][a:b], ks[d])[:, :, None] * B[:, None, :]).reshape(b - a, -1)
+        out += B.T @ A
+    return out.reshape(tuple(reversed(sizes)))
+
+
+def direct_type2_points(points, f, isign=-1):
+    """The direct sum of tests/conftest.py:178-198 at a few points (each of
+    `points` holds the d coordinates of the same rows), over every CMCL mode of
+    f (n_d, ..., n_1), contracted one axis at a time (x first)."""
+    dim = len(points)
+    n_modes = [f.shape[f.ndim - 1 - d] for d in range(dim)]
+    ks = mode_grid(n_modes)
+    X = [np.asarray(p, dtype=np.float64) for p in points]
+    E = [np.exp(1j * isign * np.outer(X[d], ks[d])) for d in range(dim)]  # (J, n_d)
+    G = np.tensordot(np.asarray(f, dtype=np.complex128), E[0].T, axes=([f.ndim - 1], [0]))  # (..., n2, J)
+    for d in range(1, dim):
+        # G: (n_{dim-1}.., n_d, J); contract n_d with E[d][j, :] row-wise
+        G = np.einsum("...kj,jk->...j", G, E[d])
+    return G
 
 
 def modes_as_flat(f: np.ndarray, dim: int):
