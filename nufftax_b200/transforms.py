@@ -21,9 +21,9 @@ JAX primitives of nufftax/transforms/primitives.py, with the same three rules:
     type 2: df = type-1 adjoint pipeline of G; dx from the ES-derivative
             interpolation of the forward fine grid;
     type 3: dc, dx, ds through type-3 transforms of weighted cotangents
-            (primitives.py:534-659);
-  forward mode (torch.func.jvp, torch.autograd.forward_ad; the JVP rules of
-    primitives.py:271-284, 443-465, 606-633): the tangent is the transform of
+            (primitives.py:358-497);
+  forward mode (torch.func.jvp, torch.autograd.forward_ad; the JVP rules
+    _jvp_{1,2,3}d{1,2,3} of primitives.py:88-473): the tangent is the transform of
     dc (df) plus k-weighted transforms for the coordinate tangents, all of them
     stacked along n_trans into ONE call, so they share one sort and one launch
     of each kernel;
@@ -152,7 +152,10 @@ def _bdim_front(t, bdim, B):
 
 
 # ---------------------------------------------------------------------------
-# Type 1
+# Kernel layer: library calls on plain device tensors.  Only the forward
+# methods of the autograd Functions below call these; their backward, jvp and
+# vmap rules use Function.apply and torch operations only, so that torch.func
+# transforms can unwrap the inputs level by level.
 # ---------------------------------------------------------------------------
 def _type1_forward(c2, n_modes, eps, isign, uf, coords):
     dim = len(coords)
@@ -164,6 +167,55 @@ def _type1_forward(c2, n_modes, eps, isign, uf, coords):
     return deconv_shuffle(fw, n_modes, kp)
 
 
+def _type1_coord_grad(c2, G, n_modes, eps, isign, uf_t, need_c, need_x, coords):
+    """(dc or None, [dx_d or None]) of f = type 1 (c2 at coords) for the mode
+    cotangent G: G deconvolved, zero-padded and transformed back onto the fine
+    grid, then one fused ES-derivative pass over the points."""
+    dim = len(coords)
+    kp = compute_kernel_params(eps, uf_t)
+    nf = tuple(compute_grid_size(n, uf_t, kp.nspread) for n in n_modes)
+    H = deconv_pad(G.contiguous(), nf, kp)
+    fft_inplace(H, dim, -_fft_sign_type1(isign))
+    ps = sort_cache.get(list(coords), nf, kp, prenorm=True)
+    return ps.spread_grad(c2.contiguous(), H, need_c, need_x)
+
+
+def _type2_grid(f2, n_modes, eps, isign, uf, dim):
+    kp = compute_kernel_params(eps, uf)
+    nf = tuple(compute_grid_size(n, uf, kp.nspread) for n in n_modes)
+    fw = deconv_pad(f2, nf, kp)
+    fft_inplace(fw, dim, _fft_sign_type2(isign))
+    return fw, nf, kp
+
+
+def _type2_forward(f2, eps, isign, uf, coords):
+    dim = len(coords)
+    n_modes = tuple(int(v) for v in reversed(f2.shape[1:]))
+    fw, nf, kp = _type2_grid(f2, n_modes, eps, isign, uf, dim)
+    return sort_cache.get(list(coords), nf, kp, prenorm=True).interp(fw)
+
+
+def _type2_coord_grad(f2, G, n_modes, eps, isign, uf, need_x, coords):
+    """[dx_d or None] of c = type 2 (f2 at coords) for the point cotangent G:
+    the forward fine grid again (deconvolve + FFT), then the ES-derivative
+    interpolation on it."""
+    dim = len(coords)
+    fw, nf, kp = _type2_grid(f2.contiguous(), n_modes, eps, isign, uf, dim)
+    return sort_cache.get(list(coords), nf, kp, prenorm=True).interp_grad(fw, G.contiguous(), need_x)
+
+
+def _split_stack(F, nt, first):
+    """Rows [0, nt) of a stacked call when `first` is set, and the offset of the next block."""
+    return (F[:nt], nt) if first else (None, 0)
+
+
+def _add(a, b):
+    return b if a is None else a + b
+
+
+# ---------------------------------------------------------------------------
+# Type 1
+# ---------------------------------------------------------------------------
 class _Type1(torch.autograd.Function):
     """f = type 1 (c2 at coords), c2: (n_trans, M) -> (n_trans, N_d..N_1)."""
 
@@ -182,24 +234,21 @@ class _Type1(torch.autograd.Function):
     def backward(ctx, G):
         c2, *coords = ctx.saved_tensors
         n_modes, eps, isign, uf, uf_t = ctx.meta
-        dim = len(coords)
         need_c = ctx.needs_input_grad[0]
-        need_x = list(ctx.needs_input_grad[6:])
-        kp = compute_kernel_params(eps, uf_t)
-        nf = tuple(compute_grid_size(n, uf_t, kp.nspread) for n in n_modes)
-        H = deconv_pad(G.contiguous(), nf, kp)
-        fft_inplace(H, dim, -_fft_sign_type1(isign))
-        ps = sort_cache.get(list(coords), nf, kp, prenorm=True)
-        dc, dxs = None, [None] * dim
+        need_x = tuple(ctx.needs_input_grad[6:])
         if any(need_x):
-            dc, dxs = ps.spread_grad(c2, H, need_c, need_x)
-        elif need_c:
-            dc = ps.interp(H)
+            dc, *dxs = _Type1CoordGrad.apply(c2, G, n_modes, eps, isign, uf_t, need_c, need_x, *coords)
+        else:
+            # transpose rule (_transpose_{1,2,3}d1, primitives.py:104, 191, 285):
+            # type 2 of G with the upsampling factors swapped, and the sign
+            # conjugated for torch's cotangent convention
+            dxs = [None] * len(coords)
+            dc = _Type2.apply(G.contiguous(), eps, -isign, uf_t, uf, *coords) if need_c else None
         return (dc, None, None, None, None, None, *dxs)
 
     @staticmethod
     def jvp(ctx, dc, _n, _e, _i, _u, _ut, *dxs):
-        # df = T1(dc) + sum_d (i isign k_d) T1(c dx_d)   (primitives.py:271-284, 443-465)
+        # df = T1(dc) + sum_d (i isign k_d) T1(c dx_d)   (_jvp_{1,2,3}d1, primitives.py:88, 170, 260)
         c2, *coords = ctx.saved_tensors
         n_modes, eps, isign, uf, uf_t = ctx.meta
         dim = len(coords)
@@ -207,35 +256,58 @@ class _Type1(torch.autograd.Function):
         parts = ([dc] if dc is not None else []) + [c2 * dx.to(c2.dtype)[None, :] for dx in dxs if dx is not None]
         if not parts:
             return None
-        F = _type1_forward(torch.cat(parts, 0).contiguous(), n_modes, eps, isign, uf, coords)
-        i = 0
-        out = None
-        if dc is not None:
-            out = F[:nt]
-            i = nt
+        F = _Type1.apply(torch.cat(parts, 0).contiguous(), n_modes, eps, isign, uf, uf_t, *coords)
+        out, i = _split_stack(F, nt, dc is not None)
         for d, dx in enumerate(dxs):
-            if dx is None:
-                continue
-            k = _modes_axis(n_modes[d], d, dim, F.device, F.real.dtype)
-            term = (1j * isign) * k * F[i:i + nt]
-            out = term if out is None else out + term
-            i += nt
+            if dx is not None:
+                k = _modes_axis(n_modes[d], d, dim, F.device, F.real.dtype)
+                out = _add(out, (1j * isign) * k * F[i:i + nt])
+                i += nt
         return out
 
     @staticmethod
     def vmap(info, in_dims, c2, n_modes, eps, isign, uf, uf_t, *coords):
         cdim, xdims = in_dims[0], in_dims[6:]
         B = info.batch_size
+        cb = _bdim_front(c2, cdim, B)
         if all(d is None for d in xdims):
             # shared points: the batch becomes part of n_trans (one call)
-            cb = _bdim_front(c2, cdim, B)
             nt = cb.shape[1]
             f = _Type1.apply(cb.reshape((B * nt,) + tuple(cb.shape[2:])), n_modes, eps, isign, uf, uf_t, *coords)
             return f.reshape((B, nt) + tuple(f.shape[1:])), 0
-        cb = _bdim_front(c2, cdim, B)
         xb = [_bdim_front(x, d, B) for x, d in zip(coords, xdims)]
         outs = [_Type1.apply(cb[b], n_modes, eps, isign, uf, uf_t, *[x[b] for x in xb]) for b in range(B)]
         return torch.stack(outs, 0), 0
+
+
+class _Type1CoordGrad(torch.autograd.Function):
+    """(dc, dx_1, .., dx_d) of a type 1 for the mode cotangent G (the fused
+    ES-derivative adjoint pass).  Not differentiable itself: second derivatives
+    with respect to the coordinates are not provided."""
+
+    @staticmethod
+    def forward(c2, G, n_modes, eps, isign, uf_t, need_c, need_x, *coords):
+        dc, dxs = _type1_coord_grad(c2, G, n_modes, eps, isign, uf_t, need_c, need_x, coords)
+        return (dc, *dxs)
+
+    @staticmethod
+    def setup_context(ctx, inputs, output):
+        pass
+
+    @staticmethod
+    def backward(ctx, *grads):
+        raise NotImplementedError("second derivatives with respect to the coordinates are not implemented")
+
+    @staticmethod
+    def vmap(info, in_dims, c2, G, n_modes, eps, isign, uf_t, need_c, need_x, *coords):
+        # the coordinate gradients sum over n_trans, so batch elements stay apart
+        B = info.batch_size
+        cb, Gb = _bdim_front(c2, in_dims[0], B), _bdim_front(G, in_dims[1], B)
+        xb = [_bdim_front(x, d, B) for x, d in zip(coords, in_dims[8:])]
+        outs = [_Type1CoordGrad.apply(cb[b], Gb[b], n_modes, eps, isign, uf_t, need_c, need_x,
+                                      *[x[b] for x in xb]) for b in range(B)]
+        res = tuple(None if outs[0][i] is None else torch.stack([o[i] for o in outs]) for i in range(len(outs[0])))
+        return res, tuple(None if r is None else 0 for r in res)
 
 
 def _type1(coords, c, n_modes: Sequence[int], eps, isign, upsampfac):
@@ -274,21 +346,6 @@ def nufft3d1(x, y, z, c, n_modes, eps: float = 1e-6, isign: int = 1, upsampfac=2
 # ---------------------------------------------------------------------------
 # Type 2
 # ---------------------------------------------------------------------------
-def _type2_grid(f2, n_modes, eps, isign, uf, dim):
-    kp = compute_kernel_params(eps, uf)
-    nf = tuple(compute_grid_size(n, uf, kp.nspread) for n in n_modes)
-    fw = deconv_pad(f2, nf, kp)
-    fft_inplace(fw, dim, _fft_sign_type2(isign))
-    return fw, nf, kp
-
-
-def _type2_forward(f2, eps, isign, uf, coords):
-    dim = len(coords)
-    n_modes = tuple(int(v) for v in reversed(f2.shape[1:]))
-    fw, nf, kp = _type2_grid(f2, n_modes, eps, isign, uf, dim)
-    return sort_cache.get(list(coords), nf, kp, prenorm=True).interp(fw)
-
-
 class _Type2(torch.autograd.Function):
     """c = type 2 (f2 at coords), f2: (n_trans, N_d..N_1) -> (n_trans, M)."""
 
@@ -307,29 +364,19 @@ class _Type2(torch.autograd.Function):
     def backward(ctx, G):
         f2, *coords = ctx.saved_tensors
         n_modes, eps, isign, uf, uf_t = ctx.meta
-        dim = len(coords)
-        need_f = ctx.needs_input_grad[0]
-        need_x = list(ctx.needs_input_grad[5:])
-        G = G.contiguous()
-        df = None
-        if need_f:
-            kp = compute_kernel_params(eps, uf_t)
-            nf = tuple(compute_grid_size(n, uf_t, kp.nspread) for n in n_modes)
-            ps_t = sort_cache.get(list(coords), nf, kp, prenorm=True)
-            gw = ps_t.spread(G)
-            fft_inplace(gw, dim, -_fft_sign_type2(isign))
-            df = deconv_shuffle(gw, n_modes, kp)
-        dxs = [None] * dim
-        if any(need_x):
-            # the forward fine grid again (deconvolve + FFT), then the
-            # ES-derivative interpolation on it
-            fw, nf, kp = _type2_grid(f2.contiguous(), n_modes, eps, isign, uf, dim)
-            dxs = sort_cache.get(list(coords), nf, kp, prenorm=True).interp_grad(fw, G, need_x)
+        need_x = tuple(ctx.needs_input_grad[5:])
+        # transpose rule (_transpose_{1,2,3}d2, primitives.py:145, 235, 334):
+        # type 1 of G with the upsampling factors swapped, and the sign
+        # conjugated for torch's cotangent convention
+        df = _Type1.apply(G.contiguous(), n_modes, eps, -isign, uf_t, uf, *coords) if ctx.needs_input_grad[0] \
+            else None
+        dxs = list(_Type2CoordGrad.apply(f2, G, n_modes, eps, isign, uf, need_x, *coords)) if any(need_x) \
+            else [None] * len(coords)
         return (df, None, None, None, None, *dxs)
 
     @staticmethod
     def jvp(ctx, df, _e, _i, _u, _ut, *dxs):
-        # dc = T2(df) + sum_d dx_d T2(i isign k_d f)   (primitives.py:211-231)
+        # dc = T2(df) + sum_d dx_d T2(i isign k_d f)   (_jvp_{1,2,3}d2, primitives.py:127, 212, 306)
         f2, *coords = ctx.saved_tensors
         n_modes, eps, isign, uf, uf_t = ctx.meta
         dim = len(coords)
@@ -340,18 +387,12 @@ class _Type2(torch.autograd.Function):
                 parts.append((1j * isign) * _modes_axis(n_modes[d], d, dim, f2.device, f2.real.dtype) * f2)
         if not parts:
             return None
-        C = _type2_forward(torch.cat(parts, 0).contiguous(), eps, isign, uf, coords)
-        i = 0
-        out = None
-        if df is not None:
-            out = C[:nt]
-            i = nt
+        C = _Type2.apply(torch.cat(parts, 0).contiguous(), eps, isign, uf, uf_t, *coords)
+        out, i = _split_stack(C, nt, df is not None)
         for dx in dxs:
-            if dx is None:
-                continue
-            term = dx.to(C.dtype)[None, :] * C[i:i + nt]
-            out = term if out is None else out + term
-            i += nt
+            if dx is not None:
+                out = _add(out, dx.to(C.dtype)[None, :] * C[i:i + nt])
+                i += nt
         return out
 
     @staticmethod
@@ -366,6 +407,33 @@ class _Type2(torch.autograd.Function):
         xb = [_bdim_front(x, d, B) for x, d in zip(coords, xdims)]
         outs = [_Type2.apply(fb[b], eps, isign, uf, uf_t, *[x[b] for x in xb]) for b in range(B)]
         return torch.stack(outs, 0), 0
+
+
+class _Type2CoordGrad(torch.autograd.Function):
+    """(dx_1, .., dx_d) of a type 2 for the point cotangent G (ES-derivative
+    interpolation of the forward fine grid).  Not differentiable itself."""
+
+    @staticmethod
+    def forward(f2, G, n_modes, eps, isign, uf, need_x, *coords):
+        return tuple(_type2_coord_grad(f2, G, n_modes, eps, isign, uf, need_x, coords))
+
+    @staticmethod
+    def setup_context(ctx, inputs, output):
+        pass
+
+    @staticmethod
+    def backward(ctx, *grads):
+        raise NotImplementedError("second derivatives with respect to the coordinates are not implemented")
+
+    @staticmethod
+    def vmap(info, in_dims, f2, G, n_modes, eps, isign, uf, need_x, *coords):
+        B = info.batch_size
+        fb, Gb = _bdim_front(f2, in_dims[0], B), _bdim_front(G, in_dims[1], B)
+        xb = [_bdim_front(x, d, B) for x, d in zip(coords, in_dims[7:])]
+        outs = [_Type2CoordGrad.apply(fb[b], Gb[b], n_modes, eps, isign, uf, need_x, *[x[b] for x in xb])
+                for b in range(B)]
+        res = tuple(None if outs[0][i] is None else torch.stack([o[i] for o in outs]) for i in range(len(outs[0])))
+        return res, tuple(None if r is None else 0 for r in res)
 
 
 def _type2(coords, f, eps, isign, upsampfac):
@@ -461,37 +529,42 @@ class _Type3(torch.autograd.Function):
 
     @staticmethod
     def backward(ctx, G):
+        # _transpose_{1,2,3}d3 (primitives.py:376, 422, 473) and the coordinate
+        # terms of the JVP rules, transposed: the conjugate transpose is a type 3 from the
+        # targets to the sources with -isign; the coordinate terms are weighted
+        # transforms.  Each direction is one stacked call.
         c2, *pts = ctx.saved_tensors
         nf, eps, isign, uf, dim = ctx.meta
-        src, tgt = pts[:dim], pts[dim:]
-        G = G.contiguous()
+        src, tgt = list(pts[:dim]), list(pts[dim:])
+        nt = c2.shape[0]
         need_c = ctx.needs_input_grad[0]
-        need = ctx.needs_input_grad[6:]
-        dc = None
-        if need_c:
-            # conjugate transpose: type 3 from targets to sources with -isign
-            dc = _type3_forward(list(tgt), G, list(src), nf, eps, -isign, uf)
-        grads = []
-        for d in range(dim):
-            if need[d]:
-                w = (-1j * isign) * tgt[d].to(G.dtype)[None, :] * G
-                T = _type3_forward(list(tgt), w.contiguous(), list(src), nf, eps, -isign, uf)
-                grads.append((c2.conj() * T).real.sum(0))
-            else:
-                grads.append(None)
-        for d in range(dim):
-            if need[dim + d]:
-                F = _type3_forward(list(src), (src[d].to(c2.dtype)[None, :] * c2).contiguous(), list(tgt), nf, eps,
-                                   isign, uf)
-                grads.append((G.conj() * (1j * isign) * F).real.sum(0))
-            else:
-                grads.append(None)
-        return (dc, None, None, None, None, None, *grads)
+        need_x = ctx.needs_input_grad[6:6 + dim]
+        need_s = ctx.needs_input_grad[6 + dim:]
+        G = G.contiguous()
+        dc, gx, gs = None, [None] * dim, [None] * dim
+        parts = ([G] if need_c else []) + [(-1j * isign) * tgt[d].to(G.dtype)[None, :] * G
+                                           for d in range(dim) if need_x[d]]
+        if parts:
+            T = _Type3.apply(torch.cat(parts, 0).contiguous(), nf, eps, -isign, uf, dim, *tgt, *src)
+            dc, i = _split_stack(T, nt, need_c)
+            for d in range(dim):
+                if need_x[d]:
+                    gx[d] = (c2.conj() * T[i:i + nt]).real.sum(0)
+                    i += nt
+        parts = [src[d].to(c2.dtype)[None, :] * c2 for d in range(dim) if need_s[d]]
+        if parts:
+            F = _Type3.apply(torch.cat(parts, 0).contiguous(), nf, eps, isign, uf, dim, *src, *tgt)
+            i = 0
+            for d in range(dim):
+                if need_s[d]:
+                    gs[d] = (G.conj() * (1j * isign) * F[i:i + nt]).real.sum(0)
+                    i += nt
+        return (dc, None, None, None, None, None, *gx, *gs)
 
     @staticmethod
     def jvp(ctx, dc, _nf, _e, _i, _u, _d, *dpts):
         # df = T3(dc) + sum_d (i isign s_d) T3(c dx_d) + sum_d (i isign ds_d) T3(x_d c)
-        # (primitives.py:606-633), all strengths stacked into one call
+        # (_jvp_{1,2,3}d3, primitives.py:358, 398, 443), all strengths stacked into one call
         c2, *pts = ctx.saved_tensors
         nf, eps, isign, uf, dim = ctx.meta
         src, tgt = pts[:dim], pts[dim:]
@@ -502,21 +575,15 @@ class _Type3(torch.autograd.Function):
         parts += [src[d].to(c2.dtype)[None, :] * c2 for d in range(dim) if dss[d] is not None]
         if not parts:
             return None
-        F = _type3_forward(list(src), torch.cat(parts, 0).contiguous(), list(tgt), nf, eps, isign, uf)
-        i = 0
-        out = None
-        if dc is not None:
-            out = F[:nt]
-            i = nt
+        F = _Type3.apply(torch.cat(parts, 0).contiguous(), nf, eps, isign, uf, dim, *pts)
+        out, i = _split_stack(F, nt, dc is not None)
         for d, dx in enumerate(dxs):
             if dx is not None:
-                term = (1j * isign) * tgt[d].to(F.dtype)[None, :] * F[i:i + nt]
-                out = term if out is None else out + term
+                out = _add(out, (1j * isign) * tgt[d].to(F.dtype)[None, :] * F[i:i + nt])
                 i += nt
         for d, ds in enumerate(dss):
             if ds is not None:
-                term = (1j * isign) * ds.to(F.dtype)[None, :] * F[i:i + nt]
-                out = term if out is None else out + term
+                out = _add(out, (1j * isign) * ds.to(F.dtype)[None, :] * F[i:i + nt])
                 i += nt
         return out
 
