@@ -16,11 +16,20 @@ reference's result depends on it bit-for-bit:
 * accumulations (segment_sum / gather-sum), the FFT and deconvolution run in
   float64 (the oracle is at least as accurate as the reference in float32).
 
-Parity status: pinned to the reference's own test oracles, not to an execution of
-the reference (JAX is not installable here): the direct-DFT oracles of
-``tests/conftest.py:154-198`` and ``tests/test_nufft3.py:26-72``, the known answers of
-``tests/test_edge_cases.py``, the adjoint identity of ``tests/test_spread.py:300-347``
-and the kernel-parameter table computed from ``nufftax/core/kernel.py:165-206``.
+Parity status: pinned to outputs of the reference's own source.  jax is not
+installable here, so ``tests/golden/make_reference_golden.py`` runs nufftax's
+pure-JAX modules unmodified on NumPy through ``tests/golden/jax_numpy_shim.py``
+(a stand-in for the jax API subset they use, in the reference tests' x64
+configuration) and stores seeded inputs with the reference's outputs in
+``tests/golden/ref_*.npz``; ``tests/test_reference_golden.py`` holds this module
+to them: the fold and pre-normalisation bit for bit, complex128 transforms, core
+spread / interp and custom_vjp backward rules to 1e-12, complex64 within 2 eps
+(the reference accumulates complex64 in float32).  The stand-in does not
+reproduce XLA's fusion or scatter-add order, so the pin is to float rounding.
+Also checked: the direct-DFT oracles of ``tests/conftest.py:154-198`` and
+``tests/test_nufft3.py:26-72``, the known answers of ``tests/test_edge_cases.py``,
+the adjoint identity of ``tests/test_spread.py:300-347`` and the kernel-parameter
+table computed from ``nufftax/core/kernel.py:165-206``.
 """
 
 from __future__ import annotations
