@@ -253,6 +253,31 @@ int nfx_batch_deconv(int precision, int pad, const void* dev_table, int nprob, i
  *   e^{i isign sum_d (s_d - D_d) C_d} / prod_d phihat(h_d gamma_d (s_d - D_d))
  *   (nufft3.py:176-213, 390-394).  nf[d] is the type-3 grid per axis.
  * nfx_t3_finish: out[t][k] *= factor[k]. */
+/* ---- type 3 in one call ------------------------------------------------------
+ * The whole of nufftax/transforms/nufft3.py:216-515 with its pre- and
+ * post-processing fused into the passes: the source sort applies the rescaling
+ * x' = mod((x - C)/gamma + pi, 2 pi) - pi on the fly and stores each point's
+ * pre-phase e^{i isign sum_d D_d x_d}, which the spread multiplies into the
+ * strength; the inner type 2 (deconvolve + zero-pad of the fine grid as modes,
+ * FFT) follows; the target sort applies s' = (h gamma)(s - D) and stores
+ * each target's factor e^{i isign sum_d (s_d - D_d) C_d} / prod_d phihat(s'_d),
+ * which the interpolation multiplies into the value it writes.  The scalars
+ * are computed on the device in the working precision (no host round trip).
+ * opts: precision, dim, kernel (nspread, beta, kc) and nf = the type-3 grid
+ * per axis (compute_type3_grid_size*); tile / max_subproblem apply to the
+ * source sort; prenorm is ignored.  nf_inner[d] = the inner type 2's grid
+ * (compute_grid_size(nf[d], upsampfac, nspread)); fac1..fac3 its
+ * deconvolution factors for nf[d] modes on nf_inner[d] (as nfx_deconv_pad).
+ * src / tgt: dim device arrays of M sources and K targets; c: n_trans x M;
+ * out: n_trans x K.  The workspace (nfx_nufft3_workspace_bytes) holds
+ * everything, the FFT's work area included, so the call can be captured in a
+ * CUDA graph.  M >= 1. */
+int nfx_nufft3_workspace_bytes(const nfx_opts* opts, const int nf_inner[3], int64_t M, int64_t K, int n_trans,
+                               size_t* bytes);
+int nfx_nufft3(const nfx_opts* opts, const int nf_inner[3], double upsampfac, int isign, const void* const* src,
+               int64_t M, const void* c, int n_trans, const void* const* tgt, int64_t K, const void* fac1,
+               const void* fac2, const void* fac3, void* out, void* workspace, size_t workspace_bytes, void* stream);
+
 size_t nfx_t3_params_bytes(void);
 int nfx_t3_prepare(int precision, int dim, const int nf[3], int nspread, double beta, double kc, double upsampfac,
                    int isign, const void* const* src, int64_t M, const void* c, int n_trans, const void* const* tgt,

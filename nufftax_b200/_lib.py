@@ -116,6 +116,10 @@ _SIGNATURES = {
                                  POINTER(c_void_p), POINTER(c_void_p), c_int, _vp, c_size_t, POINTER(c_int64), _vp],
                                 c_int),
     "nfx_batch_deconv": ([c_int, c_int, _vp, c_int, c_int64, _vp], c_int),
+    "nfx_nufft3_workspace_bytes": ([POINTER(NfxOpts), POINTER(c_int), c_int64, c_int64, c_int, POINTER(c_size_t)],
+                                   c_int),
+    "nfx_nufft3": ([POINTER(NfxOpts), POINTER(c_int), c_double, c_int, POINTER(c_void_p), c_int64, _vp, c_int,
+                    POINTER(c_void_p), c_int64, _vp, _vp, _vp, _vp, _vp, c_size_t, _vp], c_int),
     "nfx_t3_params_bytes": ([], c_size_t),
     "nfx_t3_scratch_bytes": ([c_int, c_int64, c_int64], c_size_t),
     "nfx_t3_prepare": ([c_int, c_int, POINTER(c_int), c_int, c_double, c_double, c_double, c_int, POINTER(c_void_p),

@@ -183,6 +183,10 @@ static void fill_geom(const nfx_opts* o, Geom& g) {
   g.pitch = choose_pitch(g.pad[0], g.pad[1], o->nspread, o->dim);
   g.nbins = g.nb[0] * g.nb[1] * g.nb[2];
   g.prenorm = o->prenorm;
+  g.t3_mode = 0;
+  g.t3_isign = 0;
+  g.t3_beta = g.t3_kc = 0.0;
+  g.t3 = nullptr;
 }
 
 static int validate_opts(const nfx_opts* o) {
@@ -339,6 +343,7 @@ static void make_layout(const nfx_opts& o, const Geom& g, int64_t M, SortLayout&
   L.off_sub_start = take((size_t)L.max_subs * 4);
   L.off_nsub = take(4);
   for (int d = 0; d < 3; ++d) L.off_coord[d] = d < o.dim ? take((size_t)M * real_bytes(o.precision)) : 0;
+  L.off_extra = g.t3_mode != 0 ? take((size_t)M * 2 * real_bytes(o.precision)) : 0;
   L.total = off;
 }
 
@@ -364,6 +369,7 @@ static SortPtrs carve(const SortLayout& L, void* ws) {
   P.sub_start = (int*)(b + L.off_sub_start);
   P.nsub = (int*)(b + L.off_nsub);
   for (int d = 0; d < 3; ++d) P.coord[d] = L.off_coord[d] != 0 ? (void*)(b + L.off_coord[d]) : nullptr;
+  P.extra = L.off_extra != 0 ? (void*)(b + L.off_extra) : nullptr;
   return P;
 }
 
@@ -371,6 +377,7 @@ static SortView view(const SortLayout& L, const void* ws) {
   SortPtrs P = carve(L, const_cast<void*>(ws));
   SortView v;
   for (int d = 0; d < 3; ++d) v.coord[d] = P.coord[d];
+  v.extra = P.extra;
   v.perm = P.perm;
   v.bin_start = P.bin_start;
   v.sub_bin = P.sub_bin;
@@ -580,6 +587,109 @@ static size_t batch_item_bytes(int precision) {
 }
 
 static size_t batch_prefix_offset(int precision, int n) { return align256(batch_item_bytes(precision) * n); }
+
+// Workspace of one fused type 3: the type-3 scalars and their min / max
+// scratch, the source sort (type-3 mode 1: rescale + pre-phase per point), the
+// target sort (mode 2: rescale + output factor per point), the fine grid of the
+// spread, the inner type 2's fine grid and the cuFFT work area of its FFT.
+struct Nufft3Layout {
+  Prepared src, tgt;
+  size_t off_params, off_scratch, off_src, off_tgt, off_fw, off_fw2, off_fft, fft_bytes, total;
+  int64_t fw_cells, fw2_cells;
+};
+
+static int nufft3_layout(const nfx_opts* opts, const int nf_inner[3], int64_t M, int64_t K, int n_trans,
+                         Nufft3Layout& L3) {
+  if (opts == nullptr || nf_inner == nullptr || n_trans < 1 || M < 0 || K < 0 || M > (int64_t)INT32_MAX - 1 ||
+      K > (int64_t)INT32_MAX - 1) {
+    set_error("nfx_nufft3: invalid arguments");
+    return NFX_ERR_INVALID;
+  }
+  nfx_opts os = *opts;
+  os.prenorm = 0;
+  int st = resolve_opts(&os, L3.src.o);
+  if (st != NFX_OK) return st;
+  nfx_opts ot = *opts;
+  for (int d = 0; d < 3; ++d) {
+    ot.nf[d] = d < opts->dim ? nf_inner[d] : 1;
+    ot.tile[d] = 0;
+  }
+  ot.prenorm = 1;
+  ot.max_subproblem = 0;
+  st = resolve_opts(&ot, L3.tgt.o);
+  if (st != NFX_OK) return st;
+  fill_geom(&L3.src.o, L3.src.g);
+  fill_geom(&L3.tgt.o, L3.tgt.g);
+  L3.src.g.t3_mode = 1;
+  L3.tgt.g.t3_mode = 2;
+  make_layout(L3.src.o, L3.src.g, M, L3.src.L);
+  make_layout(L3.tgt.o, L3.tgt.g, K, L3.tgt.L);
+  if (!key_fits(L3.src.L) || !key_fits(L3.tgt.L)) return NFX_ERR_UNSUPPORTED;
+  const size_t cb = 2 * real_bytes(opts->precision);
+  L3.fw_cells = grid_cells(L3.src.g);
+  L3.fw2_cells = grid_cells(L3.tgt.g);
+  st = nfx_fft_work_bytes(opts->precision, opts->dim, L3.tgt.o.nf, n_trans, &L3.fft_bytes);
+  if (st != NFX_OK) return st;
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    size_t at = off;
+    off += align256(bytes);
+    return at;
+  };
+  L3.off_params = take(sizeof(T3Params));
+  L3.off_scratch = take(t3_scratch_bytes());
+  L3.off_src = take(L3.src.L.total);
+  L3.off_tgt = take(L3.tgt.L.total);
+  L3.off_fw = take((size_t)L3.fw_cells * n_trans * cb);
+  L3.off_fw2 = take((size_t)L3.fw2_cells * n_trans * cb);
+  L3.off_fft = take(L3.fft_bytes);
+  L3.total = off;
+  return NFX_OK;
+}
+
+template <typename T>
+static int nufft3_run(Nufft3Layout& L3, double upsampfac, int isign, const void* const* src, int64_t M,
+                      const void* c, int n_trans, const void* const* tgt, int64_t K, const void* fac1,
+                      const void* fac2, const void* fac3, void* out, char* ws, cudaStream_t st) {
+  const int dim = L3.src.o.dim;
+  const int ns = L3.src.o.nspread;
+  T3Params* params = (T3Params*)(ws + L3.off_params);
+  cudaError_t e = launch_t3_params<T>(dim, L3.src.o.nf, upsampfac, src, M, tgt, K, params, ws + L3.off_scratch, st);
+  if (e != cudaSuccess) return cuda_fail(e, "nfx_nufft3 set-up");
+  for (Prepared* P : {&L3.src, &L3.tgt}) {
+    P->g.t3 = params;
+    P->g.t3_isign = isign;
+    P->g.t3_beta = P->o.beta;
+    P->g.t3_kc = P->o.kc;
+  }
+  const void* s3[3] = {nullptr, nullptr, nullptr};
+  const void* t3[3] = {nullptr, nullptr, nullptr};
+  for (int d = 0; d < dim; ++d) {
+    s3[d] = src[d];
+    t3[d] = tgt[d];
+  }
+  // spread of the pre-phased strengths at the rescaled sources (nufft3.py:271-283)
+  char* src_ws = ws + L3.off_src;
+  e = launch_sort<T>(L3.src.L, L3.src.g, ns, s3[0], s3[1], s3[2], M, carve(L3.src.L, src_ws), st);
+  if (e != cudaSuccess) return cuda_fail(e, "nfx_nufft3 source sort");
+  void* fw = ws + L3.off_fw;
+  e = cudaMemsetAsync(fw, 0, (size_t)L3.fw_cells * n_trans * 2 * sizeof(T), st);
+  if (e == cudaSuccess) e = spread_dim<T>(L3.src, nullptr, nullptr, nullptr, M, c, n_trans, fw, src_ws, st);
+  if (e != cudaSuccess) return cuda_fail(e, "nfx_nufft3 spread");
+  // inner type 2: the fine grid as modes, deconvolved and zero-padded, FFT
+  // (nufft3.py:287-293, 381-387)
+  void* fw2 = ws + L3.off_fw2;
+  int stt = nfx_deconv_pad(L3.src.o.precision, dim, L3.tgt.o.nf, L3.src.o.nf, fac1, fac2, fac3, fw, fw2, n_trans, st);
+  if (stt != NFX_OK) return stt;
+  stt = nfx_fft_ws(L3.src.o.precision, dim, L3.tgt.o.nf, n_trans, fw2, isign < 0 ? -1 : 1,
+                   L3.fft_bytes ? ws + L3.off_fft : nullptr, L3.fft_bytes, st);
+  if (stt != NFX_OK) return stt;
+  // interpolation at the rescaled targets, times phase / phihat (nufft3.py:293-299, 387-394)
+  char* tgt_ws = ws + L3.off_tgt;
+  e = launch_sort<T>(L3.tgt.L, L3.tgt.g, ns, t3[0], t3[1], t3[2], K, carve(L3.tgt.L, tgt_ws), st);
+  if (e == cudaSuccess) e = interp_dim<T>(L3.tgt, nullptr, nullptr, nullptr, K, fw2, n_trans, out, tgt_ws, st);
+  return e == cudaSuccess ? NFX_OK : cuda_fail(e, "nfx_nufft3 interp");
+}
 
 }  // namespace nfx
 
@@ -949,6 +1059,48 @@ int nfx_batch_launch(const nfx_opts* common, int spread, const void* dev_table, 
                            : dispatch_batch<double, 3>(ns, sp, dev_table, nprob, prefix, info->max_subs, info->smem_bytes, s);
   }
   return e == cudaSuccess ? NFX_OK : cuda_fail(e, "nfx_batch_launch");
+}
+
+int nfx_nufft3_workspace_bytes(const nfx_opts* opts, const int nf_inner[3], int64_t M, int64_t K, int n_trans,
+                               size_t* bytes) {
+  if (bytes == nullptr) {
+    set_error("nfx_nufft3_workspace_bytes: bytes is NULL");
+    return NFX_ERR_INVALID;
+  }
+  Nufft3Layout L3;
+  int st = nufft3_layout(opts, nf_inner, M, K, n_trans, L3);
+  if (st == NFX_OK) *bytes = L3.total;
+  return st;
+}
+
+int nfx_nufft3(const nfx_opts* opts, const int nf_inner[3], double upsampfac, int isign, const void* const* src,
+               int64_t M, const void* c, int n_trans, const void* const* tgt, int64_t K, const void* fac1,
+               const void* fac2, const void* fac3, void* out, void* workspace, size_t workspace_bytes, void* stream) {
+  Nufft3Layout L3;
+  int st = nufft3_layout(opts, nf_inner, M, K, n_trans, L3);
+  if (st != NFX_OK) return st;
+  const int dim = opts->dim;
+  if (M < 1 || src == nullptr || tgt == nullptr || c == nullptr || (K > 0 && out == nullptr) || fac1 == nullptr ||
+      (dim >= 2 && fac2 == nullptr) || (dim >= 3 && fac3 == nullptr)) {
+    set_error("nfx_nufft3: need M >= 1 and non-NULL sources, targets, strengths, output and factors");
+    return NFX_ERR_INVALID;
+  }
+  for (int d = 0; d < dim; ++d)
+    if (src[d] == nullptr || (K > 0 && tgt[d] == nullptr) || opts->nf[d] < 2) {
+      set_error("nfx_nufft3: NULL coordinate axis or type-3 grid below 2");
+      return NFX_ERR_INVALID;
+    }
+  if (workspace == nullptr || workspace_bytes < L3.total) {
+    set_error("nfx_nufft3: workspace too small: need " + std::to_string(L3.total) + " bytes");
+    return NFX_ERR_WORKSPACE;
+  }
+  if (K == 0) return NFX_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  return opts->precision == NFX_F32
+             ? nufft3_run<float>(L3, upsampfac, isign, src, M, c, n_trans, tgt, K, fac1, fac2, fac3, out,
+                                 (char*)workspace, s)
+             : nufft3_run<double>(L3, upsampfac, isign, src, M, c, n_trans, tgt, K, fac1, fac2, fac3, out,
+                                  (char*)workspace, s);
 }
 
 size_t nfx_batch_deconv_table_bytes(int precision, int nprob) {

@@ -191,6 +191,14 @@ __device__ __forceinline__ int fast_div(int n, FastDiv f) {
   return f.shr < 0 ? n : (int)(__umulhi((unsigned)n, f.mul) >> f.shr);
 }
 
+// Type-3 scalars per axis (nufftax/transforms/nufft3.py:258-268, 354-362),
+// computed on the device: source centre C, target centre D, target half-width
+// S, scale gamma = nf / (2 upsampfac S) and h = 2 pi / nf.  Values of the
+// working type stored as doubles.
+struct T3Params {
+  double C[3], D[3], S[3], gamma[3], h[3];
+};
+
 // Grid geometry shared by the sort, spread and interp kernels (plain values).
 struct Geom {
   int dim;
@@ -202,6 +210,34 @@ struct Geom {
   int nbins;
   int prenorm;
   FastDiv tdiv[3];  // division by tile[d]
+  // Type 3 fused into the sort (0: off).  1: the points are type-3 sources,
+  // rescaled as x' = mod((x - C) / gamma + pi, 2 pi) - pi before the fold, and
+  // the sort writes each point's pre-phase e^{i isign sum_d D_d x_d};
+  // 2: type-3 targets, s' = (h gamma)(s - D) folded into [-pi, pi), and the
+  // sort writes each point's output factor e^{i isign sum_d (s_d - D_d) C_d} /
+  // prod_d phihat(s'_d).  t3 points at the device T3Params.
+  int t3_mode;
+  int t3_isign;
+  double t3_beta, t3_kc;
+  const T3Params* t3;
 };
+
+// The type-3 rescaling of one coordinate, in the working type and in the
+// reference's order (nufft3.py:271-272, 287-288, 365-366, 381-384).
+template <typename T>
+__device__ __forceinline__ T t3_rescaled(T x, int d, const Geom& g) {
+  const T3Params* p = g.t3;
+  if (g.t3_mode == 1) return rn_sub(x, (T)p->C[d]) / (T)p->gamma[d];
+  return rn_mul(rn_mul((T)p->h[d], (T)p->gamma[d]), rn_sub(x, (T)p->D[d]));
+}
+
+// Folded grid coordinate of axis d of a point (the value every pass and the
+// bin keys use): the type-3 rescaling and its pre-normalisation when enabled,
+// then the transforms' pre-normalisation (prenorm) and fold_rescale.
+template <typename T>
+__device__ __forceinline__ T point_fold(T x, int d, const Geom& g) {
+  if (g.t3_mode != 0) x = premod(t3_rescaled(x, d, g));
+  return scaled_coord(x, g.nf[d], g.prenorm);
+}
 
 }  // namespace nfx

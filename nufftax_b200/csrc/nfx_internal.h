@@ -27,6 +27,7 @@ struct SortLayout {
   size_t off_keys, off_keys_tmp, off_vals_tmp, off_keys_sorted, off_perm, off_counts, off_totals, off_bin_start,
       off_sub_bin, off_sub_start, off_nsub;
   size_t off_coord[3];  // folded coordinates in sorted order, one array per axis (0 = unused axis)
+  size_t off_extra;     // type 3 only: one complex factor per sorted point (0 = none)
   size_t total;
 };
 
@@ -43,6 +44,7 @@ struct SortPtrs {
   int* sub_start;
   int* nsub;
   void* coord[3];  // sorted folded coordinates (working precision), nullptr for unused axes
+  void* extra;     // type 3: complex factor per sorted point, else nullptr
 };
 
 // Pointers a spread / interp / gradient launch needs from a finished sort.
@@ -51,6 +53,10 @@ struct SortPtrs {
 // passes read coordinates in sorted order instead of gathering them.
 struct SortView {
   const void* coord[3];
+  // Type-3 sorts only (else nullptr): a complex factor per sorted point that
+  // the spread multiplies into the strength (sources: the pre-phase) or the
+  // interpolation into the value it writes (targets: phase / phihat).
+  const void* extra;
   const int* perm;
   const int* bin_start;
   const int* sub_bin;
@@ -68,6 +74,13 @@ cudaError_t bin_keys_of(const SortLayout& L, const int* K, int* out, cudaStream_
 template <typename T>
 cudaError_t launch_sort(const SortLayout& L, const Geom& g, int ns, const void* x, const void* y, const void* z,
                         int64_t M, const SortPtrs& P, cudaStream_t st);
+
+// Type-3 set-up on the device: min / max of sources and targets per axis and
+// the T3Params from them (scratch of t3_scratch_bytes()).
+size_t t3_scratch_bytes();
+template <typename T>
+cudaError_t launch_t3_params(int dim, const int nf[3], double upsampfac, const void* const* src, int64_t M,
+                             const void* const* tgt, int64_t K, T3Params* params, void* scratch, cudaStream_t st);
 
 // Spread: fw (n_trans x prod nf, complex) must be zeroed by the caller.
 template <typename T>

@@ -57,7 +57,7 @@ __device__ __forceinline__ void cell_keys(const T (&c)[DIM], const Geom& g, int 
   int kb = 0, kc = 0, mb = 1, mc = 1;
 #pragma unroll
   for (int d = 0; d < DIM; ++d) {
-    const T xs = scaled_coord(c[d], g.nf[d], g.prenorm);
+    const T xs = point_fold(c[d], d, g);
     const int i0w = wrap_index(ceil_to_int(rn_sub(xs, (T)ns_half)), g.nf[d]);
     const int bq = fast_div(i0w, g.tdiv[d]);
     kb += bq * mb;
@@ -446,6 +446,42 @@ __global__ void k_subproblems(const int* __restrict__ bin_start, int nbins, int 
   }
 }
 
+// ---- (3a) folded coordinates in sorted order ----------------------------------
+// coord_d[k] = fold(x_d[perm[k]]) for every axis: the same float operations as
+// the keys (so the spread / interp passes see exactly the coordinates the sort
+// binned), written once in sorted order.  Each thread takes 4 consecutive
+// positions: one vector load of the permutation, all gathers in flight together,
+// one vector store per axis.  Type-3 sorts also write extra[k], the point's
+// complex factor (Geom::t3_mode): sources the pre-phase e^{i isign sum D_d x_d}
+// (nufft3.py:275-280, 368-372), targets e^{i isign sum (s_d - D_d) C_d} /
+// prod_d phihat(s'_d) with phihat by the reference's trapezoid on
+// [-ns/2, ns/2] (nufft3.py:176-213, 390-394), in double before one rounding.
+constexpr int kMaxQuad = 32;
+
+template <typename T>
+__device__ __forceinline__ cplx_t<T> t3_factor(const T (&xr)[3], int dim, const Geom& g, int nq, double dz,
+                                               const double* __restrict__ s_qw) {
+  const T3Params* p = g.t3;
+  double phase = 0.0, phi_prod = 1.0;
+  for (int d = 0; d < dim; ++d) {
+    if (g.t3_mode == 1) {
+      phase += p->D[d] * (double)xr[d];
+    } else {
+      const double sr = (double)t3_rescaled(xr[d], d, g);
+      double acc = 0.0;
+      for (int q = 0; q < nq; ++q) acc += s_qw[q] * cos(sr * (-0.5 * dz * (nq - 1) + q * dz));
+      phi_prod *= acc;
+      phase += ((double)xr[d] - p->D[d]) * p->C[d];
+    }
+  }
+  double sn, cs;
+  sincos(phase * (double)g.t3_isign, &sn, &cs);
+  cplx_t<T> f;
+  f.x = (T)(cs / phi_prod);
+  f.y = (T)(sn / phi_prod);
+  return f;
+}
+
 __device__ __forceinline__ void store_quad(float* o, const float (&r)[4]) {
   *reinterpret_cast<float4*>(o) = make_float4(r[0], r[1], r[2], r[3]);
 }
@@ -454,21 +490,29 @@ __device__ __forceinline__ void store_quad(double* o, const double (&r)[4]) {
   reinterpret_cast<double2*>(o)[1] = make_double2(r[2], r[3]);
 }
 
-// ---- (3a) folded coordinates in sorted order ----------------------------------
-// coord_d[k] = fold(x_d[perm[k]]) for every axis: the same float operations as
-// the keys (so the spread / interp passes see exactly the coordinates the sort
-// binned), written once in sorted order.  Each thread takes 4 consecutive
-// positions: one vector load of the permutation, all gathers in flight together,
-// one vector store per axis.
 template <typename T, int DIM>
 __global__ void __launch_bounds__(256) k_sorted_coords(const T* __restrict__ x, const T* __restrict__ y,
                                                        const T* __restrict__ z, const int* __restrict__ perm, int M,
-                                                       Geom g, T* __restrict__ o0, T* __restrict__ o1,
-                                                       T* __restrict__ o2) {
+                                                       Geom g, int nspread, T* __restrict__ o0, T* __restrict__ o1,
+                                                       T* __restrict__ o2, cplx_t<T>* __restrict__ extra) {
   const T* cs[3] = {x, y, z};
   T* os[3] = {o0, o1, o2};
-  const int nq = (M + 3) / 4;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nq; t += gridDim.x * blockDim.x) {
+  // trapezoid nodes and weights phi(z_q) w_q of the type-3 targets' phihat
+  __shared__ double s_qw[kMaxQuad];
+  const double j2 = nspread / 2.0;
+  const int nq = min(max((int)(4 + 3.0 * j2), 20), kMaxQuad);
+  const double dz = 2.0 * j2 / (nq - 1);
+  if (g.t3_mode == 2) {
+    for (int q = threadIdx.x; q < nq; q += blockDim.x) {
+      const double zq = -j2 + q * dz;
+      const double arg = 1.0 - g.t3_kc * zq * zq;
+      const double phi = arg >= 0.0 ? exp(g.t3_beta * (sqrt(arg > 0.0 ? arg : 0.0) - 1.0)) : 0.0;
+      s_qw[q] = phi * ((q == 0 || q == nq - 1) ? dz / 2 : dz);
+    }
+    __syncthreads();
+  }
+  const int nquad = (M + 3) / 4;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nquad; t += gridDim.x * blockDim.x) {
     const int i0 = 4 * t;
     int p[4];
     if (i0 + 3 < M) {
@@ -490,13 +534,23 @@ __global__ void __launch_bounds__(256) k_sorted_coords(const T* __restrict__ x, 
     for (int d = 0; d < DIM; ++d) {
       T r[4];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) r[j] = scaled_coord(v[d][j], g.nf[d], g.prenorm);
+      for (int j = 0; j < 4; ++j) r[j] = point_fold(v[d][j], d, g);
       if (i0 + 3 < M) {
         store_quad(os[d] + i0, r);  // 16-byte aligned: 256-aligned arrays, i0 % 4 == 0
       } else {
 #pragma unroll
         for (int j = 0; j < 4; ++j)
           if (p[j] >= 0) os[d][i0 + j] = r[j];
+      }
+    }
+    if (g.t3_mode != 0) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        if (p[j] < 0) continue;
+        T xr[3] = {(T)0, (T)0, (T)0};
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) xr[d] = v[d][j];
+        extra[i0 + j] = t3_factor<T>(xr, DIM, g, nq, dz, s_qw);
       }
     }
   }
@@ -569,8 +623,8 @@ cudaError_t launch_sort(const SortLayout& L, const Geom& g, int ns, const void* 
   const int bgrid = (int)std::max<int64_t>(1, std::min<int64_t>((M / 4 + 256) / 256, (int64_t)num_sms() * 8));
   if (M > 0) {
     auto sc = g.dim == 1 ? k_sorted_coords<T, 1> : (g.dim == 2 ? k_sorted_coords<T, 2> : k_sorted_coords<T, 3>);
-    sc<<<bgrid, 256, 0, st>>>((const T*)x, (const T*)y, (const T*)z, P.perm, (int)M, g, (T*)P.coord[0],
-                              (T*)P.coord[1], (T*)P.coord[2]);
+    sc<<<bgrid, 256, 0, st>>>((const T*)x, (const T*)y, (const T*)z, P.perm, (int)M, g, ns, (T*)P.coord[0],
+                              (T*)P.coord[1], (T*)P.coord[2], (cplx_t<T>*)P.extra);
   }
   k_bin_bounds<<<bgrid, 256, 0, st>>>(P.keys_sorted, (int)M, L.cbits, g.nbins, P.bin_start);
   const int max_subs = (int)std::min<int64_t>(L.max_subs, INT32_MAX);

@@ -98,6 +98,21 @@ __device__ __forceinline__ T sorted_coord(const PointArgs<T>& a, int d, int k) {
   return a.sc[d][k];
 }
 
+template <typename T>
+__device__ __forceinline__ cplx_t<T> cmul(cplx_t<T> u, cplx_t<T> v) {
+  cplx_t<T> r;
+  r.x = u.x * v.x - u.y * v.y;
+  r.y = u.x * v.y + u.y * v.x;
+  return r;
+}
+
+// Type-3 sorts carry a complex factor per sorted point (SortView::extra): the
+// spread multiplies it into the strength, the interpolation into its result.
+template <typename T>
+__device__ __forceinline__ cplx_t<T> with_extra(const PointArgs<T>& a, int k, cplx_t<T> v) {
+  return a.s.extra != nullptr ? cmul<T>(v, reinterpret_cast<const cplx_t<T>*>(a.s.extra)[k]) : v;
+}
+
 // ---------------------------------------------------------------------------
 // Spread
 // ---------------------------------------------------------------------------
@@ -410,6 +425,7 @@ __device__ __forceinline__ void spread_subproblem_runs(const PointArgs<T>& a, co
       if (valid) {
         T w[DIM][NS];
         const bool inside = footprint<T, DIM, NS>(a, xv, o, row, plane, off, w);
+        cv = with_extra(a, kb + lane, cv);
         if (!inside) {
           cv.x = cv.y = (T)0;
           off = 0;
@@ -506,7 +522,7 @@ __device__ __forceinline__ void spread_subproblem_cells(const PointArgs<T>& a, c
         for (int d = 0; d < DIM; ++d)
 #pragma unroll
           for (int q = 0; q < NS; ++q) s_w[(d * NS + q) * SW + slot] = w[d][q];
-        const CT cv = c[(int64_t)t * a.M + p];
+        const CT cv = with_extra(a, k, c[(int64_t)t * a.M + p]);
         s_off[slot] = inside ? off : 0;
         s_cr[slot] = inside ? cv.x : (T)0;
         s_ci[slot] = inside ? cv.y : (T)0;
@@ -654,7 +670,7 @@ __device__ __forceinline__ void spread_subproblem_owner(const PointArgs<T>& a, c
         int off;
         T w[3][NS];
         const bool inside = footprint<T, 3, NS>(a, xv, o, row, plane, off, w);
-        CT cv = c[(int64_t)t * a.M + p];
+        CT cv = with_extra(a, k, c[(int64_t)t * a.M + p]);
         if (!inside) {
           cv.x = cv.y = (T)0;
           off = 0;
@@ -953,7 +969,7 @@ __device__ __forceinline__ void interp3_group(const PointArgs<T>& a, const cplx_
           CT r;
           r.x = sr;
           r.y = si;
-          cout[(int64_t)t * a.M + pt.p] = r;
+          cout[(int64_t)t * a.M + pt.p] = with_extra(a, kb + j, r);
         }
       }
     }
@@ -1057,7 +1073,7 @@ __device__ __forceinline__ void interp_subproblem(const PointArgs<T>& a, const c
         CT r;
         r.x = ar;
         r.y = ai;
-        cout[(int64_t)t * a.M + p] = r;
+        cout[(int64_t)t * a.M + p] = with_extra(a, k, r);
       }
     }
   }

@@ -15,10 +15,6 @@
 
 namespace nfx {
 
-struct T3Params {
-  double C[3], D[3], S[3], gamma[3], h[3];
-};
-
 constexpr int kT3Blocks = 256;
 
 template <typename T>
@@ -175,18 +171,33 @@ static unsigned ew_grid(int64_t n) {
   return (unsigned)(want < cap ? (want > 0 ? want : 1) : cap);
 }
 
+size_t t3_scratch_bytes() { return (size_t)6 * kT3Blocks * 2 * sizeof(double); }
+
 template <typename T>
-static cudaError_t t3_prepare(int dim, const int nf[3], int nspread, double beta, double kc, double upsampfac,
-                              int isign, const void* const* src, int64_t M, const void* c, int n_trans,
-                              const void* const* tgt, int64_t K, void* params, void* const* src_out, void* c_out,
-                              void* const* tgt_out, void* factor, void* scratch, cudaStream_t st) {
+cudaError_t launch_t3_params(int dim, const int nf[3], double upsampfac, const void* const* src, int64_t M,
+                             const void* const* tgt, int64_t K, T3Params* params, void* scratch, cudaStream_t st) {
   double* partial = (double*)scratch;
   for (int d = 0; d < dim; ++d) {
     k_minmax<T><<<kT3Blocks, 256, 0, st>>>((const T*)src[d], M, partial + (size_t)d * kT3Blocks * 2);
     k_minmax<T><<<kT3Blocks, 256, 0, st>>>((const T*)tgt[d], K, partial + (size_t)(dim + d) * kT3Blocks * 2);
   }
   k_t3_params<T><<<1, 32, 0, st>>>(partial, dim, nf[0], dim > 1 ? nf[1] : 1, dim > 2 ? nf[2] : 1, upsampfac,
-                                   (T3Params*)params);
+                                   params);
+  return cudaGetLastError();
+}
+
+template cudaError_t launch_t3_params<float>(int, const int*, double, const void* const*, int64_t,
+                                             const void* const*, int64_t, T3Params*, void*, cudaStream_t);
+template cudaError_t launch_t3_params<double>(int, const int*, double, const void* const*, int64_t,
+                                              const void* const*, int64_t, T3Params*, void*, cudaStream_t);
+
+template <typename T>
+static cudaError_t t3_prepare(int dim, const int nf[3], int nspread, double beta, double kc, double upsampfac,
+                              int isign, const void* const* src, int64_t M, const void* c, int n_trans,
+                              const void* const* tgt, int64_t K, void* params, void* const* src_out, void* c_out,
+                              void* const* tgt_out, void* factor, void* scratch, cudaStream_t st) {
+  cudaError_t e = launch_t3_params<T>(dim, nf, upsampfac, src, M, tgt, K, (T3Params*)params, scratch, st);
+  if (e != cudaSuccess) return e;
   const T* s3[3] = {nullptr, nullptr, nullptr};
   const T* t3[3] = {nullptr, nullptr, nullptr};
   T* so[3] = {nullptr, nullptr, nullptr};
@@ -219,7 +230,7 @@ size_t nfx_t3_scratch_bytes(int precision, int64_t M, int64_t K) {
   (void)precision;
   (void)M;
   (void)K;
-  return (size_t)6 * kT3Blocks * 2 * sizeof(double);
+  return t3_scratch_bytes();
 }
 
 int nfx_t3_prepare(int precision, int dim, const int nf[3], int nspread, double beta, double kc, double upsampfac,

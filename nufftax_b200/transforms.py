@@ -37,7 +37,7 @@ forward and reverse mode flow through the same Functions.
 
 from __future__ import annotations
 
-from ctypes import c_void_p
+from ctypes import byref, c_size_t, c_void_p
 from typing import Sequence
 
 import numpy as np
@@ -45,8 +45,9 @@ import torch
 import torch.autograd.forward_ad as _fwad
 
 from . import _lib
-from ._plan import (PointSort, complex_dtype, deconv_pad, deconv_shuffle, fft_inplace, precision_of, ptr,
-                    real_dtype, sort_cache, stream_of)
+from ._plan import (_facs, complex_dtype, deconv_pad, deconv_shuffle, fft_inplace, make_opts, precision_of, ptr,
+                    real_dtype, sort_cache, sort_launches, stream_of)
+from .profiling import span
 from .grid import compute_grid_size
 from .kernel import compute_kernel_params
 
@@ -470,10 +471,13 @@ def nufft3d2(x, y, z, f, eps: float = 1e-6, isign: int = -1, upsampfac=2.0):
 # ---------------------------------------------------------------------------
 def _type3_forward(src: list[torch.Tensor], c2: torch.Tensor, tgt: list[torch.Tensor], nf: tuple[int, ...],
                    eps: float, isign: int, uf: float) -> torch.Tensor:
+    """One nfx_nufft3 call: the type-3 scalars on the device, the source sort
+    with the rescaling and pre-phase fused in, spread, the inner type 2's
+    deconvolution / zero-pad and FFT, the target sort with the phase / phihat
+    factor fused in, interpolation (nufftax/transforms/nufft3.py:216-515)."""
     dim = len(src)
     dev = c2.device
     precision = precision_of(c2.dtype)
-    rdt = real_dtype(precision)
     M = src[0].shape[0]
     K = tgt[0].shape[0]
     nt = c2.shape[0]
@@ -481,35 +485,30 @@ def _type3_forward(src: list[torch.Tensor], c2: torch.Tensor, tgt: list[torch.Te
     lib = _lib.load()
     if M == 0 or K == 0:
         return torch.zeros((nt, K), dtype=c2.dtype, device=dev)
-    params = torch.empty(int(lib.nfx_t3_params_bytes()), dtype=torch.uint8, device=dev)
-    sbytes = int(lib.nfx_t3_scratch_bytes(precision, M, K))
-    scratch = torch.empty(sbytes, dtype=torch.uint8, device=dev)
-    src_out = [torch.empty(M, dtype=rdt, device=dev) for _ in range(dim)]
-    tgt_out = [torch.empty(K, dtype=rdt, device=dev) for _ in range(dim)]
-    c_out = torch.empty_like(c2)
-    factor = torch.empty(K, dtype=c2.dtype, device=dev)
+    nf = tuple(int(n) for n in nf)
+    nf_in = tuple(compute_grid_size(n, uf, kp.nspread) for n in nf)
+    opts = make_opts(precision, nf, kp, prenorm=False)
+    nbytes = c_size_t(0)
+    _lib.check(lib.nfx_nufft3_workspace_bytes(byref(opts), _lib.int3c(nf_in), M, K, nt, byref(nbytes)),
+               "nfx_nufft3_workspace_bytes")
+    ws = torch.empty(max(int(nbytes.value), 1), dtype=torch.uint8, device=dev)
+    facs = _facs(nf_in, nf, kp, precision, dev)
+    out = torch.empty((nt, K), dtype=c2.dtype, device=dev)
     arr = c_void_p * 3
 
     def parr(ts):
         return arr(*([t.data_ptr() for t in ts] + [None] * (3 - len(ts))))
 
-    with torch.cuda.device(dev):
-        _lib.check(lib.nfx_t3_prepare(precision, dim, _lib.int3(nf), kp.nspread, kp.beta, kp.c, uf, int(isign),
-                                      parr(src), M, ptr(c2), nt, parr(tgt), K, ptr(params), parr(src_out),
-                                      ptr(c_out), parr(tgt_out), ptr(factor), ptr(scratch), sbytes,
-                                      c_void_p(stream_of(dev))), "nfx_t3_prepare")
-    # spread at the rescaled sources (fold only, like nufft3.py:283/378/483)
-    ps = PointSort(src_out, nf, kp, prenorm=False)
-    fw = ps.spread(c_out)
-    # inner type 2 on the fine grid treated as modes (nufft3.py:381-387)
-    nf_in = tuple(compute_grid_size(n, uf, kp.nspread) for n in nf)
-    fw2 = deconv_pad(fw, nf_in, kp)
-    fft_inplace(fw2, dim, _fft_sign_type2(isign))
-    ps2 = PointSort(tgt_out, nf_in, kp, prenorm=True)
-    out = ps2.interp(fw2)
-    with torch.cuda.device(dev):
-        _lib.check(lib.nfx_t3_finish(precision, ptr(factor), K, nt, ptr(out), c_void_p(stream_of(dev))),
-                   "nfx_t3_finish")
+    src = [a.contiguous() for a in src]
+    tgt = [a.contiguous() for a in tgt]
+    c2 = c2.contiguous()
+    # our kernels: min / max per array, the scalars, both sorts, spread, zero-pad, interp
+    launches = lambda: (2 * dim + 1 + sort_launches(opts, M) + 2  # noqa: E731 (evaluated only when recording)
+                        + sort_launches(make_opts(precision, nf_in, kp, prenorm=True), K) + 1)
+    with torch.cuda.device(dev), span("nfx_nufft3", dev, launches):
+        _lib.check(lib.nfx_nufft3(byref(opts), _lib.int3c(nf_in), float(uf), int(isign), parr(src), M, ptr(c2), nt,
+                                  parr(tgt), K, ptr(facs[0]), ptr(facs[1]), ptr(facs[2]), ptr(out), ptr(ws),
+                                  ws.numel(), c_void_p(stream_of(dev))), "nfx_nufft3")
     return out
 
 
