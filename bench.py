@@ -32,6 +32,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -167,6 +168,23 @@ class ClockSampler:
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": sorted(reasons), "samples": len(sm)}
+
+
+class clocked:
+    """`with clocked(index) as ck: ...` samples the SM clocks and throttle
+    reasons while the block runs; ck.summary afterwards."""
+
+    def __init__(self, index: int):
+        self.sampler = ClockSampler(index)
+        self.summary = None
+
+    def __enter__(self):
+        self.sampler.start()
+        return self
+
+    def __exit__(self, *exc):
+        self.summary = self.sampler.stop()
+        return False
 
 
 def dist_setup():
@@ -436,6 +454,14 @@ def run_gpu(args):
         "clocks": clocks,
         "breakdown": breakdown,
     }
+    if world == 1 and not args.no_subconfigs:
+        # the other BASELINE configurations, measured in the same run (each with
+        # its own clock record): 1D, the 64-problem batched mix, the
+        # differentiated 3D step and a served mixed stream
+        line["configs"] = {"plain_1d": measure_1d(dev, 50, 5),
+                           "batched": measure_batched(dev, 10, 3),
+                           "grad3d": measure_grad3d(dev, 5, 3),
+                           "served": measure_serve(dev, args.served_requests, 300, [1.0, 4.0])}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         # GPU results of one step at full size (the compute path of the timed
         # steps), checked in the CPU leg below against the oracle and the FP64
@@ -633,7 +659,7 @@ def batched_workload(seed=77, P=64):
     return probs
 
 
-def run_batched(args):
+def measure_batched(dev, steps: int, warmup: int, autotune: bool = False) -> dict:
     """Batched plan (one persistent launch per pass, CUDA graph) vs the per-problem plain path."""
     import torch
 
@@ -641,7 +667,6 @@ def run_batched(args):
     from nufftax_b200.autotune import tune
     from nufftax_b200.batch import BatchPlan
 
-    dev = torch.device("cuda", 0)
     eps = 1e-5
     probs = batched_workload()
     d = [{k: (torch.from_numpy(v).to(dev) if isinstance(v, np.ndarray) else v) for k, v in q.items()} for q in probs]
@@ -654,8 +679,8 @@ def run_batched(args):
             nb.nufft2d1(q["x"], q["y"], q["c"], q["n_modes"], eps=eps)
             nb.nufft2d2(q["x"], q["y"], q["f"], eps=eps)
 
-    def timed(fn, steps, warm):
-        for _ in range(warm):
+    def timed(fn):
+        for _ in range(warmup):
             fn()
         torch.cuda.synchronize()
         tot = 0.0
@@ -670,10 +695,9 @@ def run_batched(args):
             tot += a.elapsed_time(b)
         return tot / steps
 
-    plain_ms = timed(plain_step, args.steps, args.warmup)
     kp = nb.compute_kernel_params(eps)
     tiles, maxsubs = [], []
-    if args.autotune:
+    if autotune:
         for q in d:
             nf = tuple(nb.compute_grid_size(n, 2.0, kp.nspread) for n in q["n_modes"])
             t, m = tune([q["x"], q["y"]], nf, kp)
@@ -684,36 +708,40 @@ def run_batched(args):
     for p, q in enumerate(d):
         plan.c_in[p].copy_(q["c"])
         plan.f_in[p].copy_(q["f"])
-    batch_ms = timed(lambda: plan.run(), args.steps, args.warmup)
-    line = {"metric": "batched 2D type-1 + type-2 NU points/s (64 problems, eps 1e-5, complex64)",
+    with clocked(dev.index) as ck:
+        plain_ms = timed(plain_step)
+        batch_ms = timed(lambda: plan.run())
+    return {"metric": "batched 2D type-1 + type-2 NU points/s (64 problems, eps 1e-5, complex64)",
             "value": pts / (batch_ms / 1e3), "unit": "NU points/s", "plain_value": pts / (plain_ms / 1e3),
             "speedup_vs_plain": plain_ms / batch_ms, "ms_per_step": batch_ms, "plain_ms_per_step": plain_ms,
-            "points_per_step": pts, "steps": args.steps, "warmup": args.warmup, "autotune": bool(args.autotune),
+            "points_per_step": pts, "steps": steps, "warmup": warmup, "autotune": bool(autotune),
+            "clocks": ck.summary,
             "config": {"workload": "64 problems, M log-uniform [1e4, 2e6], modes per axis from {128,256,384,512}, "
                                    "half uniform / half clustered N(0,0.3^2), sort included every step",
                        "l2": "flushed between steps"}}
-    print(json.dumps(line), flush=True)
 
 
-def run_grad3d(args):
-    """3D type 1, M = 8e6 uniform points, 128^3 modes, eps 1e-6, complex64:
+def run_batched(args):
+    import torch
+
+    print(json.dumps(measure_batched(torch.device("cuda", 0), args.steps, args.warmup, args.autotune)), flush=True)
+
+
+def measure_grad3d(dev, steps: int, warmup: int, M: int = 8_000_000) -> dict:
+    """3D type 1, M uniform points, 128^3 modes, eps 1e-6, complex64:
     loss = ||nufft3d1(x, y, z, c) - f_target||^2 and its gradients w.r.t. c, x, y, z
     through the hand-written adjoint kernels (forward + backward per step).
-    --check adds, at full size: central finite differences in complex128 on 32
-    random entries, and the reference's spectral gradient formula (JVP with
-    k-weighted transforms, then transpose; nufftax/transforms/primitives.py:443-471)
-    evaluated with this library's type-2 transforms."""
+    Inputs are drawn on the device (seeded)."""
     import torch
 
     import nufftax_b200 as nb
 
-    dev = torch.device("cuda", 0)
-    M, N, eps = int(8_000_000 * args.scale), (128, 128, 128), 1e-6
-    rng = np.random.default_rng(4)
-    X = [torch.from_numpy(rng.uniform(-np.pi, np.pi, M).astype(np.float32)).to(dev) for _ in range(3)]
-    c = torch.from_numpy((rng.standard_normal(M) + 1j * rng.standard_normal(M)).astype(np.complex64)).to(dev)
-    tgt = torch.from_numpy((rng.standard_normal(N[::-1]) + 1j * rng.standard_normal(N[::-1])).astype(np.complex64)
-                           ).to(dev)
+    N, eps = (128, 128, 128), 1e-6
+    g = torch.Generator(device=dev)
+    g.manual_seed(4)
+    X = [(torch.rand(M, device=dev, generator=g) * 2 - 1) * np.pi for _ in range(3)]
+    c = torch.complex(torch.randn(M, device=dev, generator=g), torch.randn(M, device=dev, generator=g))
+    tgt = torch.complex(torch.randn(N[::-1], device=dev, generator=g), torch.randn(N[::-1], device=dev, generator=g))
 
     def step():
         nb.sort_cache.clear()
@@ -724,24 +752,35 @@ def run_grad3d(args):
         loss.backward()
         return loss, cc.grad, [x.grad for x in xs]
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         step()
     torch.cuda.synchronize()
     tot = 0.0
-    for _ in range(args.steps):
-        a = torch.cuda.Event(enable_timing=True)
-        b = torch.cuda.Event(enable_timing=True)
-        a.record()
-        step()
-        b.record()
-        torch.cuda.synchronize()
-        tot += a.elapsed_time(b)
-    ms = tot / args.steps
-    line = {"metric": "differentiated 3D type-1 NU points/s (forward + backward w.r.t. c, x, y, z)",
-            "value": M / (ms / 1e3), "unit": "NU points/s", "ms_per_step": ms, "steps": args.steps,
-            "config": {"workload": f"M={M} uniform 3D, 128^3 modes, nf 256^3, eps 1e-6, complex64"}}
+    with clocked(dev.index) as ck:
+        for _ in range(steps):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record()
+            step()
+            b.record()
+            torch.cuda.synchronize()
+            tot += a.elapsed_time(b)
+    ms = tot / steps
+    return {"metric": "differentiated 3D type-1 NU points/s (forward + backward w.r.t. c, x, y, z)",
+            "value": M / (ms / 1e3), "unit": "NU points/s", "ms_per_step": ms, "steps": steps, "warmup": warmup,
+            "clocks": ck.summary,
+            "config": {"workload": f"M={M} uniform 3D, 128^3 modes, nf 256^3, eps 1e-6, complex64, "
+                                   "loss ||f - t||^2, gradients w.r.t. c, x, y, z; sort every step"}}
+
+
+def run_grad3d(args):
+    import torch
+
+    dev = torch.device("cuda", 0)
+    M = int(8_000_000 * args.scale)
+    line = measure_grad3d(dev, args.steps, args.warmup, M)
     if args.check:
-        line["check"] = grad3d_check(M, N, rng)
+        line["check"] = grad3d_check(M, (128, 128, 128), np.random.default_rng(4))
     print(json.dumps(line), flush=True)
 
 
@@ -816,13 +855,38 @@ def grad3d_check(M, N, rng):
     return out
 
 
+class _DevicePool:
+    """Pre-drawn device random numbers that the served requests' inputs are
+    sliced from (no kernel launches per request, the same cost in the served
+    and the one-at-a-time paths): uniform coordinates in [-pi, pi), target
+    frequencies in [-300, 300) and standard normals viewed as complex."""
+
+    _pools: dict = {}
+
+    def __init__(self, device, n_uniform=1 << 26, n_normal=1 << 27):
+        import torch
+
+        g = torch.Generator(device=device)
+        g.manual_seed(5)
+        self.u = (torch.rand(n_uniform, device=device, generator=g) * 2 - 1) * np.pi
+        self.t = self.u * (300.0 / np.pi)
+        self.n = torch.randn(n_normal, device=device, generator=g)
+
+    @classmethod
+    def get(cls, device):
+        key = str(device)
+        if key not in cls._pools:
+            cls._pools[key] = cls(device)
+        return cls._pools[key]
+
+
 def served_requests(n, seed=5):
     """The served mix: 50 % 2D type 1/2 (modes per axis from 128..512 in steps of
     32, M log-uniform 1e3..4e6), 30 % 3D type 1/2 (modes per axis from 64..160 in
     steps of 16, M log-uniform 1e4..8e6),
     20 % 2D type 3 (sources uniform in [-pi, pi)^2, targets uniform in
     [-300, 300]^2, M = K log-uniform 1e3..1e6); eps 1e-6, complex64.  Inputs are
-    generated on the device at admission from a per-request seed."""
+    slices, at seeded offsets, of random numbers drawn on the device once."""
     import torch
 
     from nufftax_b200 import compute_type3_grid_sizes_2d
@@ -847,23 +911,25 @@ def served_requests(n, seed=5):
             nm = compute_type3_grid_sizes_2d(np.pi, np.pi, 300.0, 300.0, eps=1e-6)
 
         def make(device, kind=kind, dim=dim, M=M, nm=nm, sd=int(rng.integers(1 << 31))):
-            g = torch.Generator(device=device)
-            g.manual_seed(sd)
-            X = [(torch.rand(M, device=device, generator=g) * 2 - 1) * np.pi for _ in range(dim)]
+            pool = _DevicePool.get(device)
+            r = np.random.default_rng(sd)
+            off = lambda n_, total: 2 * int(r.integers(0, (total - n_) // 2))  # noqa: E731 (even: complex views)
+            X = [pool.u[o:o + M] for o in (off(M, pool.u.numel()) for _ in range(dim))]
             if kind == 2:
                 shape = tuple(reversed(nm))
-                f = torch.complex(torch.randn(shape, device=device, generator=g),
-                                  torch.randn(shape, device=device, generator=g))
-                return X, f, None
-            c = torch.complex(torch.randn(M, device=device, generator=g), torch.randn(M, device=device, generator=g))
-            T = [(torch.rand(M, device=device, generator=g) * 2 - 1) * 300.0 for _ in range(dim)] if kind == 3 else None
+                k = math.prod(shape)
+                o = off(2 * k, pool.n.numel())
+                return X, torch.view_as_complex(pool.n[o:o + 2 * k].view(k, 2)).view(shape), None
+            o = off(2 * M, pool.n.numel())
+            c = torch.view_as_complex(pool.n[o:o + 2 * M].view(M, 2))
+            T = [pool.t[o2:o2 + M] for o2 in (off(M, pool.t.numel()) for _ in range(dim))] if kind == 3 else None
             return X, c, T
 
         reqs.append(Request(kind=kind, dim=dim, n_modes=nm, M=M, K=M if kind == 3 else 0, make_inputs=make))
     return reqs
 
 
-def run_serve(args):
+def measure_serve(dev, n: int, plain_sample: int, loads, slots: int = 8) -> dict:
     """Served stream vs one-at-a-time plain execution; Poisson arrivals."""
     import copy
 
@@ -872,8 +938,6 @@ def run_serve(args):
     import nufftax_b200 as nb
     from nufftax_b200.serve import NufftServer
 
-    dev = torch.device("cuda", 0)
-    n = args.requests
     reqs = served_requests(n)
     # both paths start with warm cuFFT plans: one small transform per distinct shape
     shapes = sorted({(r.kind, r.dim, tuple(r.n_modes)) for r in reqs})
@@ -890,48 +954,98 @@ def run_serve(args):
                                                                 device=dev))
     torch.cuda.synchronize()
     # one-at-a-time: each request alone through the public API, synchronised
-    sample = [copy.copy(r) for r in reqs[: min(n, args.plain_sample)]]
+    sample = [copy.copy(r) for r in reqs[: min(n, plain_sample)]]
     for r in sample[:5]:
         _plain(nb, r, dev)
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for r in sample:
-        _plain(nb, r, dev)
-        torch.cuda.synchronize()
-    plain_s = time.perf_counter() - t0
-    plain_pts = sum(r.points() for r in sample) / plain_s
-    plain_rps = len(sample) / plain_s
-    out = {"metric": "served mixed stream NU points/s (p50/p99 latency)", "unit": "NU points/s",
-           "requests": n, "distinct_shapes": len(shapes),
-           "one_at_a_time": {"points_per_s": plain_pts, "requests_per_s": plain_rps,
-                                            "sample": len(sample)}, "loads": []}
-    rng = np.random.default_rng(11)
-    for load in args.loads:
-        rate = load * plain_rps
-        arrivals = np.cumsum(rng.exponential(1.0 / rate, n))
-        server = NufftServer(dev, slots=args.slots, hbm_budget=150e9, keep_results=False)
-        batch = [copy.copy(r) for r in reqs]
-        # warm the caches (plans, grid pool) with the first few requests
-        server.serve([copy.copy(r) for r in reqs[:20]])
-        torch.cuda.synchronize()
-        server.completed = []
-        retries0 = torch.cuda.memory_stats(dev).get("num_alloc_retries", 0)
-        torch.cuda.reset_peak_memory_stats(dev)
-        done = server.serve(batch, list(arrivals))
-        st = server.stats(done)
-        mem = torch.cuda.memory_stats(dev)
-        # allocator retries free the cache and synchronise the device: a stall
-        st["alloc_retries"] = int(mem.get("num_alloc_retries", 0) - retries0)
-        st["peak_reserved_gb"] = round(mem.get("reserved_bytes.all.peak", 0) / 1e9, 1)
-        st["offered_load"] = load
-        st["offered_requests_per_s"] = rate
-        out["loads"].append(st)
+    with clocked(dev.index) as ck:
+        t0 = time.perf_counter()
+        for r in sample:
+            _plain(nb, r, dev)
+            torch.cuda.synchronize()
+        plain_s = time.perf_counter() - t0
+        plain_pts = sum(r.points() for r in sample) / plain_s
+        plain_rps = len(sample) / plain_s
+        out = {"metric": "served mixed stream NU points/s (p50/p99 latency)", "unit": "NU points/s",
+               "requests": n, "distinct_shapes": len(shapes),
+               "one_at_a_time": {"points_per_s": plain_pts, "requests_per_s": plain_rps, "sample": len(sample)},
+               "loads": []}
+        rng = np.random.default_rng(11)
+        for load in loads:
+            rate = load * plain_rps
+            arrivals = np.cumsum(rng.exponential(1.0 / rate, n))
+            server = NufftServer(dev, slots=slots, hbm_budget=150e9, keep_results=False)
+            batch = [copy.copy(r) for r in reqs]
+            # warm the caches (plans, grid pool) with the first few requests
+            server.serve([copy.copy(r) for r in reqs[:20]])
+            torch.cuda.synchronize()
+            server.completed = []
+            retries0 = torch.cuda.memory_stats(dev).get("num_alloc_retries", 0)
+            torch.cuda.reset_peak_memory_stats(dev)
+            done = server.serve(batch, list(arrivals))
+            st = server.stats(done)
+            mem = torch.cuda.memory_stats(dev)
+            # allocator retries free the cache and synchronise the device: a stall
+            st["alloc_retries"] = int(mem.get("num_alloc_retries", 0) - retries0)
+            st["peak_reserved_gb"] = round(mem.get("reserved_bytes.all.peak", 0) / 1e9, 1)
+            st["offered_load"] = load
+            st["offered_requests_per_s"] = rate
+            out["loads"].append(st)
     best = max(out["loads"], key=lambda d: d["points_per_s"])
     out["value"] = best["points_per_s"]
     out["p50_ms"] = best["p50_ms"]
     out["p99_ms"] = best["p99_ms"]
     out["speedup_vs_one_at_a_time"] = best["points_per_s"] / plain_pts
-    print(json.dumps(out), flush=True)
+    out["clocks"] = ck.summary
+    out["config"] = {"workload": "Poisson arrivals: 50% 2D type 1/2 (modes 128..512 per axis, M log-uniform 1e3..4e6), "
+                                 "30% 3D type 1/2 (modes 64..160, M log-uniform 1e4..8e6), 20% 2D type 3 (targets in "
+                                 "[-300,300]^2, M = K log-uniform 1e3..1e6), eps 1e-6, complex64, HBM budget 150 GB",
+                     "offered_load": "multiples of the measured one-at-a-time request rate",
+                     "inputs": "sliced at admission from random numbers drawn on the device once (seeded offsets), "
+                               "the same in both paths"}
+    return out
+
+
+def run_serve(args):
+    import torch
+
+    print(json.dumps(measure_serve(torch.device("cuda", 0), args.requests, args.plain_sample, args.loads,
+                                   args.slots)), flush=True)
+
+
+def measure_1d(dev, steps: int, warmup: int) -> dict:
+    """The 1D configuration: type 1 then type 2, M = 200,000 uniform points,
+    N = 8192 modes, eps 1e-6, complex64 (sort included every step)."""
+    import torch
+
+    import nufftax_b200 as nb
+
+    rng = np.random.default_rng(21)
+    M, N = 200_000, 8192
+    x = torch.from_numpy(rng.uniform(-np.pi, np.pi, M).astype(np.float32)).to(dev)
+    c = torch.from_numpy((rng.standard_normal(M) + 1j * rng.standard_normal(M)).astype(np.complex64)).to(dev)
+    f = torch.from_numpy((rng.standard_normal(N) + 1j * rng.standard_normal(N)).astype(np.complex64)).to(dev)
+
+    def step():
+        nb.sort_cache.clear()
+        nb.nufft1d1(x, c, N, eps=EPS)
+        nb.nufft1d2(x, f, eps=EPS)
+
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    with clocked(dev.index) as ck:
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(steps):
+            step()
+        b.record()
+        torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / steps
+    return {"metric": "1D type-1 + type-2 NU points/s (M=200000, N=8192, eps 1e-6, complex64)", "value": 2 * M / (ms / 1e3),
+            "unit": "NU points/s", "ms_per_step": ms, "steps": steps, "warmup": warmup, "clocks": ck.summary,
+            "note": "inputs resident, back-to-back steps (launch-bound at this size)"}
 
 
 def _plain(nb, r, dev):
@@ -952,6 +1066,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="nufftax_b200", choices=["nufftax_b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-subconfigs", action="store_true", help="headline only (no batched / grad3d / served / 1D)")
+    ap.add_argument("--served-requests", type=int, default=1000, help="requests of the served sub-record")
     ap.add_argument("--case", choices=["radial", "clustered", "uniform3d"],
                     help="profile one point set only (no timing)")
     ap.add_argument("--reps", type=int, default=2)

@@ -253,6 +253,42 @@ int nfx_batch_deconv(int precision, int pad, const void* dev_table, int nprob, i
  *   e^{i isign sum_d (s_d - D_d) C_d} / prod_d phihat(h_d gamma_d (s_d - D_d))
  *   (nufft3.py:176-213, 390-394).  nf[d] is the type-3 grid per axis.
  * nfx_t3_finish: out[t][k] *= factor[k]. */
+/* ---- a wave of independent type-1 / type-2 transforms in one call -------------
+ * No counterpart in the reference.  For serving loops: n problems of one
+ * precision, dimension and kernel (`common`; its nf / tile / max_subproblem are
+ * ignored, each item has its own grid), each a type 1 (in: M strengths, out:
+ * n_modes modes in CMCL order) or a type 2 (in: modes, out: M values), one
+ * transform each, are enqueued on `stream` as: one zero-pad launch for every
+ * type-2 problem, their FFTs, every problem's sort, ONE persistent spread over
+ * the bin tiles of all type-1 problems, ONE persistent interpolation over those
+ * of all type-2 problems, the type-1 FFTs and one crop launch for all of them.
+ * fac[d]: the problem's deconvolution factors (as nfx_deconv_*); fw: its fine
+ * grid buffer; workspace: its sort workspace (nfx_sort_workspace_bytes with
+ * its nf).  The problem table is built in `host_staging` (pinned host memory of
+ * nfx_wave_table_bytes) and copied to `dev_table` asynchronously: both must stay
+ * untouched until the wave's work on the stream is done.  The FFTs use the
+ * stream's cuFFT work area (as nfx_fft), so a capturing stream is refused. */
+typedef struct nfx_wave_item {
+  int kind;              /* 1 or 2 */
+  int64_t M;
+  const void* x;
+  const void* y;
+  const void* z;
+  int nf[3];             /* fine grid per axis; unused axes 1 */
+  int n_modes[3];        /* modes per axis; unused axes 1 */
+  int fft_sign;          /* +1 or -1, as nfx_fft */
+  const void* fac[3];
+  const void* in;
+  void* out;
+  void* fw;
+  void* workspace;
+  size_t workspace_bytes;
+} nfx_wave_item;
+
+int nfx_wave_table_bytes(const nfx_opts* common, const nfx_wave_item* items, int n, size_t* table_bytes);
+int nfx_wave(const nfx_opts* common, const nfx_wave_item* items, int n, void* dev_table, void* host_staging,
+             size_t table_bytes, void* stream);
+
 /* ---- type 3 in one call ------------------------------------------------------
  * The whole of nufftax/transforms/nufft3.py:216-515 with its pre- and
  * post-processing fused into the passes: the source sort applies the rescaling

@@ -69,6 +69,27 @@ class NfxBatchProblem(ctypes.Structure):
     ]
 
 
+class NfxWaveItem(ctypes.Structure):
+    """Mirror of `nfx_wave_item` in include/nfx.h."""
+
+    _fields_ = [
+        ("kind", c_int),
+        ("M", c_int64),
+        ("x", c_void_p),
+        ("y", c_void_p),
+        ("z", c_void_p),
+        ("nf", c_int * 3),
+        ("n_modes", c_int * 3),
+        ("fft_sign", c_int),
+        ("fac", c_void_p * 3),
+        ("in_", c_void_p),
+        ("out", c_void_p),
+        ("fw", c_void_p),
+        ("workspace", c_void_p),
+        ("workspace_bytes", c_size_t),
+    ]
+
+
 class NfxBatchInfo(ctypes.Structure):
     """Mirror of `nfx_batch_info` in include/nfx.h."""
 
@@ -116,6 +137,8 @@ _SIGNATURES = {
                                  POINTER(c_void_p), POINTER(c_void_p), c_int, _vp, c_size_t, POINTER(c_int64), _vp],
                                 c_int),
     "nfx_batch_deconv": ([c_int, c_int, _vp, c_int, c_int64, _vp], c_int),
+    "nfx_wave_table_bytes": ([POINTER(NfxOpts), POINTER(NfxWaveItem), c_int, POINTER(c_size_t)], c_int),
+    "nfx_wave": ([POINTER(NfxOpts), POINTER(NfxWaveItem), c_int, _vp, _vp, c_size_t, _vp], c_int),
     "nfx_nufft3_workspace_bytes": ([POINTER(NfxOpts), POINTER(c_int), c_int64, c_int64, c_int, POINTER(c_size_t)],
                                    c_int),
     "nfx_nufft3": ([POINTER(NfxOpts), POINTER(c_int), c_double, c_int, POINTER(c_void_p), c_int64, _vp, c_int,

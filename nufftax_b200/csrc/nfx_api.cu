@@ -691,6 +691,119 @@ static int nufft3_run(Nufft3Layout& L3, double upsampfac, int isign, const void*
   return e == cudaSuccess ? NFX_OK : cuda_fail(e, "nfx_nufft3 interp");
 }
 
+// Device table of one wave (nfx_wave): spread items and their subproblem
+// prefix, interp items and theirs, then the zero-pad items of the type-2
+// problems and the crop items of the type-1 problems.
+struct WaveLayout {
+  int n1 = 0, n2 = 0;
+  size_t off_spread, off_prefix_s, off_interp, off_prefix_i, off_pad, off_shuffle, total;
+  size_t smem_s = 0, smem_i = 0;
+  int64_t subs_s = 0, subs_i = 0;
+};
+
+static int wave_layout(const nfx_opts* common, const nfx_wave_item* items, int n, WaveLayout& W,
+                       std::vector<Prepared>* prep) {
+  if (common == nullptr || items == nullptr || n < 1) {
+    set_error("nfx_wave: invalid arguments");
+    return NFX_ERR_INVALID;
+  }
+  const size_t rb = real_bytes(common->precision);
+  for (int i = 0; i < n; ++i) {
+    const nfx_wave_item& it = items[i];
+    if (it.kind != 1 && it.kind != 2) {
+      set_error("nfx_wave: kind must be 1 or 2");
+      return NFX_ERR_INVALID;
+    }
+    nfx_opts o = *common;
+    for (int d = 0; d < 3; ++d) o.nf[d] = it.nf[d];
+    Prepared P;
+    int st = prepare(&o, it.M, it.x, it.y, it.z, it.workspace, it.workspace_bytes, P);
+    if (st != NFX_OK) return st;
+    if (it.in == nullptr || it.out == nullptr || it.fw == nullptr) {
+      set_error("nfx_wave: NULL in / out / fw");
+      return NFX_ERR_INVALID;
+    }
+    if (it.kind == 1) {
+      ++W.n1;
+      W.smem_s = std::max(W.smem_s, spread_smem_bytes(rb, P.o.dim, P.o.nspread, P.g));
+      W.subs_s += P.L.max_subs;
+    } else {
+      ++W.n2;
+      W.smem_i = std::max(W.smem_i, tile_smem_bytes(rb, P.g));
+      W.subs_i += P.L.max_subs;
+    }
+    if (prep) prep->push_back(P);
+  }
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    size_t at = off;
+    off += align256(bytes);
+    return at;
+  };
+  const size_t ib = batch_item_bytes(common->precision), db = deconv_item_bytes(common->precision == NFX_F64);
+  W.off_spread = take(ib * W.n1);
+  W.off_prefix_s = take((size_t)(W.n1 + 1) * 4);
+  W.off_interp = take(ib * W.n2);
+  W.off_prefix_i = take((size_t)(W.n2 + 1) * 4);
+  W.off_pad = take(db * W.n2);
+  W.off_shuffle = take(db * W.n1);
+  W.total = off;
+  return NFX_OK;
+}
+
+template <typename T>
+static void wave_items(const nfx_opts* common, const nfx_wave_item* items, int n, const std::vector<Prepared>& prep,
+                       const WaveLayout& W, unsigned char* host) {
+  BatchItem<T>* sp = (BatchItem<T>*)(host + W.off_spread);
+  BatchItem<T>* ip = (BatchItem<T>*)(host + W.off_interp);
+  int a = 0, b = 0;
+  std::vector<int> nf1, nm1, nf2, nm2;
+  std::vector<const void*> fac1, fac2, src1, src2;
+  std::vector<void*> dst1, dst2;
+  for (int i = 0; i < n; ++i) {
+    const nfx_wave_item& it = items[i];
+    const Prepared& P = prep[i];
+    BatchItem<T>& bi = it.kind == 1 ? sp[a++] : ip[b++];
+    bi.a = make_args<T>(P.g, P.o.beta, P.o.kc, it.M, 1, view(P.L, it.workspace));
+    attach_poly(bi.a, P.o.nspread, P.o.beta, P.o.kc);
+    bi.src = it.kind == 1 ? it.in : it.fw;
+    bi.dst = it.kind == 1 ? it.fw : it.out;
+    auto& nf = it.kind == 1 ? nf1 : nf2;
+    auto& nm = it.kind == 1 ? nm1 : nm2;
+    auto& fac = it.kind == 1 ? fac1 : fac2;
+    for (int d = 0; d < 3; ++d) {
+      nf.push_back(d < common->dim ? it.nf[d] : 1);
+      nm.push_back(d < common->dim ? it.n_modes[d] : 1);
+      fac.push_back(d < common->dim ? it.fac[d] : nullptr);
+    }
+    if (it.kind == 1) {
+      src1.push_back(it.fw);
+      dst1.push_back(it.out);
+    } else {
+      src2.push_back(it.in);
+      dst2.push_back(it.fw);
+    }
+  }
+  const int prec = common->precision == NFX_F64 ? 1 : 0;
+  if (W.n2 > 0)
+    fill_deconv_items(prec, common->dim, true, nf2.data(), nm2.data(), fac2.data(), src2.data(), dst2.data(), W.n2,
+                      host + W.off_pad);
+  if (W.n1 > 0)
+    fill_deconv_items(prec, common->dim, false, nf1.data(), nm1.data(), fac1.data(), src1.data(), dst1.data(), W.n1,
+                      host + W.off_shuffle);
+}
+
+static int64_t deconv_total(const nfx_wave_item* items, int n, int kind, int dim, bool pad) {
+  int64_t t = 0;
+  for (int i = 0; i < n; ++i) {
+    if (items[i].kind != kind) continue;
+    int64_t c = 1;
+    for (int d = 0; d < dim; ++d) c *= pad ? items[i].nf[d] : items[i].n_modes[d];
+    t += c;
+  }
+  return t;
+}
+
 }  // namespace nfx
 
 using namespace nfx;
@@ -1101,6 +1214,101 @@ int nfx_nufft3(const nfx_opts* opts, const int nf_inner[3], double upsampfac, in
                                  (char*)workspace, s)
              : nufft3_run<double>(L3, upsampfac, isign, src, M, c, n_trans, tgt, K, fac1, fac2, fac3, out,
                                   (char*)workspace, s);
+}
+
+int nfx_wave_table_bytes(const nfx_opts* common, const nfx_wave_item* items, int n, size_t* table_bytes) {
+  if (table_bytes == nullptr) {
+    set_error("nfx_wave_table_bytes: table_bytes is NULL");
+    return NFX_ERR_INVALID;
+  }
+  WaveLayout W;
+  int st = wave_layout(common, items, n, W, nullptr);
+  if (st == NFX_OK) *table_bytes = W.total;
+  return st;
+}
+
+int nfx_wave(const nfx_opts* common, const nfx_wave_item* items, int n, void* dev_table, void* host_staging,
+             size_t table_bytes, void* stream) {
+  WaveLayout W;
+  std::vector<Prepared> prep;
+  int st = wave_layout(common, items, n, W, &prep);
+  if (st != NFX_OK) return st;
+  if (dev_table == nullptr || host_staging == nullptr || table_bytes < W.total) {
+    set_error("nfx_wave: table or staging buffer too small: need " + std::to_string(W.total) + " bytes");
+    return NFX_ERR_WORKSPACE;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  const bool f32 = common->precision == NFX_F32;
+  unsigned char* host = (unsigned char*)host_staging;
+  if (f32)
+    wave_items<float>(common, items, n, prep, W, host);
+  else
+    wave_items<double>(common, items, n, prep, W, host);
+  cudaError_t e = cudaMemcpyAsync(dev_table, host_staging, W.total, cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return cuda_fail(e, "nfx_wave table upload");
+  char* tab = (char*)dev_table;
+  const int dim = common->dim;
+  const int64_t tot_pad = deconv_total(items, n, 2, dim, true);
+  const int64_t tot_shuffle = deconv_total(items, n, 1, dim, false);
+  // type 2: deconvolve + zero-pad every grid in one launch, then the FFTs
+  if (W.n2 > 0) {
+    e = f32 ? launch_deconv_batch<float>(true, tab + W.off_pad, W.n2, tot_pad, s)
+            : launch_deconv_batch<double>(true, tab + W.off_pad, W.n2, tot_pad, s);
+    if (e != cudaSuccess) return cuda_fail(e, "nfx_wave zero-pad");
+    for (int i = 0; i < n; ++i)
+      if (items[i].kind == 2) {
+        st = nfx_fft(common->precision, dim, items[i].nf, 1, items[i].fw, items[i].fft_sign, stream);
+        if (st != NFX_OK) return st;
+      }
+  }
+  // every problem's sort; zeroed grids for the spreads
+  for (int i = 0; i < n; ++i) {
+    const Prepared& P = prep[i];
+    const nfx_wave_item& it = items[i];
+    st = nfx_sort_points(&P.o, it.x, it.y, it.z, it.M, it.workspace, it.workspace_bytes, stream);
+    if (st != NFX_OK) return st;
+    if (it.kind == 1) {
+      e = cudaMemsetAsync(it.fw, 0, (size_t)grid_cells(P.g) * 2 * real_bytes(common->precision), s);
+      if (e != cudaSuccess) return cuda_fail(e, "nfx_wave grid zeroing");
+    }
+  }
+  // one persistent spread over all type-1 problems, one interp over all type-2 problems
+  for (int kind = 1; kind <= 2; ++kind) {
+    const int np = kind == 1 ? W.n1 : W.n2;
+    if (np == 0) continue;
+    const void* table = tab + (kind == 1 ? W.off_spread : W.off_interp);
+    int* prefix = (int*)(tab + (kind == 1 ? W.off_prefix_s : W.off_prefix_i));
+    if (f32)
+      k_batch_prefix<float><<<1, 32, 0, s>>>((const BatchItem<float>*)table, np, prefix);
+    else
+      k_batch_prefix<double><<<1, 32, 0, s>>>((const BatchItem<double>*)table, np, prefix);
+    const bool sp = kind == 1;
+    const int64_t subs = sp ? W.subs_s : W.subs_i;
+    const size_t smem = sp ? W.smem_s : W.smem_i;
+    const int ns = common->nspread;
+    if (f32)
+      e = dim == 1   ? dispatch_batch<float, 1>(ns, sp, table, np, prefix, subs, smem, s)
+          : dim == 2 ? dispatch_batch<float, 2>(ns, sp, table, np, prefix, subs, smem, s)
+                     : dispatch_batch<float, 3>(ns, sp, table, np, prefix, subs, smem, s);
+    else
+      e = dim == 1   ? dispatch_batch<double, 1>(ns, sp, table, np, prefix, subs, smem, s)
+          : dim == 2 ? dispatch_batch<double, 2>(ns, sp, table, np, prefix, subs, smem, s)
+                     : dispatch_batch<double, 3>(ns, sp, table, np, prefix, subs, smem, s);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, sp ? "nfx_wave spread" : "nfx_wave interp");
+  }
+  // type 1: the FFTs, then deconvolve + crop every problem in one launch
+  if (W.n1 > 0) {
+    for (int i = 0; i < n; ++i)
+      if (items[i].kind == 1) {
+        st = nfx_fft(common->precision, dim, items[i].nf, 1, items[i].fw, items[i].fft_sign, stream);
+        if (st != NFX_OK) return st;
+      }
+    e = f32 ? launch_deconv_batch<float>(false, tab + W.off_shuffle, W.n1, tot_shuffle, s)
+            : launch_deconv_batch<double>(false, tab + W.off_shuffle, W.n1, tot_shuffle, s);
+    if (e != cudaSuccess) return cuda_fail(e, "nfx_wave crop");
+  }
+  return NFX_OK;
 }
 
 size_t nfx_batch_deconv_table_bytes(int precision, int nprob) {

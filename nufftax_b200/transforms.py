@@ -470,11 +470,13 @@ def nufft3d2(x, y, z, f, eps: float = 1e-6, isign: int = -1, upsampfac=2.0):
 # Type 3
 # ---------------------------------------------------------------------------
 def _type3_forward(src: list[torch.Tensor], c2: torch.Tensor, tgt: list[torch.Tensor], nf: tuple[int, ...],
-                   eps: float, isign: int, uf: float) -> torch.Tensor:
+                   eps: float, isign: int, uf: float, ws_alloc=None) -> torch.Tensor:
     """One nfx_nufft3 call: the type-3 scalars on the device, the source sort
     with the rescaling and pre-phase fused in, spread, the inner type 2's
     deconvolution / zero-pad and FFT, the target sort with the phase / phihat
-    factor fused in, interpolation (nufftax/transforms/nufft3.py:216-515)."""
+    factor fused in, interpolation (nufftax/transforms/nufft3.py:216-515).
+    ws_alloc(nbytes), when given, supplies the workspace (a caller's reusable
+    buffer) instead of a fresh allocation."""
     dim = len(src)
     dev = c2.device
     precision = precision_of(c2.dtype)
@@ -491,7 +493,7 @@ def _type3_forward(src: list[torch.Tensor], c2: torch.Tensor, tgt: list[torch.Te
     nbytes = c_size_t(0)
     _lib.check(lib.nfx_nufft3_workspace_bytes(byref(opts), _lib.int3c(nf_in), M, K, nt, byref(nbytes)),
                "nfx_nufft3_workspace_bytes")
-    ws = torch.empty(max(int(nbytes.value), 1), dtype=torch.uint8, device=dev)
+    ws = (ws_alloc or (lambda n: torch.empty(n, dtype=torch.uint8, device=dev)))(max(int(nbytes.value), 1))
     facs = _facs(nf_in, nf, kp, precision, dev)
     out = torch.empty((nt, K), dtype=c2.dtype, device=dev)
     arr = c_void_p * 3

@@ -259,3 +259,74 @@ def test_malformed_request_fails_alone():
         assert r.error is None
         assert rel_l2(r.result.cpu().numpy(), _alone(r).cpu().numpy()) <= 2e-6
     assert server.stats(done)["requests"] == 8
+
+
+@pytest.mark.parametrize("dim,dtype", [(2, torch.complex64), (3, torch.complex64), (2, torch.complex128)])
+def test_wave_entry_point_matches_api(dim, dtype):
+    """nfx_wave: type-1 and type-2 problems of different grids and sizes in one
+    call (one persistent spread and one interp launch) equal the public API
+    transform by transform; the call is made twice with the same buffers."""
+    from ctypes import byref, c_size_t, c_void_p
+
+    from nufftax_b200 import _lib
+    from nufftax_b200._plan import _facs, make_opts, ptr
+    from nufftax_b200.grid import compute_grid_size
+    from nufftax_b200.kernel import compute_kernel_params
+
+    dev = cuda_device()
+    rng = np.random.default_rng(40 + dim)
+    eps = 1e-6 if dtype == torch.complex64 else 1e-9
+    prec = _lib.NFX_F32 if dtype == torch.complex64 else _lib.NFX_F64
+    rdt = torch.float32 if dtype == torch.complex64 else torch.float64
+    kp = compute_kernel_params(eps)
+    lib = _lib.load()
+    n = 7
+    items = (_lib.NfxWaveItem * n)()
+    keep, probs = [], []
+    common = None
+    for i in range(n):
+        kind = 1 + i % 2
+        M = int(rng.integers(0 if i == 3 else 200, 20000))
+        nm = tuple(int(rng.choice([12, 16, 24, 33])) for _ in range(dim))
+        nf = tuple(compute_grid_size(v, 2.0, kp.nspread) for v in nm)
+        o = make_opts(prec, nf, kp, prenorm=True)
+        common = common or o
+        X = [torch.from_numpy(rng.uniform(-np.pi, np.pi, M)).to(dev, rdt) for _ in range(dim)]
+        if kind == 1:
+            src = torch.from_numpy(rng.standard_normal(M) + 1j * rng.standard_normal(M)).to(dev, dtype)
+            out = torch.empty(nm[::-1], dtype=dtype, device=dev)
+        else:
+            src = torch.from_numpy(rng.standard_normal(nm[::-1]) + 1j * rng.standard_normal(nm[::-1])).to(dev, dtype)
+            out = torch.empty(M, dtype=dtype, device=dev)
+        nb_ = c_size_t(0)
+        assert lib.nfx_sort_workspace_bytes(byref(o), M, byref(nb_)) == 0
+        ws = torch.empty(max(nb_.value, 1), dtype=torch.uint8, device=dev)
+        fw = torch.empty(nf[::-1], dtype=dtype, device=dev)
+        facs = _facs(nf, nm, kp, prec, dev)
+        it = items[i]
+        it.kind, it.M = kind, M
+        cs = [x.data_ptr() for x in X] + [None] * (3 - dim)
+        it.x, it.y, it.z = cs
+        it.nf, it.n_modes = _lib.int3(nf), _lib.int3(nm)
+        it.fft_sign = 1 if kind == 1 else -1
+        it.fac = (c_void_p * 3)(*[f.data_ptr() if f is not None else None for f in facs])
+        it.in_, it.out, it.fw = src.data_ptr(), out.data_ptr(), fw.data_ptr()
+        it.workspace, it.workspace_bytes = ws.data_ptr(), ws.numel()
+        keep += [X, src, out, ws, fw, facs]
+        probs.append((kind, X, src, out, nm))
+    tb = c_size_t(0)
+    assert lib.nfx_wave_table_bytes(byref(common), items, n, byref(tb)) == 0, lib.nfx_last_error()
+    table = torch.empty(tb.value, dtype=torch.uint8, device=dev)
+    staging = torch.empty(tb.value, dtype=torch.uint8).pin_memory()
+    st = c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    tol = 2e-6 if dtype == torch.complex64 else 1e-12
+    for rep in range(2):
+        assert lib.nfx_wave(byref(common), items, n, ptr(table), ptr(staging), table.numel(), st) == 0, \
+            lib.nfx_last_error()
+        torch.cuda.synchronize()
+        for kind, X, src, out, nm in probs:
+            if kind == 1:
+                ref = {2: nb.nufft2d1, 3: nb.nufft3d1}[dim](*X, src, nm, eps=eps, isign=1)
+            else:
+                ref = {2: nb.nufft2d2, 3: nb.nufft3d2}[dim](*X, src, eps=eps, isign=-1)
+            assert rel_l2(out.cpu().numpy(), ref.cpu().numpy()) <= tol or (X[0].numel() == 0)
