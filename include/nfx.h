@@ -38,6 +38,19 @@ enum {
 
 enum { NFX_F32 = 0, NFX_F64 = 1 };
 
+/* Threads per point of the spread / interpolation kernels (nfx_opts::spread_mode,
+ * interp_mode).  AUTO: the library's choice (spread: the CTA in 3D when there are
+ * fewer points than grid cells, else a warp; interpolation: a lane group in 3D,
+ * one thread in 1D/2D).  THREAD: one thread per point (interpolation).  GROUP:
+ * one lane group of the power of two >= nspread lanes per point, a lane per
+ * footprint column (interpolation, 2D/3D).  WARP: one warp per point, a lane per
+ * footprint column, runs of same-cell points summed in registers (spread).
+ * CTA: every warp of the CTA on each point, a warp per tile z-plane, no atomics
+ * (spread, 3D, nspread >= 4).  A mode that does not apply to a dimension falls
+ * back to AUTO. */
+enum { NFX_PER_POINT_AUTO = 0, NFX_PER_POINT_THREAD = 1, NFX_PER_POINT_GROUP = 2,
+       NFX_PER_POINT_WARP = 3, NFX_PER_POINT_CTA = 4 };
+
 /* Spreading/interpolation options: the grid, the ES kernel and the tiling.
  * nspread/beta/kc are nufftax's KernelParams (nufftax/core/kernel.py:19-25,
  * computed by compute_kernel_params, kernel.py:165-206).  tile[] = 0 and
@@ -55,6 +68,8 @@ typedef struct nfx_opts {
   int tile[3];         /* bin edge per axis in cells; 0 = default */
   int max_subproblem;  /* points per subproblem; 0 = default (2048 in 3D; in 1D/2D
                           1024, doubled up to 4096 while M / (2 * size) >= 1480) */
+  int spread_mode;     /* NFX_PER_POINT_AUTO, _WARP or _CTA */
+  int interp_mode;     /* NFX_PER_POINT_AUTO, _THREAD or _GROUP */
 } nfx_opts;
 
 /* Library identity and last error of the calling thread. */
@@ -214,6 +229,7 @@ typedef struct nfx_batch_problem {
   int nf[3];
   int tile[3];         /* 0 = default */
   int max_subproblem;  /* 0 = default */
+  int interp_mode;     /* NFX_PER_POINT_*, this problem's interpolation (0 = common's) */
   void* workspace;     /* sort workspace of nfx_sort_workspace_bytes for this problem */
   size_t workspace_bytes;
   const void* src;

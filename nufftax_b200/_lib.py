@@ -23,6 +23,12 @@ NFX_ERR_CUFFT = 4
 NFX_ERR_UNSUPPORTED = 5
 NFX_F32 = 0
 NFX_F64 = 1
+# threads per point of the spread / interpolation (nfx_opts::spread_mode, interp_mode)
+NFX_PER_POINT_AUTO = 0
+NFX_PER_POINT_THREAD = 1
+NFX_PER_POINT_GROUP = 2
+NFX_PER_POINT_WARP = 3
+NFX_PER_POINT_CTA = 4
 
 _STATUS = {
     NFX_ERR_INVALID: ValueError,
@@ -48,6 +54,8 @@ class NfxOpts(ctypes.Structure):
         ("prenorm", c_int),
         ("tile", c_int * 3),
         ("max_subproblem", c_int),
+        ("spread_mode", c_int),
+        ("interp_mode", c_int),
     ]
 
 
@@ -62,6 +70,7 @@ class NfxBatchProblem(ctypes.Structure):
         ("nf", c_int * 3),
         ("tile", c_int * 3),
         ("max_subproblem", c_int),
+        ("interp_mode", c_int),
         ("workspace", c_void_p),
         ("workspace_bytes", c_size_t),
         ("src", c_void_p),

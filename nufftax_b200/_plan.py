@@ -64,15 +64,16 @@ _opts_lock = threading.Lock()
 
 
 def make_opts(precision: int, nf: Sequence[int], kp: KernelParams, prenorm: bool, tile=None,
-              max_subproblem: int = 0) -> _lib.NfxOpts:
+              max_subproblem: int = 0, modes=(0, 0)) -> _lib.NfxOpts:
     """Library options with default tiles filled in; a private copy of a cached
-    struct per (precision, grid, kernel, tiling) key."""
+    struct per (precision, grid, kernel, tiling, threads-per-point modes) key.
+    modes = (spread_mode, interp_mode), NFX_PER_POINT_* (0: the library's choice)."""
     key = (precision, tuple(int(n) for n in nf), int(kp.nspread), float(kp.beta), float(kp.c), bool(prenorm),
-           None if tile is None else tuple(int(t) for t in tile), int(max_subproblem))
+           None if tile is None else tuple(int(t) for t in tile), int(max_subproblem), tuple(modes))
     with _opts_lock:
         o = _opts_cache.get(key)
     if o is None:
-        o = _make_opts(precision, nf, kp, prenorm, tile, max_subproblem)
+        o = _make_opts(precision, nf, kp, prenorm, tile, max_subproblem, modes)
         with _opts_lock:
             if len(_opts_cache) >= 4096:
                 _opts_cache.clear()
@@ -81,7 +82,7 @@ def make_opts(precision: int, nf: Sequence[int], kp: KernelParams, prenorm: bool
 
 
 def _make_opts(precision: int, nf: Sequence[int], kp: KernelParams, prenorm: bool, tile,
-               max_subproblem: int) -> _lib.NfxOpts:
+               max_subproblem: int, modes=(0, 0)) -> _lib.NfxOpts:
     o = _lib.NfxOpts()
     o.precision = precision
     o.dim = len(nf)
@@ -92,6 +93,7 @@ def _make_opts(precision: int, nf: Sequence[int], kp: KernelParams, prenorm: boo
     o.prenorm = 1 if prenorm else 0
     o.tile = (c_int * 3)(0, 0, 0) if tile is None else _lib.int3(tile)
     o.max_subproblem = int(max_subproblem)
+    o.spread_mode, o.interp_mode = (int(m) for m in modes)
     lib = _lib.load()
     _lib.check(lib.nfx_default_tiles(byref(o)), "nfx_default_tiles")
     return o
@@ -119,7 +121,7 @@ class PointSort:
     """Bin-sorted non-uniform points on one fine grid."""
 
     def __init__(self, coords: Sequence[torch.Tensor], nf: Sequence[int], kp: KernelParams, prenorm: bool,
-                 tile=None, max_subproblem: int = 0):
+                 tile=None, max_subproblem: int = 0, modes=(0, 0)):
         self.dim = len(coords)
         if self.dim not in (1, 2, 3) or len(nf) != self.dim:
             raise ValueError("coords and nf must have 1, 2 or 3 axes")
@@ -134,7 +136,7 @@ class PointSort:
         self.nf = tuple(int(n) for n in nf)
         self.kp = kp
         self.prenorm = prenorm
-        self.opts = make_opts(self.precision, self.nf, kp, prenorm, tile, max_subproblem)
+        self.opts = make_opts(self.precision, self.nf, kp, prenorm, tile, max_subproblem, modes)
         lib = _lib.load()
         nbytes = c_size_t(0)
         _lib.check(lib.nfx_sort_workspace_bytes(byref(self.opts), self.M, byref(nbytes)), "nfx_sort_workspace_bytes")

@@ -41,7 +41,8 @@ def _fft_sign_type2(isign: int) -> int:
 class BatchPlan:
     def __init__(self, points: Sequence[Sequence[torch.Tensor]], n_modes: Sequence[Sequence[int]], eps: float = 1e-6,
                  isign_type1: int = 1, isign_type2: int = -1, upsampfac: float = 2.0,
-                 dtype: torch.dtype = torch.complex64, tiles=None, max_subproblem=None, graph: bool = True):
+                 dtype: torch.dtype = torch.complex64, tiles=None, max_subproblem=None, interp_modes=None,
+                 graph: bool = True):
         if len(points) == 0 or len(points) != len(n_modes):
             raise ValueError("need one n_modes entry per problem")
         self.P = len(points)
@@ -62,6 +63,7 @@ class BatchPlan:
         self.nf = [tuple(compute_grid_size(n, upsampfac, self.kp.nspread) for n in nm) for nm in self.n_modes]
         tiles = tiles if tiles is not None else [None] * self.P
         maxsub = max_subproblem if max_subproblem is not None else [0] * self.P
+        imodes = interp_modes if interp_modes is not None else [0] * self.P
         self.lib = _lib.load()
         dev = self.device
 
@@ -121,6 +123,7 @@ class BatchPlan:
                 pb.nf = _lib.int3(self.nf[p])
                 pb.tile = o.tile
                 pb.max_subproblem = o.max_subproblem
+                pb.interp_mode = int(imodes[p])
                 pb.workspace = ws.data_ptr()
                 pb.workspace_bytes = ws.numel()
                 pb.src = src.data_ptr()

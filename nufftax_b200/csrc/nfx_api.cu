@@ -183,6 +183,8 @@ static void fill_geom(const nfx_opts* o, Geom& g) {
   g.pitch = choose_pitch(g.pad[0], g.pad[1], o->nspread, o->dim);
   g.nbins = g.nb[0] * g.nb[1] * g.nb[2];
   g.prenorm = o->prenorm;
+  g.spread_mode = o->spread_mode;
+  g.interp_mode = o->interp_mode;
   g.t3_mode = 0;
   g.t3_isign = 0;
   g.t3_beta = g.t3_kc = 0.0;
@@ -224,6 +226,13 @@ static int validate_opts(const nfx_opts* o) {
   }
   if (o->max_subproblem < 0) {
     set_error("max_subproblem must be >= 0");
+    return NFX_ERR_INVALID;
+  }
+  if ((o->spread_mode != NFX_PER_POINT_AUTO && o->spread_mode != NFX_PER_POINT_WARP &&
+       o->spread_mode != NFX_PER_POINT_CTA) ||
+      (o->interp_mode != NFX_PER_POINT_AUTO && o->interp_mode != NFX_PER_POINT_THREAD &&
+       o->interp_mode != NFX_PER_POINT_GROUP)) {
+    set_error("spread_mode must be AUTO, WARP or CTA and interp_mode AUTO, THREAD or GROUP");
     return NFX_ERR_INVALID;
   }
   return NFX_OK;
@@ -579,6 +588,7 @@ static int batch_problem_opts(const nfx_opts* common, const nfx_batch_problem& p
     o.tile[d] = pb.tile[d];
   }
   o.max_subproblem = pb.max_subproblem;
+  if (pb.interp_mode != NFX_PER_POINT_AUTO) o.interp_mode = pb.interp_mode;
   return prepare(&o, pb.M, pb.x, pb.y, pb.z, pb.workspace, pb.workspace_bytes, P);
 }
 

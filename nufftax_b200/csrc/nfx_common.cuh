@@ -209,6 +209,8 @@ struct Geom {
   int pitch;     // shared-memory row pitch along x (>= pad[0])
   int nbins;
   int prenorm;
+  int spread_mode;  // nfx_opts::spread_mode (threads per point of the spread)
+  int interp_mode;  // nfx_opts::interp_mode (threads per point of the interpolation)
   FastDiv tdiv[3];  // division by tile[d]
   // Type 3 fused into the sort (0: off).  1: the points are type-3 sources,
   // rescaled as x' = mod((x - C) / gamma + pi, 2 pi) - pi before the fold, and

@@ -6,6 +6,7 @@
 #include <cstdint>
 #include <string>
 
+#include "nfx.h"
 #include "nfx_common.cuh"
 
 namespace nfx {

@@ -52,12 +52,12 @@ __device__ __forceinline__ unsigned peer_mask(int key, int nbits) {
 
 // Bin of the tile holding the footprint's left cell, and that cell's index
 // inside the tile (both x-fastest), from the point's coordinates.
-template <typename T, int DIM>
+template <typename T, int DIM, bool T3>
 __device__ __forceinline__ void cell_keys(const T (&c)[DIM], const Geom& g, int ns_half, int& kbin, int& kcell) {
   int kb = 0, kc = 0, mb = 1, mc = 1;
 #pragma unroll
   for (int d = 0; d < DIM; ++d) {
-    const T xs = point_fold(c[d], d, g);
+    const T xs = T3 ? point_fold(c[d], d, g) : scaled_coord(c[d], g.nf[d], g.prenorm);
     const int i0w = wrap_index(ceil_to_int(rn_sub(xs, (T)ns_half)), g.nf[d]);
     const int bq = fast_div(i0w, g.tdiv[d]);
     kb += bq * mb;
@@ -106,7 +106,9 @@ constexpr int kRadixChunk = kRadixThreads * kRadixItems;  // elements per chunk 
 // One CTA per chunk of kRadixChunk consecutive points: K = bin << cbits | cell
 // for every point, and the chunk's histogram of digit 0 as row `chunk` of
 // counts (chunk-major, so the row is one coalesced write).
-template <typename T, int DIM>
+// T3: the points are type-3 sources or targets (Geom::t3_mode), a separate
+// instantiation so the common kernel carries no type-3 code.
+template <typename T, int DIM, bool T3>
 __global__ void __launch_bounds__(kRadixThreads) k_sort_keys(const T* __restrict__ x, const T* __restrict__ y,
                                                             const T* __restrict__ z, int M, Geom g, int ns_half,
                                                             int cbits, int dbits, int* __restrict__ K,
@@ -131,7 +133,7 @@ __global__ void __launch_bounds__(kRadixThreads) k_sort_keys(const T* __restrict
     const int p = c0 + u * kRadixThreads + threadIdx.x;
     if (p < M) {
       int kb, kc;
-      cell_keys<T, DIM>(cv[u], g, ns_half, kb, kc);
+      cell_keys<T, DIM, T3>(cv[u], g, ns_half, kb, kc);
       const int key = (kb << cbits) | kc;
       K[p] = key;
       atomicAdd(&s_h[key & mask], 1);
@@ -490,19 +492,20 @@ __device__ __forceinline__ void store_quad(double* o, const double (&r)[4]) {
   reinterpret_cast<double2*>(o)[1] = make_double2(r[2], r[3]);
 }
 
-template <typename T, int DIM>
+constexpr int kCoordItems = 8;  // sorted positions per thread of k_sorted_coords
+
+template <typename T, int DIM, bool T3>
 __global__ void __launch_bounds__(256) k_sorted_coords(const T* __restrict__ x, const T* __restrict__ y,
                                                        const T* __restrict__ z, const int* __restrict__ perm, int M,
                                                        Geom g, int nspread, T* __restrict__ o0, T* __restrict__ o1,
                                                        T* __restrict__ o2, cplx_t<T>* __restrict__ extra) {
-  const T* cs[3] = {x, y, z};
-  T* os[3] = {o0, o1, o2};
+  constexpr int Q = kCoordItems;
   // trapezoid nodes and weights phi(z_q) w_q of the type-3 targets' phihat
   __shared__ double s_qw[kMaxQuad];
   const double j2 = nspread / 2.0;
   const int nq = min(max((int)(4 + 3.0 * j2), 20), kMaxQuad);
   const double dz = 2.0 * j2 / (nq - 1);
-  if (g.t3_mode == 2) {
+  if (T3 && g.t3_mode == 2) {
     for (int q = threadIdx.x; q < nq; q += blockDim.x) {
       const double zq = -j2 + q * dz;
       const double arg = 1.0 - g.t3_kc * zq * zq;
@@ -511,41 +514,52 @@ __global__ void __launch_bounds__(256) k_sorted_coords(const T* __restrict__ x, 
     }
     __syncthreads();
   }
-  const int nquad = (M + 3) / 4;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nquad; t += gridDim.x * blockDim.x) {
-    const int i0 = 4 * t;
-    int p[4];
-    if (i0 + 3 < M) {
-      const int4 v = *reinterpret_cast<const int4*>(perm + i0);
-      p[0] = v.x;
-      p[1] = v.y;
-      p[2] = v.z;
-      p[3] = v.w;
+  const int ngroups = (M + Q - 1) / Q;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ngroups; t += gridDim.x * blockDim.x) {
+    const int i0 = Q * t;
+    int p[Q];
+    if (i0 + Q - 1 < M) {
+#pragma unroll
+      for (int h = 0; h < Q / 4; ++h) {
+        const int4 v = *reinterpret_cast<const int4*>(perm + i0 + 4 * h);  // 16-byte aligned
+        p[4 * h] = v.x;
+        p[4 * h + 1] = v.y;
+        p[4 * h + 2] = v.z;
+        p[4 * h + 3] = v.w;
+      }
     } else {
 #pragma unroll
-      for (int j = 0; j < 4; ++j) p[j] = i0 + j < M ? perm[i0 + j] : -1;
+      for (int j = 0; j < Q; ++j) p[j] = i0 + j < M ? perm[i0 + j] : -1;
     }
-    T v[DIM][4];
+    // every gather of the group in flight before any use
+    T v[DIM][Q];
 #pragma unroll
-    for (int d = 0; d < DIM; ++d)
-#pragma unroll
-      for (int j = 0; j < 4; ++j) v[d][j] = p[j] >= 0 ? cs[d][p[j]] : (T)0;
+    for (int j = 0; j < Q; ++j) {
+      v[0][j] = p[j] >= 0 ? x[p[j]] : (T)0;
+      if (DIM > 1) v[DIM > 1 ? 1 : 0][j] = p[j] >= 0 ? y[p[j]] : (T)0;
+      if (DIM > 2) v[DIM > 2 ? 2 : 0][j] = p[j] >= 0 ? z[p[j]] : (T)0;
+    }
 #pragma unroll
     for (int d = 0; d < DIM; ++d) {
-      T r[4];
+      T* od = d == 0 ? o0 : (d == 1 ? o1 : o2);
+      T r[Q];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) r[j] = point_fold(v[d][j], d, g);
-      if (i0 + 3 < M) {
-        store_quad(os[d] + i0, r);  // 16-byte aligned: 256-aligned arrays, i0 % 4 == 0
+      for (int j = 0; j < Q; ++j) r[j] = T3 ? point_fold(v[d][j], d, g) : scaled_coord(v[d][j], g.nf[d], g.prenorm);
+      if (i0 + Q - 1 < M) {
+#pragma unroll
+        for (int h = 0; h < Q / 4; ++h) {
+          const T rq[4] = {r[4 * h], r[4 * h + 1], r[4 * h + 2], r[4 * h + 3]};
+          store_quad(od + i0 + 4 * h, rq);  // 16-byte aligned: 256-aligned arrays, i0 % 8 == 0
+        }
       } else {
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
-          if (p[j] >= 0) os[d][i0 + j] = r[j];
+        for (int j = 0; j < Q; ++j)
+          if (p[j] >= 0) od[i0 + j] = r[j];
       }
     }
-    if (g.t3_mode != 0) {
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
+    if constexpr (T3) {
+#pragma unroll 1
+      for (int j = 0; j < Q; ++j) {
         if (p[j] < 0) continue;
         T xr[3] = {(T)0, (T)0, (T)0};
 #pragma unroll
@@ -599,7 +613,10 @@ cudaError_t launch_sort(const SortLayout& L, const Geom& g, int ns, const void* 
     if (e == cudaSuccess) e = prefer_max_smem(reinterpret_cast<const void*>(scatter));
     if (e != cudaSuccess) return e;
     const unsigned scan_grid = (unsigned)((B + kScanDigits - 1) / kScanDigits);
-    auto keys = g.dim == 1 ? k_sort_keys<T, 1> : (g.dim == 2 ? k_sort_keys<T, 2> : k_sort_keys<T, 3>);
+    auto keys = g.t3_mode != 0
+                    ? (g.dim == 1 ? k_sort_keys<T, 1, true> : (g.dim == 2 ? k_sort_keys<T, 2, true> : k_sort_keys<T, 3, true>))
+                    : (g.dim == 1 ? k_sort_keys<T, 1, false>
+                                  : (g.dim == 2 ? k_sort_keys<T, 2, false> : k_sort_keys<T, 3, false>));
     keys<<<L.nchunks, kRadixThreads, hist_smem, st>>>((const T*)x, (const T*)y, (const T*)z, (int)M, g, ns / 2,
                                                       L.cbits, L.dbits, P.keys, P.counts);
     // ping-pong so that the last pass writes (keys_sorted, perm)
@@ -622,8 +639,13 @@ cudaError_t launch_sort(const SortLayout& L, const Geom& g, int ns, const void* 
   }
   const int bgrid = (int)std::max<int64_t>(1, std::min<int64_t>((M / 4 + 256) / 256, (int64_t)num_sms() * 8));
   if (M > 0) {
-    auto sc = g.dim == 1 ? k_sorted_coords<T, 1> : (g.dim == 2 ? k_sorted_coords<T, 2> : k_sorted_coords<T, 3>);
-    sc<<<bgrid, 256, 0, st>>>((const T*)x, (const T*)y, (const T*)z, P.perm, (int)M, g, ns, (T*)P.coord[0],
+    auto sc = g.t3_mode != 0 ? (g.dim == 1 ? k_sorted_coords<T, 1, true>
+                                           : (g.dim == 2 ? k_sorted_coords<T, 2, true> : k_sorted_coords<T, 3, true>))
+                             : (g.dim == 1 ? k_sorted_coords<T, 1, false>
+                                           : (g.dim == 2 ? k_sorted_coords<T, 2, false> : k_sorted_coords<T, 3, false>));
+    const int cgrid =
+        (int)std::max<int64_t>(1, std::min<int64_t>((M / kCoordItems + 256) / 256, (int64_t)num_sms() * 8));
+    sc<<<cgrid, 256, 0, st>>>((const T*)x, (const T*)y, (const T*)z, P.perm, (int)M, g, ns, (T*)P.coord[0],
                               (T*)P.coord[1], (T*)P.coord[2], (cplx_t<T>*)P.extra);
   }
   k_bin_bounds<<<bgrid, 256, 0, st>>>(P.keys_sorted, (int)M, L.cbits, g.nbins, P.bin_start);

@@ -777,14 +777,14 @@ __device__ __forceinline__ void stage_tile(const Geom& g, const int o[3], const 
 }
 
 // ---------------------------------------------------------------------------
-// 3D interpolation, one lane group per point.  GL lanes (the power
+// Interpolation with one lane group per point (2D and 3D).  GL lanes (the power
 // of two >= NS) share a point: lane kx = lane % GL reads footprint column kx of
-// every (ky, kz) row.  The 32 / GL points of one warp instruction are
-// consecutive in cell order, so their rows overlap in shared memory (few
-// wavefronts; thread-per-point reads of 32 scattered footprints conflicted on
-// about half of theirs).  Each lane computes only its own column's weight per
-// axis; the y and z weights reach the other lanes of the group by shuffles, and
-// the group sums its columns with a butterfly of shuffles.
+// every row (ky, or (ky, kz) in 3D).  The 32 / GL points of one warp
+// instruction are consecutive in cell order, so their rows overlap in shared
+// memory (few wavefronts; thread-per-point reads of 32 scattered footprints
+// conflict on many of theirs).  Each lane computes only its own column's weight
+// per axis; the other axes' weights reach the group's lanes by shuffles, and the
+// group sums its columns with a butterfly of shuffles.
 // ---------------------------------------------------------------------------
 template <int NS>
 __host__ __device__ constexpr int group_lanes() {
@@ -808,14 +808,14 @@ __device__ __forceinline__ T axis_weight_q(const PointArgs<T>& a, const float (&
 
 // Left cells and tile offset of a point with folded coordinates xv (false:
 // outside its bin's tile, see footprint).
-template <typename T, int NS>
+template <typename T, int DIM, int NS>
 __device__ __forceinline__ bool group_point(const PointArgs<T>& a, const T (&xv)[3], const int o[3], int row,
                                             int plane, int& off, T (&xs)[3], int (&i0)[3]) {
   const Geom& g = a.g;
   bool inside = true;
   off = 0;
 #pragma unroll
-  for (int d = 0; d < 3; ++d) {
+  for (int d = 0; d < DIM; ++d) {
     xs[d] = xv[d];
     i0[d] = left_cell<T, NS>(xs[d]);
     const int l = wrap_index(i0[d], g.nf[d]) - o[d];
@@ -842,14 +842,14 @@ __device__ __forceinline__ int round_perm(const SortView& s, int kb, int k1) {
   return k < k1 ? s.perm[k] : -1;
 }
 
-template <typename T>
+template <typename T, int DIM>
 __device__ __forceinline__ void round_coords(const PointArgs<T>& a, int kb, int k1, T (&xv)[3]) {
   const int k = kb + (threadIdx.x & 31);
 #pragma unroll
-  for (int d = 0; d < 3; ++d) xv[d] = k < k1 ? sorted_coord(a, d, k) : (T)0;
+  for (int d = 0; d < 3; ++d) xv[d] = (d < DIM && k < k1) ? sorted_coord(a, d, k) : (T)0;
 }
 
-template <typename T, int NS>
+template <typename T, int DIM, int NS>
 __device__ __forceinline__ WarpPoints<T> warp_points(const PointArgs<T>& a, int p, const T (&xv)[3], const int o[3],
                                                      int row, int plane) {
   WarpPoints<T> w;
@@ -862,13 +862,13 @@ __device__ __forceinline__ WarpPoints<T> warp_points(const PointArgs<T>& a, int 
   }
   if (p >= 0) {
     int off;
-    const bool inside = group_point<T, NS>(a, xv, o, row, plane, off, w.xs, w.i0);
+    const bool inside = group_point<T, DIM, NS>(a, xv, o, row, plane, off, w.xs, w.i0);
     w.off = inside ? off : -1;
   }
   return w;
 }
 
-template <typename T>
+template <typename T, int DIM>
 __device__ __forceinline__ WarpPoints<T> group_take(const WarpPoints<T>& w, int src) {
   constexpr unsigned kAll = 0xffffffffu;
   WarpPoints<T> r;
@@ -876,15 +876,15 @@ __device__ __forceinline__ WarpPoints<T> group_take(const WarpPoints<T>& w, int 
   r.off = __shfl_sync(kAll, w.off, src);
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    r.xs[d] = __shfl_sync(kAll, w.xs[d], src);
-    r.i0[d] = __shfl_sync(kAll, w.i0[d], src);
+    r.xs[d] = d < DIM ? __shfl_sync(kAll, w.xs[d], src) : (T)0;
+    r.i0[d] = d < DIM ? __shfl_sync(kAll, w.i0[d], src) : 0;
   }
   return r;
 }
 
-template <typename T, int NS, int NW>
-__device__ __forceinline__ void interp3_group(const PointArgs<T>& a, const cplx_t<T>* __restrict__ fw,
-                                              cplx_t<T>* __restrict__ cout, int sidx, unsigned char* smem_raw) {
+template <typename T, int DIM, int NS, int NW>
+__device__ __forceinline__ void interp_group(const PointArgs<T>& a, const cplx_t<T>* __restrict__ fw,
+                                             cplx_t<T>* __restrict__ cout, int sidx, unsigned char* smem_raw) {
   using CT = cplx_t<T>;
   constexpr int GL = group_lanes<NS>();
   constexpr int PPW = 32 / GL;
@@ -919,12 +919,12 @@ __device__ __forceinline__ void interp3_group(const PointArgs<T>& a, const cplx_
     constexpr int kStep = NW * 32;
     int p_cur = round_perm(a.s, k0 + warp * 32, k1);
     T x_cur[3];
-    round_coords(a, k0 + warp * 32, k1, x_cur);
+    round_coords<T, DIM>(a, k0 + warp * 32, k1, x_cur);
     for (int kb = k0 + warp * 32; kb < k1; kb += kStep) {  // warp-uniform
       const int p_next = round_perm(a.s, kb + kStep, k1);
       T x_next[3];
-      round_coords(a, kb + kStep, k1, x_next);
-      const WarpPoints<T> wp = warp_points<T, NS>(a, p_cur, x_cur, o, row, plane);
+      round_coords<T, DIM>(a, kb + kStep, k1, x_next);
+      const WarpPoints<T> wp = warp_points<T, DIM, NS>(a, p_cur, x_cur, o, row, plane);
       p_cur = p_next;
 #pragma unroll
       for (int d = 0; d < 3; ++d) x_cur[d] = x_next[d];
@@ -932,32 +932,47 @@ __device__ __forceinline__ void interp3_group(const PointArgs<T>& a, const cplx_
       for (int j0 = 0; j0 < npts; j0 += PPW) {
         const int j = j0 + lane / GL;
         const bool valid = j < npts;
-        const WarpPoints<T> pt = group_take(wp, valid ? j : 0);
+        const WarpPoints<T> pt = group_take<T, DIM>(wp, valid ? j : 0);
         const bool on = col_on && pt.off >= 0;
         const T wx = axis_weight_q<T, NS>(a, cq, pt.i0[0], pt.xs[0], kx);
         const T wyq = axis_weight_q<T, NS>(a, cq, pt.i0[1], pt.xs[1], kx);
-        const T wzq = axis_weight_q<T, NS>(a, cq, pt.i0[2], pt.xs[2], kx);
-        T wy[NS], wz[NS];
+        T wy[NS];
 #pragma unroll
-        for (int q = 0; q < NS; ++q) {
-          wy[q] = __shfl_sync(kAll, wyq, leader + q);
-          wz[q] = __shfl_sync(kAll, wzq, leader + q);
-        }
+        for (int q = 0; q < NS; ++q) wy[q] = __shfl_sync(kAll, wyq, leader + q);
         CT s;
         s.x = s.y = (T)0;
-        if (on) {
-          const CT* base = s_tile + pt.off + kx;
-          // one independent accumulator per z plane: NS chains in flight
-          CT acc[NS];
+        if constexpr (DIM == 3) {
+          const T wzq = axis_weight_q<T, NS>(a, cq, pt.i0[2], pt.xs[2], kx);
+          T wz[NS];
 #pragma unroll
-          for (int kz = 0; kz < NS; ++kz) acc[kz].x = acc[kz].y = (T)0;
+          for (int q = 0; q < NS; ++q) wz[q] = __shfl_sync(kAll, wzq, leader + q);
+          if (on) {
+            const CT* base = s_tile + pt.off + kx;
+            // one independent accumulator per z plane: NS chains in flight
+            CT acc[NS];
 #pragma unroll
-          for (int ky = 0; ky < NS; ++ky) {
+            for (int kz = 0; kz < NS; ++kz) acc[kz].x = acc[kz].y = (T)0;
 #pragma unroll
-            for (int kz = 0; kz < NS; ++kz) acc[kz] = fma2(splat2(wy[ky]), base[kz * plane + ky * row], acc[kz]);
+            for (int ky = 0; ky < NS; ++ky) {
+#pragma unroll
+              for (int kz = 0; kz < NS; ++kz) acc[kz] = fma2(splat2(wy[ky]), base[kz * plane + ky * row], acc[kz]);
+            }
+#pragma unroll
+            for (int kz = 0; kz < NS; ++kz) s = fma2(splat2(wz[kz]), acc[kz], s);
           }
+        } else {
+          if (on) {
+            const CT* base = s_tile + pt.off + kx;
+            CT s1;
+            s1.x = s1.y = (T)0;  // two chains
 #pragma unroll
-          for (int kz = 0; kz < NS; ++kz) s = fma2(splat2(wz[kz]), acc[kz], s);
+            for (int ky = 0; ky < NS; ky += 2) {
+              s = fma2(splat2(wy[ky]), base[ky * row], s);
+              s1 = fma2(splat2(wy[ky + 1]), base[(ky + 1) * row], s1);
+            }
+            s.x += s1.x;
+            s.y += s1.y;
+          }
         }
         T sr = on ? s.x * wx : (T)0, si = on ? s.y * wx : (T)0;
 #pragma unroll
@@ -979,13 +994,24 @@ __device__ __forceinline__ void interp3_group(const PointArgs<T>& a, const cplx_
 // ---------------------------------------------------------------------------
 // Interp
 // ---------------------------------------------------------------------------
-template <typename T, int DIM, int NS, int NW>
+// Threads per point of the interpolation: one lane group (the 3D default) or
+// one thread.  MODE is the variant compiled into a kernel (NFX_PER_POINT_GROUP
+// or _THREAD), or NFX_PER_POINT_AUTO to choose per problem at run time from
+// Geom::interp_mode (the batched kernel).
+template <int DIM>
+__host__ __device__ __forceinline__ bool interp_by_group(int mode) {
+  return DIM >= 2 && (mode == NFX_PER_POINT_GROUP || (mode == NFX_PER_POINT_AUTO && DIM == 3));
+}
+
+template <typename T, int DIM, int NS, int NW, int MODE = NFX_PER_POINT_AUTO>
 __device__ __forceinline__ void interp_subproblem(const PointArgs<T>& a, const cplx_t<T>* __restrict__ fw,
                                                   cplx_t<T>* __restrict__ cout, int sidx, unsigned char* smem_raw) {
   using CT = cplx_t<T>;
-  if constexpr (DIM == 3) {
-    interp3_group<T, NS, NW>(a, fw, cout, sidx, smem_raw);
-    return;
+  if constexpr (DIM >= 2 && MODE != NFX_PER_POINT_THREAD) {
+    if (MODE == NFX_PER_POINT_GROUP || interp_by_group<DIM>(a.g.interp_mode)) {
+      interp_group<T, DIM, NS, NW>(a, fw, cout, sidx, smem_raw);
+      return;
+    }
   }
   CT* s_tile = reinterpret_cast<CT*>(smem_raw);
   const Geom& g = a.g;
@@ -1079,13 +1105,13 @@ __device__ __forceinline__ void interp_subproblem(const PointArgs<T>& a, const c
   }
 }
 
-template <typename T, int DIM, int NS, int NW>
+template <typename T, int DIM, int NS, int NW, int MODE>
 __global__ void __launch_bounds__(NW * 32) k_interp(PointArgs<T> a, const cplx_t<T>* __restrict__ fw,
                                                     cplx_t<T>* __restrict__ cout) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int nsub = *a.s.nsub;
   for (int sidx = blockIdx.x; sidx < nsub; sidx += gridDim.x)
-    interp_subproblem<T, DIM, NS, NW>(a, fw, cout, sidx, smem_raw);
+    interp_subproblem<T, DIM, NS, NW, MODE>(a, fw, cout, sidx, smem_raw);
 }
 
 // ---------------------------------------------------------------------------
@@ -1320,9 +1346,12 @@ struct Launch {
   static cudaError_t spread(const PointArgs<T>& a, const cplx_t<T>* c, cplx_t<T>* fw, cudaStream_t st) {
     int grid = 0;
     if constexpr (DIM == 3 && NS >= 4) {
-      // points sparser than grid cells: runs of same-cell points are rare, and
-      // the plane-owner spread avoids shared-memory atomics altogether
-      if (a.M < (int64_t)a.g.nf[0] * a.g.nf[1] * a.g.nf[2]) {
+      // threads per point (Geom::spread_mode): the whole CTA (warps own tile
+      // planes; by default when points are sparser than grid cells: runs of
+      // same-cell points are rare, and the plane-owner spread needs no
+      // shared-memory atomics) or one warp (lanes own footprint columns)
+      const bool sparse = a.M < (int64_t)a.g.nf[0] * a.g.nf[1] * a.g.nf[2];
+      if (a.g.spread_mode == NFX_PER_POINT_CTA || (a.g.spread_mode == NFX_PER_POINT_AUTO && sparse)) {
         const size_t smem = owner_smem_bytes(sizeof(T), NS, NW, a.g);
         cudaError_t e = prep(k_spread_owner<T, NS, NW>, smem, grid, a.s.max_subs);
         if (e != cudaSuccess) return e;
@@ -1336,13 +1365,20 @@ struct Launch {
     k_spread<T, DIM, NS, NW><<<grid, NW * 32, smem, st>>>(a, c, fw);
     return cudaGetLastError();
   }
-  static cudaError_t interp(const PointArgs<T>& a, const cplx_t<T>* fw, cplx_t<T>* out, cudaStream_t st) {
+  template <int MODE>
+  static cudaError_t interp_as(const PointArgs<T>& a, const cplx_t<T>* fw, cplx_t<T>* out, cudaStream_t st) {
     size_t smem = tile_smem(a.g);
     int grid = 0;
-    cudaError_t e = prep(k_interp<T, DIM, NS, NW>, smem, grid, a.s.max_subs);
+    cudaError_t e = prep(k_interp<T, DIM, NS, NW, MODE>, smem, grid, a.s.max_subs);
     if (e != cudaSuccess) return e;
-    k_interp<T, DIM, NS, NW><<<grid, NW * 32, smem, st>>>(a, fw, out);
+    k_interp<T, DIM, NS, NW, MODE><<<grid, NW * 32, smem, st>>>(a, fw, out);
     return cudaGetLastError();
+  }
+  static cudaError_t interp(const PointArgs<T>& a, const cplx_t<T>* fw, cplx_t<T>* out, cudaStream_t st) {
+    if constexpr (DIM >= 2) {
+      if (interp_by_group<DIM>(a.g.interp_mode)) return interp_as<NFX_PER_POINT_GROUP>(a, fw, out, st);
+    }
+    return interp_as<NFX_PER_POINT_THREAD>(a, fw, out, st);
   }
   static cudaError_t grad(const PointArgs<T>& a, const cplx_t<T>* G, const cplx_t<T>* V, cplx_t<T>* oi, T* dx, T* dy,
                           T* dz, cudaStream_t st) {

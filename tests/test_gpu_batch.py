@@ -83,11 +83,46 @@ def test_autotune_returns_valid_tiling():
     dev = cuda_device()
     x, y = [torch.from_numpy(rng.uniform(-np.pi, np.pi, 50000).astype(np.float32)).to(dev) for _ in range(2)]
     kp = nb.compute_kernel_params(1e-5)
-    tile, maxsub = tune([x, y], (256, 256), kp)
-    assert len(tile) == 2 and maxsub > 0
-    # the tuned tiling gives the same spread
-    ps_a = nb.PointSort([x, y], (256, 256), kp, prenorm=True, tile=tile, max_subproblem=maxsub)
+    timings = []
+    tile, maxsub, modes = tune([x, y], (256, 256), kp, timings=timings)
+    assert len(tile) == 2 and maxsub > 0 and len(modes) == 2
+    # both threads-per-point modes of the 2D interpolation were timed
+    assert {m[1] for _, _, _, m in timings} == {nb._lib.NFX_PER_POINT_THREAD, nb._lib.NFX_PER_POINT_GROUP}
+    # the tuned choice gives the same spread and interpolation
+    ps_a = nb.PointSort([x, y], (256, 256), kp, prenorm=True, tile=tile, max_subproblem=maxsub, modes=modes)
     ps_b = nb.PointSort([x, y], (256, 256), kp, prenorm=True)
     c = torch.ones((1, 50000), dtype=torch.complex64, device=dev)
-    assert rel_l2(ps_a.spread(c).cpu().numpy(), ps_b.spread(c).cpu().numpy()) < 2e-6
-    assert tune([x, y], (256, 256), kp) == (tile, maxsub)
+    fa, fb = ps_a.spread(c), ps_b.spread(c)
+    assert rel_l2(fa.cpu().numpy(), fb.cpu().numpy()) < 2e-6
+    assert rel_l2(ps_a.interp(fa).cpu().numpy(), ps_b.interp(fb).cpu().numpy()) < 2e-6
+    assert tune([x, y], (256, 256), kp) == (tile, maxsub, modes)
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("prec", ["c64", "c128"])
+def test_threads_per_point_modes_agree_with_oracle(dim, prec):
+    """Every threads-per-point mode of spread and interpolation (one thread /
+    lane group per point; one warp / the CTA per point) matches the oracle."""
+    from oracle import nufft_oracle as O
+
+    rng = np.random.default_rng(30 + dim)
+    dev = cuda_device()
+    rdt, cdt = (np.float32, np.complex64) if prec == "c64" else (np.float64, np.complex128)
+    tol = 2e-6 if prec == "c64" else 1e-12
+    kp = nb.compute_kernel_params(1e-6 if prec == "c64" else 1e-12)
+    nf = (64, 48) if dim == 2 else (32, 24, 20)
+    M = 20000
+    X = [rng.uniform(-np.pi, np.pi, M).astype(rdt) for _ in range(dim)]
+    c = (rng.standard_normal((1, M)) + 1j * rng.standard_normal((1, M))).astype(cdt)
+    g = (rng.standard_normal((1,) + nf[::-1]) + 1j * rng.standard_normal((1,) + nf[::-1])).astype(cdt)
+    ref_s = O.spread(X, c, nf, kp)
+    ref_i = O.interp(X, g, kp)
+    L = nb._lib
+    spread_modes = [L.NFX_PER_POINT_WARP] + ([L.NFX_PER_POINT_CTA] if dim == 3 else [])
+    for sm in spread_modes:
+        for im in (L.NFX_PER_POINT_THREAD, L.NFX_PER_POINT_GROUP):
+            ps = nb.PointSort([torch.from_numpy(x).to(dev) for x in X], nf, kp, prenorm=False, modes=(sm, im))
+            fw = ps.spread(torch.from_numpy(c).to(dev)).cpu().numpy()
+            ci = ps.interp(torch.from_numpy(g).to(dev)).cpu().numpy()
+            assert rel_l2(fw, ref_s) < tol, (sm, im)
+            assert rel_l2(ci, ref_i) < tol, (sm, im)

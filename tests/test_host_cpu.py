@@ -225,11 +225,11 @@ def test_autotune_cache_round_trip(tmp_path, monkeypatch):
     monkeypatch.setenv("NUFFTAX_B200_TUNE_CACHE", str(path))
     monkeypatch.setattr(autotune, "_cache", {})
     monkeypatch.setattr(autotune, "_loaded", True)
-    autotune._cache["d2-uf2-ns8-f32-rho2-clu"] = ((32, 32), 2048)
+    autotune._cache["d2-uf2-ns8-f32-rho2-clu"] = ((32, 32), 2048, (3, 2))
     autotune._save()
     monkeypatch.setattr(autotune, "_cache", {})
     monkeypatch.setattr(autotune, "_loaded", False)
-    assert autotune.cached() == {"d2-uf2-ns8-f32-rho2-clu": ((32, 32), 2048)}
+    assert autotune.cached() == {"d2-uf2-ns8-f32-rho2-clu": ((32, 32), 2048, (3, 2))}
     path.write_text("{not json")
     monkeypatch.setattr(autotune, "_cache", {})
     monkeypatch.setattr(autotune, "_loaded", False)
