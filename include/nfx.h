@@ -77,6 +77,14 @@ int nfx_version(void);
 const char* nfx_last_error(void);
 int nfx_num_sms(void);
 
+/* Status bits of the current GPU that kernels set when a bounded wait gave up
+ * instead of hanging: NFX_STATUS_TMA_TIMEOUT, a tile copy of the interpolation
+ * (staged by TMA) did not land within 0.5 s and that CTA stopped, leaving its
+ * outputs incomplete.  nfx_device_status synchronizes the device, writes the
+ * bits to *status and clears them.  (No counterpart in the reference.) */
+enum { NFX_STATUS_TMA_TIMEOUT = 1 };
+int nfx_device_status(int* status);
+
 /* Polynomial form of the ES weights used by the float kernels (no counterpart
  * in the reference, which evaluates exp/sqrt): coefficients a[q][d] of
  * phi(q - (v + ns - 1) / 2) as a degree-`degree` polynomial in v in [-1, 1],

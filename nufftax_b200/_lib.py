@@ -29,6 +29,7 @@ NFX_PER_POINT_THREAD = 1
 NFX_PER_POINT_GROUP = 2
 NFX_PER_POINT_WARP = 3
 NFX_PER_POINT_CTA = 4
+NFX_STATUS_TMA_TIMEOUT = 1
 
 _STATUS = {
     NFX_ERR_INVALID: ValueError,
@@ -110,6 +111,7 @@ _SIGNATURES = {
     "nfx_version": ([], c_int),
     "nfx_last_error": ([], ctypes.c_char_p),
     "nfx_num_sms": ([], c_int),
+    "nfx_device_status": ([POINTER(c_int)], c_int),
     "nfx_es_poly": ([c_int, c_double, c_double, POINTER(ctypes.c_float), POINTER(c_int), POINTER(c_double)], c_int),
     "nfx_default_tiles": ([POINTER(NfxOpts)], c_int),
     "nfx_sort_workspace_bytes": ([POINTER(NfxOpts), c_int64, POINTER(c_size_t)], c_int),
@@ -220,3 +222,11 @@ def int3c(vals) -> ctypes.Array:
             _int3_cache.clear()
         arr = _int3_cache[key] = int3(key)
     return arr
+
+
+def device_status() -> int:
+    """Status bits of the current GPU (NFX_STATUS_*; 0 when no bounded wait in
+    a kernel gave up), cleared by the read.  Synchronizes the device."""
+    st = c_int(0)
+    check(load().nfx_device_status(ctypes.byref(st)), "nfx_device_status")
+    return int(st.value)

@@ -2,6 +2,7 @@
 #include <algorithm>
 #include <cmath>
 #include <type_traits>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -57,6 +58,75 @@ int num_sms() {
   if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
   cache[dev] = n;
   return n;
+}
+
+// ---- device status word and TMA tensor maps ----------------------------------
+__device__ int g_status_word;
+
+int* device_status_word() {
+  static std::mutex mu;
+  static std::map<int, int*> cache;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = cache.find(dev);
+  if (it != cache.end()) return it->second;
+  void* p = nullptr;
+  if (cudaGetSymbolAddress(&p, g_status_word) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  cache[dev] = (int*)p;
+  return (int*)p;
+}
+
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      p = nullptr;
+    }
+    return (EncodeTiledFn)p;
+  }();
+  return fn;
+}
+
+bool interp_tile_map(CUtensorMap_st* map, size_t real_bytes, int dim, const Geom& g, int n_trans, const void* grid) {
+  const char* env = std::getenv("NFX_INTERP_STAGING");
+  if (env != nullptr && std::strcmp(env, "plain") == 0) return false;
+  if (dim < 2 || n_trans < 1) return false;
+  // 8-byte elements: a complex64 is one, a complex128 two, so x coordinates
+  // (tile origin x * elements per complex) stay even, i.e. 16-byte aligned,
+  // when the tile's x edge is even for complex64.
+  const int per = (int)(2 * real_bytes / 8);
+  if (per == 1 && (g.tile[0] % 2 != 0 || g.pitch % 2 != 0)) return false;
+  const uint64_t row_bytes = (uint64_t)g.nf[0] * 2 * real_bytes;
+  if (row_bytes % 16 != 0 || ((uintptr_t)grid & 15) != 0) return false;
+  if ((int64_t)g.pitch * per > 256 || g.pad[1] > 256 || g.pad[2] > 256) return false;
+  if (g.pitch > g.nf[0] || g.pad[1] > g.nf[1] || (dim == 3 && g.pad[2] > g.nf[2])) return false;
+  EncodeTiledFn enc = encode_tiled();
+  if (enc == nullptr) return false;
+  cuuint64_t dims[4], strides[3];
+  cuuint32_t box[4], estr[4] = {1, 1, 1, 1};
+  int r = 0;
+  dims[r] = (cuuint64_t)g.nf[0] * per, box[r++] = (cuuint32_t)(g.pitch * per);
+  dims[r] = (cuuint64_t)g.nf[1], box[r++] = (cuuint32_t)g.pad[1];
+  if (dim == 3) dims[r] = (cuuint64_t)g.nf[2], box[r++] = (cuuint32_t)g.pad[2];
+  dims[r] = (cuuint64_t)n_trans, box[r++] = 1;
+  strides[0] = row_bytes;
+  strides[1] = row_bytes * (uint64_t)g.nf[1];
+  if (dim == 3) strides[2] = strides[1] * (uint64_t)g.nf[2];
+  const CUresult res = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT64, (cuuint32_t)r, const_cast<void*>(grid), dims, strides,
+                           box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return res == CUDA_SUCCESS;
 }
 
 cudaError_t ensure_smem(const void* fn, size_t smem) {
@@ -839,6 +909,27 @@ int nfx_es_poly(int nspread, double beta, double kc, float* coeffs, int* degree,
 }
 const char* nfx_last_error(void) { return g_last_error.c_str(); }
 int nfx_num_sms(void) { return num_sms(); }
+
+int nfx_device_status(int* status) {
+  using namespace nfx;
+  if (status == nullptr) {
+    set_error("status is NULL");
+    return NFX_ERR_INVALID;
+  }
+  int* w = device_status_word();
+  if (w == nullptr) {
+    set_error("device status word unavailable");
+    return NFX_ERR_CUDA;
+  }
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaMemcpy(status, w, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemset(w, 0, sizeof(int));
+  if (e != cudaSuccess) {
+    set_error(std::string("nfx_device_status: ") + cudaGetErrorString(e));
+    return NFX_ERR_CUDA;
+  }
+  return NFX_OK;
+}
 
 int nfx_default_tiles(nfx_opts* opts) {
   nfx_opts o;

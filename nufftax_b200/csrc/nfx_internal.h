@@ -1,6 +1,7 @@
 // Internal declarations shared by the nufftax_b200 CUDA translation units.
 #pragma once
 
+#include <cuda.h>  // CUtensorMap (type only; the encoder is fetched from the driver at run time)
 #include <cuda_runtime.h>
 #include <cstddef>
 #include <cstdint>
@@ -116,6 +117,19 @@ int64_t fill_deconv_items(int precision, int dim, bool pad, const int* nf, const
 
 int num_sms();
 void set_error(const std::string& msg);
+
+// Tensor map of a fine grid (n_trans x nf3 x nf2 x nf1 complex of 2 * real_bytes
+// bytes) whose box is the interpolation's padded tile (pitch x pad_y [x pad_z] x 1
+// elements of 8 bytes), for TMA staging.  False (no map) when TMA staging is
+// off (NFX_INTERP_STAGING=plain in the environment), the driver lacks the
+// encoder, or the grid or box breaks a TMA rule (16-byte strides and base,
+// box edges <= 256); the caller then stages with plain loads.
+bool interp_tile_map(CUtensorMap* map, size_t real_bytes, int dim, const Geom& g, int n_trans, const void* grid);
+
+// The current device's status word (a __device__ int of this library), or
+// nullptr if its address cannot be had.  Kernels OR NFX_STATUS_* bits into it;
+// nfx_device_status reads and clears it.
+int* device_status_word();
 
 // Warps per CTA of the spread / interp / gradient kernels.
 constexpr int warps_per_cta(size_t real_bytes, int dim, int ns) { return (real_bytes == 8 && dim == 3) ? 4 : 8; }

@@ -24,6 +24,7 @@
 //    interpolated value and all coordinate gradients in one pass.
 #pragma once
 
+
 #include <type_traits>
 
 #include "nfx_internal.h"
@@ -45,6 +46,8 @@ struct PointArgs {
   int64_t M;
   int n_trans;
   int64_t grid_stride;  // complex elements per transform of the fine grid
+  int tma;              // 1: the interpolation stages interior tiles with the kernel's tensor map
+  int* status;          // device status word (nonzero after a bounded wait gave up); set when tma = 1
   Geom g;
   T beta, kc;
   SortView s;
@@ -598,7 +601,7 @@ __device__ __forceinline__ void spread_subproblem(const PointArgs<T>& a, const c
 template <typename T, int DIM, int NS, int NW>
 __global__ void __launch_bounds__(NW * 32) k_spread(PointArgs<T> a, const cplx_t<T>* __restrict__ c,
                                                     cplx_t<T>* __restrict__ fw) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   const int nsub = *a.s.nsub;
   for (int sidx = blockIdx.x; sidx < nsub; sidx += gridDim.x) spread_subproblem<T, DIM, NS, NW>(a, c, fw, sidx, smem_raw);
 }
@@ -748,7 +751,7 @@ __device__ __forceinline__ void spread_subproblem_owner(const PointArgs<T>& a, c
 template <typename T, int NS, int NW>
 __global__ void __launch_bounds__(NW * 32) k_spread_owner(PointArgs<T> a, const cplx_t<T>* __restrict__ c,
                                                           cplx_t<T>* __restrict__ fw) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   const int nsub = *a.s.nsub;
   for (int sidx = blockIdx.x; sidx < nsub; sidx += gridDim.x)
     spread_subproblem_owner<T, NS, NW>(a, c, fw, sidx, smem_raw);
@@ -774,6 +777,101 @@ __device__ __forceinline__ void stage_tile(const Geom& g, const int o[3], const 
     cplx_t<T>* dst = s_tile + lz * plane + ly * row;
     for (int lx = lane; lx < g.pad[0]; lx += 32) dst[lx] = src[wrap_up(o[0] + lx, g.nf[0])];
   }
+}
+
+// ---------------------------------------------------------------------------
+// Tile staging by TMA.  The interpolation's padded tile of a bin whose padded
+// extent lies inside the grid on every axis (no periodic wrap) is one box of
+// the fine grid: one thread issues a cp.async.bulk.tensor load of it from the
+// kernel's tensor map (this GPU's own grid, no multicast) into the tile
+// buffer, completing on an mbarrier; the others wait on the barrier.  Tiles
+// that wrap keep the plain loads (stage_tile).  Box (pitch, pad_y[, pad_z], 1)
+// of elements of 8 bytes (complex64; complex128 as two), coordinates
+// (x, y[, z], transform), so the box lands with the tile's own row pitch.
+// The barrier wait is bounded (kTmaWaitPolls polls and kTmaWaitNs of the
+// global timer, whichever ends first): a wait that gives up records
+// NFX_STATUS_TMA_TIMEOUT in the status word (nfx_device_status) and the CTA
+// stops, so a copy that never lands cannot hang the GPU.
+// ---------------------------------------------------------------------------
+constexpr int kTmaWaitPolls = 1 << 24;
+constexpr unsigned long long kTmaWaitNs = 500000000ull;  // 0.5 s
+
+struct TmaStage {
+  const CUtensorMap* map;
+  unsigned mbar;   // shared-memory address of the barrier
+  unsigned phase;  // parity of the next completion
+};
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void tma_init(uint64_t* mbar) {
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(mbar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ bool tma_wait(unsigned mbar, unsigned phase) {
+  const unsigned long long t0 = global_ns();
+  for (int it = 0; it < kTmaWaitPolls; ++it) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(mbar), "r"(phase)
+        : "memory");
+    if (done) return true;
+    if ((it & 255) == 255 && global_ns() - t0 > kTmaWaitNs) break;
+  }
+  return false;
+}
+
+// Stages transform t's padded tile at origin o into s_tile: by TMA when
+// allowed, the tile does not wrap and the buffer is 128-byte aligned, else with
+// plain loads.  Must be called by every thread of the CTA between barriers;
+// false (for every thread) when a TMA wait gave up, and the caller then stops.
+template <typename T>
+__device__ __forceinline__ bool stage_interp_tile(const PointArgs<T>& a, const int o[3], const cplx_t<T>* grid, int t,
+                                                  cplx_t<T>* s_tile, TmaStage& ts) {
+  const Geom& g = a.g;
+  const bool interior = a.tma && o[0] + g.pitch <= g.nf[0] && o[1] + g.pad[1] <= g.nf[1] &&
+                        (g.dim < 3 || o[2] + g.pad[2] <= g.nf[2]) && (smem_addr(s_tile) & 127u) == 0;
+  if (!interior) {
+    stage_tile<T>(g, o, grid + (int64_t)t * a.grid_stride, s_tile);
+    return true;
+  }
+  if (threadIdx.x == 0) {
+    const unsigned bytes = (unsigned)(sizeof(cplx_t<T>) * g.pitch * g.pad[1] * g.pad[2]);
+    const int x = o[0] * (int)(sizeof(cplx_t<T>) / 8);  // in 8-byte elements
+    const uint64_t map = reinterpret_cast<uint64_t>(ts.map);
+    const unsigned dst = smem_addr(s_tile);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // earlier reads of the buffer before the async write
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(ts.mbar), "r"(bytes) : "memory");
+    if (g.dim == 2)
+      asm volatile(
+          "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+          "[%5];" ::"r"(dst),
+          "l"(map), "r"(x), "r"(o[1]), "r"(t), "r"(ts.mbar)
+          : "memory");
+    else
+      asm volatile(
+          "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+          "%5}], [%6];" ::"r"(dst),
+          "l"(map), "r"(x), "r"(o[1]), "r"(o[2]), "r"(t), "r"(ts.mbar)
+          : "memory");
+  }
+  const bool landed = tma_wait(ts.mbar, ts.phase);
+  ts.phase ^= 1u;
+  if (__syncthreads_and(landed)) return true;
+  if (threadIdx.x == 0) atomicOr(a.status, NFX_STATUS_TMA_TIMEOUT);
+  return false;
 }
 
 // ---------------------------------------------------------------------------
@@ -884,7 +982,8 @@ __device__ __forceinline__ WarpPoints<T> group_take(const WarpPoints<T>& w, int 
 
 template <typename T, int DIM, int NS, int NW>
 __device__ __forceinline__ void interp_group(const PointArgs<T>& a, const cplx_t<T>* __restrict__ fw,
-                                             cplx_t<T>* __restrict__ cout, int sidx, unsigned char* smem_raw) {
+                                             cplx_t<T>* __restrict__ cout, int sidx, unsigned char* smem_raw,
+                                             TmaStage& ts) {
   using CT = cplx_t<T>;
   constexpr int GL = group_lanes<NS>();
   constexpr int PPW = 32 / GL;
@@ -914,7 +1013,7 @@ __device__ __forceinline__ void interp_group(const PointArgs<T>& a, const cplx_t
   bin_origin(g, b, o[0], o[1], o[2]);
   for (int t = 0; t < a.n_trans; ++t) {
     __syncthreads();
-    stage_tile<T>(g, o, fw + (int64_t)t * a.grid_stride, s_tile);
+    if (!stage_interp_tile<T>(a, o, fw, t, s_tile, ts)) return;
     __syncthreads();
     constexpr int kStep = NW * 32;
     int p_cur = round_perm(a.s, k0 + warp * 32, k1);
@@ -1005,11 +1104,12 @@ __host__ __device__ __forceinline__ bool interp_by_group(int mode) {
 
 template <typename T, int DIM, int NS, int NW, int MODE = NFX_PER_POINT_AUTO>
 __device__ __forceinline__ void interp_subproblem(const PointArgs<T>& a, const cplx_t<T>* __restrict__ fw,
-                                                  cplx_t<T>* __restrict__ cout, int sidx, unsigned char* smem_raw) {
+                                                  cplx_t<T>* __restrict__ cout, int sidx, unsigned char* smem_raw,
+                                                  TmaStage& ts) {
   using CT = cplx_t<T>;
   if constexpr (DIM >= 2 && MODE != NFX_PER_POINT_THREAD) {
     if (MODE == NFX_PER_POINT_GROUP || interp_by_group<DIM>(a.g.interp_mode)) {
-      interp_group<T, DIM, NS, NW>(a, fw, cout, sidx, smem_raw);
+      interp_group<T, DIM, NS, NW>(a, fw, cout, sidx, smem_raw, ts);
       return;
     }
   }
@@ -1025,7 +1125,7 @@ __device__ __forceinline__ void interp_subproblem(const PointArgs<T>& a, const c
     bin_origin(g, b, o[0], o[1], o[2]);
     for (int t = 0; t < a.n_trans; ++t) {
       __syncthreads();
-      stage_tile<T>(g, o, fw + (int64_t)t * a.grid_stride, s_tile);
+      if (!stage_interp_tile<T>(a, o, fw, t, s_tile, ts)) return;
       __syncthreads();
       // loads pipelined across iterations: the next iteration's permutation
       // entry and folded coordinates (both in sorted order)
@@ -1107,11 +1207,14 @@ __device__ __forceinline__ void interp_subproblem(const PointArgs<T>& a, const c
 
 template <typename T, int DIM, int NS, int NW, int MODE>
 __global__ void __launch_bounds__(NW * 32) k_interp(PointArgs<T> a, const cplx_t<T>* __restrict__ fw,
-                                                    cplx_t<T>* __restrict__ cout) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+                                                    cplx_t<T>* __restrict__ cout, const __grid_constant__ CUtensorMap tmap) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t mbar;
+  TmaStage ts{&tmap, smem_addr(&mbar), 0u};
+  if (a.tma) tma_init(&mbar);
   const int nsub = *a.s.nsub;
   for (int sidx = blockIdx.x; sidx < nsub; sidx += gridDim.x)
-    interp_subproblem<T, DIM, NS, NW, MODE>(a, fw, cout, sidx, smem_raw);
+    interp_subproblem<T, DIM, NS, NW, MODE>(a, fw, cout, sidx, smem_raw, ts);
 }
 
 // ---------------------------------------------------------------------------
@@ -1142,7 +1245,7 @@ __device__ __forceinline__ int batch_find(const int* __restrict__ prefix, int n,
 template <typename T, int DIM, int NS, int NW>
 __global__ void __launch_bounds__(NW * 32) k_spread_batch(const BatchItem<T>* __restrict__ items, int nitems,
                                                           const int* __restrict__ sub_prefix) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   const int total = sub_prefix[nitems];
   for (int gi = blockIdx.x; gi < total; gi += gridDim.x) {
     const int p = batch_find(sub_prefix, nitems, gi);
@@ -1156,13 +1259,14 @@ __global__ void __launch_bounds__(NW * 32) k_spread_batch(const BatchItem<T>* __
 template <typename T, int DIM, int NS, int NW>
 __global__ void __launch_bounds__(NW * 32) k_interp_batch(const BatchItem<T>* __restrict__ items, int nitems,
                                                           const int* __restrict__ sub_prefix) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   const int total = sub_prefix[nitems];
+  TmaStage ts{nullptr, 0u, 0u};  // batched items stage with plain loads (their PointArgs have tma = 0)
   for (int gi = blockIdx.x; gi < total; gi += gridDim.x) {
     const int p = batch_find(sub_prefix, nitems, gi);
     const BatchItem<T>& it = items[p];
     interp_subproblem<T, DIM, NS, NW>(it.a, (const cplx_t<T>*)it.src, (cplx_t<T>*)it.dst, gi - sub_prefix[p],
-                                      smem_raw);
+                                      smem_raw, ts);
   }
 }
 
@@ -1174,7 +1278,7 @@ __global__ void __launch_bounds__(NW * 32) k_grad(PointArgs<T> a, const cplx_t<T
                                                   const cplx_t<T>* __restrict__ V, cplx_t<T>* __restrict__ out_interp,
                                                   T* __restrict__ dx, T* __restrict__ dy, T* __restrict__ dz) {
   using CT = cplx_t<T>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   CT* s_tile = reinterpret_cast<CT*>(smem_raw);
   const Geom& g = a.g;
   const int row = g.pitch;
@@ -1366,12 +1470,28 @@ struct Launch {
     return cudaGetLastError();
   }
   template <int MODE>
-  static cudaError_t interp_as(const PointArgs<T>& a, const cplx_t<T>* fw, cplx_t<T>* out, cudaStream_t st) {
+  static cudaError_t interp_as(const PointArgs<T>& a0, const cplx_t<T>* fw, cplx_t<T>* out, cudaStream_t st) {
+    PointArgs<T> a = a0;
+    CUtensorMap tmap{};
+    a.tma = 0;
+    if constexpr (DIM >= 2) {
+      // The interpolation only reads the tile, so its row pitch is free: a
+      // complex64 box needs an even one (16-byte rows).
+      Geom gt = a.g;
+      if (sizeof(T) == 4 && (gt.pitch & 1)) ++gt.pitch;
+      if (interp_tile_map(&tmap, sizeof(T), DIM, gt, a.n_trans, fw)) {
+        a.status = device_status_word();
+        if (a.status != nullptr) {
+          a.g = gt;
+          a.tma = 1;
+        }
+      }
+    }
     size_t smem = tile_smem(a.g);
     int grid = 0;
     cudaError_t e = prep(k_interp<T, DIM, NS, NW, MODE>, smem, grid, a.s.max_subs);
     if (e != cudaSuccess) return e;
-    k_interp<T, DIM, NS, NW, MODE><<<grid, NW * 32, smem, st>>>(a, fw, out);
+    k_interp<T, DIM, NS, NW, MODE><<<grid, NW * 32, smem, st>>>(a, fw, out, tmap);
     return cudaGetLastError();
   }
   static cudaError_t interp(const PointArgs<T>& a, const cplx_t<T>* fw, cplx_t<T>* out, cudaStream_t st) {
@@ -1479,6 +1599,8 @@ PointArgs<T> make_args(const Geom& g, double beta, double kc, int64_t M, int n_t
   a.M = M;
   a.n_trans = n_trans;
   a.grid_stride = (int64_t)g.nf[0] * g.nf[1] * g.nf[2];
+  a.tma = 0;
+  a.status = nullptr;
   a.g = g;
   a.beta = (T)beta;
   a.kc = (T)kc;

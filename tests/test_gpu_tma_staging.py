@@ -1,0 +1,83 @@
+"""GPU: the interpolation's TMA tile staging.
+
+Interior tiles are copied by one cp.async.bulk.tensor box load, wrapping tiles
+by plain loads; NFX_INTERP_STAGING=plain forces plain loads everywhere.  Both
+stagings put the same values in the same shared-memory layout, so the outputs
+must be bit-identical, over tilings that do and do not qualify for TMA (odd
+tile edges, odd fine-grid rows, tiles as large as the grid, several
+transforms, complex128), and the device status word must stay 0 (no bounded
+wait gave up).  The TMA result is also checked against the oracle.
+"""
+
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from nufftax_b200 import _lib
+from nufftax_b200._plan import PointSort
+from nufftax_b200.kernel import compute_kernel_params
+from oracle import nufft_oracle as O
+from tests.conftest import cuda_device, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _interp_both(ps, fw):
+    old = os.environ.get("NFX_INTERP_STAGING")
+    try:
+        os.environ["NFX_INTERP_STAGING"] = "plain"
+        plain = ps.interp(fw).clone()
+        os.environ.pop("NFX_INTERP_STAGING")
+        tma = ps.interp(fw).clone()
+    finally:
+        if old is None:
+            os.environ.pop("NFX_INTERP_STAGING", None)
+        else:
+            os.environ["NFX_INTERP_STAGING"] = old
+    return plain, tma
+
+
+CASES = [
+    # dim, nf, tile, M, n_trans, dtype, clustered
+    (2, (256, 192), None, 60_000, 1, np.float32, True),
+    (2, (256, 192), (15, 17), 60_000, 1, np.float32, False),   # odd x edge: plain loads only
+    (2, (250, 130), (32, 16), 40_000, 2, np.float32, False),   # grid edge not a tile multiple
+    (2, (64, 64), (64, 64), 5_000, 1, np.float32, False),      # one tile covers the grid: always wraps
+    (2, (200, 96), None, 30_000, 3, np.float64, True),
+    (3, (48, 40, 36), None, 80_000, 1, np.float32, False),
+    (3, (48, 40, 36), (8, 8, 8), 80_000, 2, np.float32, True),
+    (3, (32, 32, 32), None, 20_000, 1, np.float64, False),
+]
+
+
+@pytest.mark.parametrize("case", range(len(CASES)))
+@pytest.mark.parametrize("mode", [_lib.NFX_PER_POINT_THREAD, _lib.NFX_PER_POINT_GROUP])
+def test_tma_staging_bit_identical(case, mode):
+    dim, nf, tile, M, ntr, dt, clustered = CASES[case]
+    dev = cuda_device()
+    rng = np.random.default_rng(100 + case)
+    if clustered:
+        X = [np.mod(0.4 * rng.standard_normal(M) + np.pi, 2 * np.pi) - np.pi for _ in range(dim)]
+    else:
+        X = [rng.uniform(-np.pi, np.pi, M) for _ in range(dim)]
+    X = [x.astype(dt) for x in X]
+    eps = 1e-6 if dt == np.float32 else 1e-10
+    kp = compute_kernel_params(eps, 2.0)
+    cdt = np.complex64 if dt == np.float32 else np.complex128
+    shape = (ntr,) + tuple(reversed(nf))
+    fw_np = (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(cdt)
+    Xt = [torch.from_numpy(x).to(dev) for x in X]
+    fw = torch.from_numpy(fw_np).to(dev)
+    ps = PointSort(Xt, nf, kp, prenorm=True, tile=tile, modes=(0, mode))
+    assert _lib.device_status() == 0
+    plain, tma = _interp_both(ps, fw)
+    assert _lib.device_status() == 0
+    assert torch.equal(plain, tma)
+    # the TMA-staged result against the oracle's interpolation
+    sel = slice(0, min(M, 4000))
+    ref = O.interp([x[sel] for x in X], fw_np, kp)
+    got = tma.cpu().numpy()[..., sel]
+    tol = 1e-5 if dt == np.float32 else 1e-11
+    assert rel_l2(got.reshape(ref.shape), ref) <= tol
