@@ -99,12 +99,13 @@ def _make_opts(precision: int, nf: Sequence[int], kp: KernelParams, prenorm: boo
     return o
 
 
-def sort_launches(opts, M: int) -> int:
+def sort_launches(opts, M: int, type3: bool = False) -> int:
     """Kernels one nfx_sort_points call launches: keys (with the first digit's
     counts), per radix pass a column scan and a scatter (plus a count for the
-    passes after the first), the sorted folded coordinates, bin bounds and
-    subproblems.  The composite key is bin << cell_bits | cell; digits have at
-    most 11 bits."""
+    passes after the first), the sorted-coordinates gather (double precision
+    and type-3 points only: float coordinates ride through the passes), bin
+    bounds and subproblems.  The composite key is bin << cell_bits | cell;
+    digits have at most 11 bits."""
     if M == 0:
         return 2
     nbins = ncell = 1
@@ -114,7 +115,8 @@ def sort_launches(opts, M: int) -> int:
         ncell *= t
     bits = max(1, (ncell - 1).bit_length() + (nbins - 1).bit_length())
     npass = 1 if bits <= 11 else (2 if bits <= 22 else 3)
-    return 3 * npass + 3
+    gather = type3 or int(opts.precision) != _lib.NFX_F32
+    return 3 * npass + 2 + int(gather)
 
 
 class PointSort:

@@ -422,6 +422,9 @@ static void make_layout(const nfx_opts& o, const Geom& g, int64_t M, SortLayout&
   L.off_sub_start = take((size_t)L.max_subs * 4);
   L.off_nsub = take(4);
   for (int d = 0; d < 3; ++d) L.off_coord[d] = d < o.dim ? take((size_t)M * real_bytes(o.precision)) : 0;
+  // float coordinates of non-type-3 points are carried through the radix passes
+  const bool carry = o.precision == NFX_F32 && g.t3_mode == 0;
+  for (int d = 0; d < 3; ++d) L.off_coord_tmp[d] = carry && d < o.dim ? take((size_t)M * 4) : 0;
   L.off_extra = g.t3_mode != 0 ? take((size_t)M * 2 * real_bytes(o.precision)) : 0;
   L.total = off;
 }
@@ -448,6 +451,7 @@ static SortPtrs carve(const SortLayout& L, void* ws) {
   P.sub_start = (int*)(b + L.off_sub_start);
   P.nsub = (int*)(b + L.off_nsub);
   for (int d = 0; d < 3; ++d) P.coord[d] = L.off_coord[d] != 0 ? (void*)(b + L.off_coord[d]) : nullptr;
+  for (int d = 0; d < 3; ++d) P.coord_tmp[d] = L.off_coord_tmp[d] != 0 ? (void*)(b + L.off_coord_tmp[d]) : nullptr;
   P.extra = L.off_extra != 0 ? (void*)(b + L.off_extra) : nullptr;
   return P;
 }

@@ -29,6 +29,7 @@ struct SortLayout {
   size_t off_keys, off_keys_tmp, off_vals_tmp, off_keys_sorted, off_perm, off_counts, off_totals, off_bin_start,
       off_sub_bin, off_sub_start, off_nsub;
   size_t off_coord[3];  // folded coordinates in sorted order, one array per axis (0 = unused axis)
+  size_t off_coord_tmp[3];  // float, non-type-3 sorts: ping-pong buffers of the coordinates the passes carry
   size_t off_extra;     // type 3 only: one complex factor per sorted point (0 = none)
   size_t total;
 };
@@ -46,6 +47,7 @@ struct SortPtrs {
   int* sub_start;
   int* nsub;
   void* coord[3];  // sorted folded coordinates (working precision), nullptr for unused axes
+  void* coord_tmp[3];  // the passes' second coordinate buffers (nullptr: coordinates are gathered instead)
   void* extra;     // type 3: complex factor per sorted point, else nullptr
 };
 

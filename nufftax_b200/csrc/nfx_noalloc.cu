@@ -8,9 +8,11 @@
 // lives in the file-scope array below, which every GPU that loads the library
 // holds until the process exits.
 //
-// * Limit: kNoAllocScratchBytes (64 MiB) of scratch, enough for about three
-//   million 2D points; a request needing more is rejected with
-//   NFX_ERR_UNSUPPORTED before any device work.
+// * Limit: kNoAllocScratchBytes (64 MiB) of scratch, enough for about 1.8
+//   million 2D complex64 points (the sort keeps 36-40 bytes per float point:
+//   keys, permutation, radix ping-pong buffers and two copies of the folded
+//   coordinates); a request needing more is rejected with NFX_ERR_UNSUPPORTED
+//   before any device work.
 // * Set-up: the first call on a device, with that device current, looks up the
 //   array's device address with cudaGetSymbolAddress (host code cannot use the
 //   array's name as a device pointer); make that first call before any stream

@@ -21,9 +21,13 @@
 //     per digit bit inside each 32-element round, per-warp running counts
 //     across rounds), stages the chunk in shared memory in digit order and
 //     writes it out as contiguous runs per digit;
-// (3) k_sorted_coords writes every point's folded coordinates in sorted order
-//     (the spread / interp / gradient passes then stream them instead of
-//     gathering through the permutation), k_bin_bounds reads the bin starts
+// (3) every point's folded coordinates in sorted order (the spread / interp /
+//     gradient passes then stream them instead of gathering through the
+//     permutation): float coordinates are written in input order by
+//     k_sort_keys and carried through the scatter passes as payload (coalesced
+//     reads, run-wise writes); double and type-3 points get them from
+//     k_sorted_coords, which gathers through the permutation (and computes the
+//     type-3 factor).  k_bin_bounds reads the bin starts
 //     off the sorted keys, and k_subproblems splits bins larger than
 //     max_subproblem points into subproblems so clustered inputs spread evenly
 //     over the SMs.  Points of a subproblem are ordered by cell, which lets
@@ -31,6 +35,7 @@
 //     near-identical addresses per warp.
 // No CTA waits for another: every dependency is a kernel boundary.
 #include <algorithm>
+#include <type_traits>
 
 #include "nfx_internal.h"
 
@@ -52,13 +57,15 @@ __device__ __forceinline__ unsigned peer_mask(int key, int nbits) {
 
 // Bin of the tile holding the footprint's left cell, and that cell's index
 // inside the tile (both x-fastest), from the point's coordinates.
+// xs[d]: the folded, rescaled coordinate the key came from.
 template <typename T, int DIM, bool T3>
-__device__ __forceinline__ void cell_keys(const T (&c)[DIM], const Geom& g, int ns_half, int& kbin, int& kcell) {
+__device__ __forceinline__ void cell_keys(const T (&c)[DIM], const Geom& g, int ns_half, int& kbin, int& kcell,
+                                          T (&xs)[DIM]) {
   int kb = 0, kc = 0, mb = 1, mc = 1;
 #pragma unroll
   for (int d = 0; d < DIM; ++d) {
-    const T xs = T3 ? point_fold(c[d], d, g) : scaled_coord(c[d], g.nf[d], g.prenorm);
-    const int i0w = wrap_index(ceil_to_int(rn_sub(xs, (T)ns_half)), g.nf[d]);
+    xs[d] = T3 ? point_fold(c[d], d, g) : scaled_coord(c[d], g.nf[d], g.prenorm);
+    const int i0w = wrap_index(ceil_to_int(rn_sub(xs[d], (T)ns_half)), g.nf[d]);
     const int bq = fast_div(i0w, g.tdiv[d]);
     kb += bq * mb;
     kc += (i0w - bq * g.tile[d]) * mc;
@@ -108,11 +115,14 @@ constexpr int kRadixChunk = kRadixThreads * kRadixItems;  // elements per chunk 
 // counts (chunk-major, so the row is one coalesced write).
 // T3: the points are type-3 sources or targets (Geom::t3_mode), a separate
 // instantiation so the common kernel carries no type-3 code.
+// f[d] (nullptr: not wanted): every point's folded coordinates in input order,
+// the payload the scatter passes then carry into sorted order.
 template <typename T, int DIM, bool T3>
 __global__ void __launch_bounds__(kRadixThreads) k_sort_keys(const T* __restrict__ x, const T* __restrict__ y,
                                                             const T* __restrict__ z, int M, Geom g, int ns_half,
                                                             int cbits, int dbits, int* __restrict__ K,
-                                                            int* __restrict__ counts) {
+                                                            int* __restrict__ counts, T* __restrict__ f0,
+                                                            T* __restrict__ f1, T* __restrict__ f2) {
   extern __shared__ int s_h[];
   const int B = 1 << dbits;
   const int mask = B - 1;
@@ -133,10 +143,16 @@ __global__ void __launch_bounds__(kRadixThreads) k_sort_keys(const T* __restrict
     const int p = c0 + u * kRadixThreads + threadIdx.x;
     if (p < M) {
       int kb, kc;
-      cell_keys<T, DIM, T3>(cv[u], g, ns_half, kb, kc);
+      T xs[DIM];
+      cell_keys<T, DIM, T3>(cv[u], g, ns_half, kb, kc, xs);
       const int key = (kb << cbits) | kc;
       K[p] = key;
       atomicAdd(&s_h[key & mask], 1);
+      if (f0 != nullptr) {
+        f0[p] = xs[0];
+        if (DIM > 1) f1[p] = xs[DIM > 1 ? 1 : 0];
+        if (DIM > 2) f2[p] = xs[DIM > 2 ? 2 : 0];
+      }
     }
   }
   __syncthreads();
@@ -230,33 +246,46 @@ __global__ void __launch_bounds__(kScanDigits * kScanGroups) k_col_scan(int* __r
 // ---- (2b) one stable scatter pass --------------------------------------------
 // Shared memory: per-warp digit counts (later reused for the staged chunk), the
 // chunk's digit starts and each digit's output offset.
-__host__ __device__ constexpr int radix_region_ints(int B) {
-  return (kRadixThreads / 32) * B > 2 * kRadixChunk ? (kRadixThreads / 32) * B : 2 * kRadixChunk;
+// Shared-memory ints of the region that first holds the per-warp digit counts
+// and then the staged chunk (keys, values and PD payload words per element).
+__host__ __device__ constexpr int radix_region_ints(int B, int PD) {
+  return (kRadixThreads / 32) * B > (2 + PD) * kRadixChunk ? (kRadixThreads / 32) * B : (2 + PD) * kRadixChunk;
 }
-__host__ __device__ constexpr size_t radix_smem_bytes(int B) {
-  return (size_t)(radix_region_ints(B) + 2 * B) * sizeof(int);
+__host__ __device__ constexpr size_t radix_smem_bytes(int B, int PD) {
+  return (size_t)(radix_region_ints(B, PD) + 2 * B) * sizeof(int);
 }
+
+// Float words carried with every element through a pass (the folded
+// coordinates, one array per axis): in[d][i] belongs to input element i and
+// lands at out[d][j] where the element lands.
+struct RadixPayload {
+  const float* in[3];
+  float* out[3];
+};
 
 // kin/vin: this pass's input keys and values (vin == nullptr: the values are
 // the element indices); kout/vout: the output, stable by digit
 // (kin >> shift) & (2^dbits - 1).  prefix[chunk][d]: digit-d elements in the
-// chunks before this one; totals[d]: digit-d elements overall.
-template <int DPT>
-__global__ void __launch_bounds__(kRadixThreads) k_radix_scatter(const int* __restrict__ kin,
+// chunks before this one; totals[d]: digit-d elements overall.  PD payload
+// arrays move with the elements (pay).
+template <int DPT, int PD>
+__global__ void __launch_bounds__(kRadixThreads, 3) k_radix_scatter(const int* __restrict__ kin,
                                                                 const int* __restrict__ vin, int M, int shift,
                                                                 int dbits, const int* __restrict__ prefix,
                                                                 const int* __restrict__ totals,
-                                                                int* __restrict__ kout, int* __restrict__ vout) {
+                                                                int* __restrict__ kout, int* __restrict__ vout,
+                                                                RadixPayload pay) {
   extern __shared__ int smem[];
   __shared__ int s_warp[32];
   constexpr int W = kRadixThreads / 32;
   const int B = 1 << dbits;
   const int mask = B - 1;
-  int* s_hw = smem;                             // [W][B] per-warp digit counts
-  int* s_key = smem;                            // [kRadixChunk] staged keys (after ranking)
-  int* s_val = smem + kRadixChunk;              // [kRadixChunk] staged values
-  int* s_dstart = smem + radix_region_ints(B);  // [B] digit starts within the chunk
-  int* s_gofs = s_dstart + B;                   // [B] output index - staged index, per digit
+  int* s_hw = smem;                                 // [W][B] per-warp digit counts
+  int* s_key = smem;                                // [kRadixChunk] staged keys (after ranking)
+  int* s_val = smem + kRadixChunk;                  // [kRadixChunk] staged values
+  float* s_pay = reinterpret_cast<float*>(smem + 2 * kRadixChunk);  // [PD][kRadixChunk] staged payload
+  int* s_dstart = smem + radix_region_ints(B, PD);  // [B] digit starts within the chunk
+  int* s_gofs = s_dstart + B;                       // [B] output index - staged index, per digit
   for (int i = threadIdx.x; i < W * B; i += blockDim.x) s_hw[i] = 0;
   const int ch = blockIdx.x;
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -352,6 +381,18 @@ __global__ void __launch_bounds__(kRadixThreads) k_radix_scatter(const int* __re
       s_val[rk[r]] = val[r];
     }
   }
+#pragma unroll
+  for (int d = 0; d < PD; ++d) {
+    float pv[kRadixItems];
+#pragma unroll
+    for (int r = 0; r < kRadixItems; ++r) {
+      const int p = wbase + r * 32 + lane;
+      pv[r] = p < M ? pay.in[d][p] : 0.f;
+    }
+#pragma unroll
+    for (int r = 0; r < kRadixItems; ++r)
+      if (key[r] >= 0) s_pay[d * kRadixChunk + rk[r]] = pv[r];
+  }
   __syncthreads();
   const int n_here = M - c0 < kRadixChunk ? M - c0 : kRadixChunk;
   for (int i = threadIdx.x; i < n_here; i += blockDim.x) {
@@ -360,8 +401,24 @@ __global__ void __launch_bounds__(kRadixThreads) k_radix_scatter(const int* __re
     if ((unsigned)gpos < (unsigned)M) {  // always: counts and keys come from the same array
       kout[gpos] = k;
       vout[gpos] = s_val[i];
+#pragma unroll
+      for (int d = 0; d < PD; ++d) pay.out[d][gpos] = s_pay[d * kRadixChunk + i];
     }
   }
+}
+
+// The scatter instantiation for 2^dbits digits and PD payload arrays.
+using ScatterFn = void (*)(const int*, const int*, int, int, int, const int*, const int*, int*, int*, RadixPayload);
+template <int PD>
+static ScatterFn scatter_for_digits(int B) {
+  return B <= kRadixThreads ? k_radix_scatter<1, PD>
+                            : (B <= 2 * kRadixThreads ? k_radix_scatter<2, PD>
+                                                      : (B <= 4 * kRadixThreads ? k_radix_scatter<4, PD>
+                                                                                : k_radix_scatter<8, PD>));
+}
+static ScatterFn scatter_for(int B, int PD) {
+  return PD == 0 ? scatter_for_digits<0>(B)
+                 : (PD == 1 ? scatter_for_digits<1>(B) : (PD == 2 ? scatter_for_digits<2>(B) : scatter_for_digits<3>(B)));
 }
 
 // ---- (3) bin starts and subproblems ----------------------------------------
@@ -602,14 +659,15 @@ cudaError_t launch_sort(const SortLayout& L, const Geom& g, int ns, const void* 
                         int64_t M, const SortPtrs& P, cudaStream_t st) {
   const int B = 1 << L.dbits;
   cudaError_t e = cudaSuccess;
+  // float coordinates of non-type-3 points ride through the passes as payload
+  // (the layout then holds coord_tmp); otherwise k_sorted_coords gathers them
+  const bool carry = std::is_same<T, float>::value && P.coord_tmp[0] != nullptr;
+  const int PD = carry ? g.dim : 0;
   if (M > 0) {
     const size_t hist_smem = (size_t)B * sizeof(int);
     // digits per thread of the scatter: 2^dbits / 256, at least 1
-    auto scatter = B <= kRadixThreads ? k_radix_scatter<1>
-                                      : (B <= 2 * kRadixThreads ? k_radix_scatter<2>
-                                                                : (B <= 4 * kRadixThreads ? k_radix_scatter<4>
-                                                                                          : k_radix_scatter<8>));
-    e = ensure_smem(reinterpret_cast<const void*>(scatter), radix_smem_bytes(B));
+    const ScatterFn scatter = scatter_for(B, PD);
+    e = ensure_smem(reinterpret_cast<const void*>(scatter), radix_smem_bytes(B, PD));
     if (e == cudaSuccess) e = prefer_max_smem(reinterpret_cast<const void*>(scatter));
     if (e != cudaSuccess) return e;
     const unsigned scan_grid = (unsigned)((B + kScanDigits - 1) / kScanDigits);
@@ -617,11 +675,16 @@ cudaError_t launch_sort(const SortLayout& L, const Geom& g, int ns, const void* 
                     ? (g.dim == 1 ? k_sort_keys<T, 1, true> : (g.dim == 2 ? k_sort_keys<T, 2, true> : k_sort_keys<T, 3, true>))
                     : (g.dim == 1 ? k_sort_keys<T, 1, false>
                                   : (g.dim == 2 ? k_sort_keys<T, 2, false> : k_sort_keys<T, 3, false>));
-    keys<<<L.nchunks, kRadixThreads, hist_smem, st>>>((const T*)x, (const T*)y, (const T*)z, (int)M, g, ns / 2,
-                                                      L.cbits, L.dbits, P.keys, P.counts);
-    // ping-pong so that the last pass writes (keys_sorted, perm)
+    // ping-pong so that the last pass writes (keys_sorted, perm[, coord]); the
+    // keys kernel writes the input-order coordinates into the buffer the first
+    // pass does not write
+    void* const* cfirst = (L.npass % 2 == 0) ? P.coord : P.coord_tmp;
+    keys<<<L.nchunks, kRadixThreads, hist_smem, st>>>(
+        (const T*)x, (const T*)y, (const T*)z, (int)M, g, ns / 2, L.cbits, L.dbits, P.keys, P.counts,
+        carry ? (T*)cfirst[0] : nullptr, carry ? (T*)cfirst[1] : nullptr, carry ? (T*)cfirst[2] : nullptr);
     const int* kin = P.keys;
     const int* vin = nullptr;
+    void* const* cin = cfirst;
     for (int ps = 0; ps < L.npass; ++ps) {
       const int shift = ps * L.dbits;
       if (ps > 0) k_digit_count<<<L.nchunks, kRadixThreads, hist_smem, st>>>(kin, (int)M, shift, L.dbits, P.counts);
@@ -629,16 +692,23 @@ cudaError_t launch_sort(const SortLayout& L, const Geom& g, int ns, const void* 
       const bool to_final = ((L.npass - 1 - ps) % 2) == 0;
       int* kout = to_final ? P.keys_sorted : P.keys_tmp;
       int* vout = to_final ? P.perm : P.vals_tmp;
-      scatter<<<L.nchunks, kRadixThreads, radix_smem_bytes(B), st>>>(kin, vin, (int)M, shift, L.dbits, P.counts,
-                                                                     P.totals, kout, vout);
+      void* const* cout = to_final ? P.coord : P.coord_tmp;
+      RadixPayload pay{{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+      for (int d = 0; d < PD; ++d) {
+        pay.in[d] = (const float*)cin[d];
+        pay.out[d] = (float*)cout[d];
+      }
+      scatter<<<L.nchunks, kRadixThreads, radix_smem_bytes(B, PD), st>>>(kin, vin, (int)M, shift, L.dbits,
+                                                                         P.counts, P.totals, kout, vout, pay);
       kin = kout;
       vin = vout;
+      cin = cout;
     }
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
   const int bgrid = (int)std::max<int64_t>(1, std::min<int64_t>((M / 4 + 256) / 256, (int64_t)num_sms() * 8));
-  if (M > 0) {
+  if (M > 0 && !carry) {
     auto sc = g.t3_mode != 0 ? (g.dim == 1 ? k_sorted_coords<T, 1, true>
                                            : (g.dim == 2 ? k_sorted_coords<T, 2, true> : k_sorted_coords<T, 3, true>))
                              : (g.dim == 1 ? k_sorted_coords<T, 1, false>

@@ -505,8 +505,8 @@ def _type3_forward(src: list[torch.Tensor], c2: torch.Tensor, tgt: list[torch.Te
     tgt = [a.contiguous() for a in tgt]
     c2 = c2.contiguous()
     # our kernels: min / max per array, the scalars, both sorts, spread, zero-pad, interp
-    launches = lambda: (2 * dim + 1 + sort_launches(opts, M) + 2  # noqa: E731 (evaluated only when recording)
-                        + sort_launches(make_opts(precision, nf_in, kp, prenorm=True), K) + 1)
+    launches = lambda: (2 * dim + 1 + sort_launches(opts, M, type3=True) + 2  # noqa: E731 (evaluated only when recording)
+                        + sort_launches(make_opts(precision, nf_in, kp, prenorm=True), K, type3=True) + 1)
     with torch.cuda.device(dev), span("nfx_nufft3", dev, launches):
         _lib.check(lib.nfx_nufft3(byref(opts), _lib.int3c(nf_in), float(uf), int(isign), parr(src), M, ptr(c2), nt,
                                   parr(tgt), K, ptr(facs[0]), ptr(facs[1]), ptr(facs[2]), ptr(out), ptr(ws),
