@@ -138,6 +138,11 @@ class ClockSampler:
             return
         self.thread = threading.Thread(target=self._read, daemon=True)
         self.thread.start()
+        # nvidia-smi takes a moment to start: wait (3 s at most) for its first
+        # sample so that the samples cover the region that follows
+        t0 = time.perf_counter()
+        while not self.rows and time.perf_counter() - t0 < 3.0 and self.proc.poll() is None:
+            time.sleep(0.02)
 
     def _read(self):
         for line in self.proc.stdout:
@@ -168,6 +173,20 @@ class ClockSampler:
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def warm(step, n_min: int, seconds: float = 1.0) -> int:
+    """Runs `step` at least n_min times and until `seconds` have passed (device
+    synchronised), so that clock samples taken from here on see the GPU under
+    this load.  Returns the number of steps run."""
+    import torch
+
+    n, t0 = 0, time.perf_counter()
+    while n < n_min or time.perf_counter() - t0 < seconds:
+        step()
+        torch.cuda.synchronize()
+        n += 1
+    return n
 
 
 class clocked:
@@ -228,13 +247,48 @@ ALG_BYTES = {
 }
 
 
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch per point set,
-# from ncu --set full captures of `bench.py --case radial|clustered --reps 1` (the step
-# launches each kernel once per set, so the per-launch figure is their mean).
-MEASURED_TRAFFIC = {
-    "nfx_spread_sorted": {"radial": 17.3e6, "clustered": 117.0e6},
-    "nfx_interp_sorted": {"radial": 13.5e6, "clustered": 108.4e6},
+# Per-launch counters of the spread / interp kernels on each point set, from
+# single-step ncu --set full captures of `bench.py --case radial|clustered --reps 1`
+# (profiles/kernels_2d_bench_sets.md): DRAM bytes (dram__bytes_read.sum +
+# dram__bytes_write.sum, caches flushed before the launch), warp instructions
+# (smsp__inst_executed.sum) and shared-memory wavefronts
+# (l1tex__data_pipe_lsu_wavefronts_mem_shared.sum).  The counts do not depend on
+# timing, so the bench divides them by the live launch times to get the
+# fractions of the issue and shared-memory roofs, the ones that bind these
+# kernels (HBM runs at a few percent of peak).
+MEASURED_COUNTERS = {
+    "nfx_spread_sorted": {"radial": {"dram": 17.3e6, "inst": 36.3e6, "smem_wf": 9.40e6},
+                          "clustered": {"dram": 85.6e6, "inst": 87.1e6, "smem_wf": 18.1e6}},
+    "nfx_interp_sorted": {"radial": {"dram": 13.5e6, "inst": 8.19e6, "smem_wf": 3.71e6},
+                          "clustered": {"dram": 102.8e6, "inst": 51.1e6, "smem_wf": 10.1e6}},
 }
+N_SMS = 148
+ISSUE_PER_SM_CLK = 4      # one warp instruction per scheduler per clock, 4 schedulers per SM
+SMEM_BYTES_PER_SM_CLK = 128  # one 128-byte shared-memory wavefront per SM per clock
+
+
+def secondary_roofs(kernel: str, avg_launch_ms: float, sm_mhz) -> dict | None:
+    """Fractions of the issue-slot and shared-memory-bandwidth roofs reached by the
+    live launches of `kernel` (captured counts per launch / live launch time, against
+    the SM count x per-clock rate x the median SM clock sampled in the run)."""
+    counts = MEASURED_COUNTERS.get(kernel)
+    if counts is None or not sm_mhz or avg_launch_ms <= 0:
+        return None
+    n = len(counts)
+    inst = sum(c["inst"] for c in counts.values()) / n
+    wf = sum(c["smem_wf"] for c in counts.values()) / n
+    t = avg_launch_ms / 1e3
+    clk = float(sm_mhz) * 1e6
+    issue_peak = N_SMS * ISSUE_PER_SM_CLK * clk / 1e9
+    smem_peak = N_SMS * SMEM_BYTES_PER_SM_CLK * clk / 1e9
+    return {
+        "issue": {"achieved": inst / t / 1e9, "peak": issue_peak, "unit": "G warp-instr/s",
+                  "frac": inst / t / 1e9 / issue_peak, "inst_per_launch": inst},
+        "shared": {"achieved": wf * 128 / t / 1e9, "peak": smem_peak, "unit": "GB/s",
+                   "frac": wf * 128 / t / 1e9 / smem_peak, "wavefronts_per_launch": wf},
+        "clock_mhz": float(sm_mhz),
+        "counts_from": "ncu --set full, one launch per point set (profiles/kernels_2d_bench_sets.md)",
+    }
 
 
 def run_gpu(args):
@@ -427,6 +481,17 @@ def run_gpu(args):
     e_ms = a.elapsed_time(b)
     clocks = sampler.stop()
     e_ms, e2e_value = aggregate_ranks(e_ms, points_per_step(sets) * args.steps, world, dev)
+    counters = MEASURED_COUNTERS.get(dom)
+    roofline = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_kind": peak_kind,
+                "traffic": (sum(c["dram"] for c in counters.values()) / len(counters) if counters else None),
+                "traffic_note": "mean per launch over the two point sets, ncu capture with caches flushed",
+                "alg_bytes_per_launch": alg_per_launch, "avg_launch_ms": avg_ms}
+    sec = secondary_roofs(dom, avg_ms, clocks.get("sm_mhz"))
+    if sec is not None:
+        roofline["secondary"] = sec
+        roofline["binding"] = max(("hbm", achieved / peak), ("issue", sec["issue"]["frac"]),
+                                  ("shared", sec["shared"]["frac"]), key=lambda kv: kv[1])[0]
 
     line = {
         "metric": METRIC,
@@ -445,11 +510,7 @@ def run_gpu(args):
         "e2e": {"value": e2e_value, "unit": "NU points/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "steps_pipelined": True,
                 "pcie_gbs": round((h2d + d2h) * args.steps / (e_ms / 1e3) / 1e9, 1)},
-        "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_kind": peak_kind,
-                     "traffic": (sum(MEASURED_TRAFFIC[dom].values()) / len(MEASURED_TRAFFIC[dom])
-                                 if dom in MEASURED_TRAFFIC else None),
-                     "alg_bytes_per_launch": alg_per_launch, "avg_launch_ms": avg_ms},
+        "roofline": roofline,
         "gpu_launches": int(launches),
         "clocks": clocks,
         "breakdown": breakdown,
@@ -680,9 +741,7 @@ def measure_batched(dev, steps: int, warmup: int, autotune: bool = False) -> dic
             nb.nufft2d2(q["x"], q["y"], q["f"], eps=eps)
 
     def timed(fn):
-        for _ in range(warmup):
-            fn()
-        torch.cuda.synchronize()
+        warm(fn, warmup, 0.5)  # under the clock sampler (the caller's clocked block)
         tot = 0.0
         for i in range(steps):
             flush.fill_(float(i))
@@ -767,11 +826,9 @@ def measure_grad3d(dev, steps: int, warmup: int, M: int = 8_000_000) -> dict:
         loss.backward()
         return loss, cc.grad, [x.grad for x in xs]
 
-    for _ in range(warmup):
-        step()
-    torch.cuda.synchronize()
     tot = 0.0
     with clocked(dev.index) as ck:
+        warmup = warm(step, warmup)
         for _ in range(steps):
             a = torch.cuda.Event(enable_timing=True)
             b = torch.cuda.Event(enable_timing=True)
@@ -1046,10 +1103,8 @@ def measure_1d(dev, steps: int, warmup: int) -> dict:
         nb.nufft1d1(x, c, N, eps=EPS)
         nb.nufft1d2(x, f, eps=EPS)
 
-    for _ in range(warmup):
-        step()
-    torch.cuda.synchronize()
     with clocked(dev.index) as ck:
+        n_warm = warm(step, warmup)
         a = torch.cuda.Event(enable_timing=True)
         b = torch.cuda.Event(enable_timing=True)
         a.record()
@@ -1059,8 +1114,9 @@ def measure_1d(dev, steps: int, warmup: int) -> dict:
         torch.cuda.synchronize()
     ms = a.elapsed_time(b) / steps
     return {"metric": "1D type-1 + type-2 NU points/s (M=200000, N=8192, eps 1e-6, complex64)", "value": 2 * M / (ms / 1e3),
-            "unit": "NU points/s", "ms_per_step": ms, "steps": steps, "warmup": warmup, "clocks": ck.summary,
-            "note": "inputs resident, back-to-back steps (launch-bound at this size)"}
+            "unit": "NU points/s", "ms_per_step": ms, "steps": steps, "warmup": n_warm, "clocks": ck.summary,
+            "note": "inputs resident, back-to-back steps (launch-bound at this size); warm-up runs 1 s under the "
+                    "clock sampler"}
 
 
 def _plain(nb, r, dev):

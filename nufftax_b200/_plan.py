@@ -104,8 +104,9 @@ def sort_launches(opts, M: int, type3: bool = False) -> int:
     counts), per radix pass a column scan and a scatter (plus a count for the
     passes after the first), the sorted-coordinates gather (double precision
     and type-3 points only: float coordinates ride through the passes), bin
-    bounds and subproblems.  The composite key is bin << cell_bits | cell;
-    digits have at most 11 bits."""
+    bounds (unless the last pass's digit is the bin: that pass writes them) and
+    subproblems.  The composite key is bin << cell_bits | cell; digits have at
+    most 11 bits."""
     if M == 0:
         return 2
     nbins = ncell = 1
@@ -113,10 +114,13 @@ def sort_launches(opts, M: int, type3: bool = False) -> int:
         t = int(opts.tile[d])
         nbins *= -(-int(opts.nf[d]) // t)
         ncell *= t
-    bits = max(1, (ncell - 1).bit_length() + (nbins - 1).bit_length())
+    cbits = (ncell - 1).bit_length()
+    bits = max(1, cbits + (nbins - 1).bit_length())
     npass = 1 if bits <= 11 else (2 if bits <= 22 else 3)
+    dbits = -(-bits // npass)
     gather = type3 or int(opts.precision) != _lib.NFX_F32
-    return 3 * npass + 2 + int(gather)
+    bounds = (npass - 1) * dbits != cbits
+    return 3 * npass + 1 + int(gather) + int(bounds)
 
 
 class PointSort:

@@ -267,14 +267,17 @@ struct RadixPayload {
 // the element indices); kout/vout: the output, stable by digit
 // (kin >> shift) & (2^dbits - 1).  prefix[chunk][d]: digit-d elements in the
 // chunks before this one; totals[d]: digit-d elements overall.  PD payload
-// arrays move with the elements (pay).
+// arrays move with the elements (pay).  bstart (not nullptr only in a last
+// pass whose digit is the bin): CTA 0 writes the bin starts (the exclusive
+// scan of the digit totals), bstart[0..nbins].
 template <int DPT, int PD>
 __global__ void __launch_bounds__(kRadixThreads, 3) k_radix_scatter(const int* __restrict__ kin,
                                                                 const int* __restrict__ vin, int M, int shift,
                                                                 int dbits, const int* __restrict__ prefix,
                                                                 const int* __restrict__ totals,
                                                                 int* __restrict__ kout, int* __restrict__ vout,
-                                                                RadixPayload pay) {
+                                                                RadixPayload pay, int* __restrict__ bstart,
+                                                                int nbins) {
   extern __shared__ int smem[];
   __shared__ int s_warp[32];
   constexpr int W = kRadixThreads / 32;
@@ -360,10 +363,12 @@ __global__ void __launch_bounds__(kRadixThreads, 3) k_radix_scatter(const int* _
     if (d < d1) {
       s_dstart[d] = run;
       s_gofs[d] = gbase + pre_d[j] - run;
+      if (bstart != nullptr && blockIdx.x == 0 && d < nbins) bstart[d] = gbase;
     }
     run += cnt_d[j];
     gbase += tot_d[j];
   }
+  if (bstart != nullptr && blockIdx.x == 0 && threadIdx.x == 0) bstart[nbins] = M;
   __syncthreads();
   // staged (digit-ordered) index of every element
 #pragma unroll
@@ -408,7 +413,8 @@ __global__ void __launch_bounds__(kRadixThreads, 3) k_radix_scatter(const int* _
 }
 
 // The scatter instantiation for 2^dbits digits and PD payload arrays.
-using ScatterFn = void (*)(const int*, const int*, int, int, int, const int*, const int*, int*, int*, RadixPayload);
+using ScatterFn = void (*)(const int*, const int*, int, int, int, const int*, const int*, int*, int*, RadixPayload,
+                           int*, int);
 template <int PD>
 static ScatterFn scatter_for_digits(int B) {
   return B <= kRadixThreads ? k_radix_scatter<1, PD>
@@ -698,8 +704,10 @@ cudaError_t launch_sort(const SortLayout& L, const Geom& g, int ns, const void* 
         pay.in[d] = (const float*)cin[d];
         pay.out[d] = (float*)cout[d];
       }
-      scatter<<<L.nchunks, kRadixThreads, radix_smem_bytes(B, PD), st>>>(kin, vin, (int)M, shift, L.dbits,
-                                                                         P.counts, P.totals, kout, vout, pay);
+      // the last pass's digit is the bin when it starts at the cell bits
+      int* bstart = (ps == L.npass - 1 && shift == L.cbits) ? P.bin_start : nullptr;
+      scatter<<<L.nchunks, kRadixThreads, radix_smem_bytes(B, PD), st>>>(
+          kin, vin, (int)M, shift, L.dbits, P.counts, P.totals, kout, vout, pay, bstart, g.nbins);
       kin = kout;
       vin = vout;
       cin = cout;
@@ -718,7 +726,8 @@ cudaError_t launch_sort(const SortLayout& L, const Geom& g, int ns, const void* 
     sc<<<cgrid, 256, 0, st>>>((const T*)x, (const T*)y, (const T*)z, P.perm, (int)M, g, ns, (T*)P.coord[0],
                               (T*)P.coord[1], (T*)P.coord[2], (cplx_t<T>*)P.extra);
   }
-  k_bin_bounds<<<bgrid, 256, 0, st>>>(P.keys_sorted, (int)M, L.cbits, g.nbins, P.bin_start);
+  const bool fused_bounds = M > 0 && (int64_t)(L.npass - 1) * L.dbits == L.cbits;
+  if (!fused_bounds) k_bin_bounds<<<bgrid, 256, 0, st>>>(P.keys_sorted, (int)M, L.cbits, g.nbins, P.bin_start);
   const int max_subs = (int)std::min<int64_t>(L.max_subs, INT32_MAX);
   const size_t sub_smem = g.nbins <= kSubSmemBins ? (size_t)(g.nbins + 1) * sizeof(int) : 0;
   k_subproblems<<<1, 1024, sub_smem, st>>>(P.bin_start, g.nbins, L.maxsub, max_subs, P.sub_bin, P.sub_start,
