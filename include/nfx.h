@@ -85,6 +85,14 @@ int nfx_num_sms(void);
 enum { NFX_STATUS_TMA_TIMEOUT = 1 };
 int nfx_device_status(int* status);
 
+/* Self-test of that bounded wait (no counterpart in the reference): one CTA
+ * arms a barrier for a tile copy that is never issued, so its wait runs out
+ * after the limit; the kernel records NFX_STATUS_TMA_TIMEOUT and returns with
+ * nothing in flight.  Synchronizes the device (about 0.5 s) and writes the
+ * status bits read (and cleared) to *status: NFX_STATUS_TMA_TIMEOUT when the
+ * bound works. */
+int nfx_selftest_bounded_wait(int* status);
+
 /* Polynomial form of the ES weights used by the float kernels (no counterpart
  * in the reference, which evaluates exp/sqrt): coefficients a[q][d] of
  * phi(q - (v + ns - 1) / 2) as a degree-`degree` polynomial in v in [-1, 1],

@@ -914,6 +914,42 @@ int nfx_es_poly(int nspread, double beta, double kc, float* coeffs, int* degree,
 const char* nfx_last_error(void) { return g_last_error.c_str(); }
 int nfx_num_sms(void) { return num_sms(); }
 
+// One CTA arms an mbarrier for 16 bytes of TMA data and issues no copy, so
+// its bounded wait (tma_wait) runs out; nothing is in flight when it returns.
+__global__ void k_bounded_wait_selftest(int* status) {
+  __shared__ __align__(8) uint64_t mbar;
+  nfx::tma_init(&mbar);
+  const unsigned mb = nfx::smem_addr(&mbar);
+  if (threadIdx.x == 0)
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(16u) : "memory");
+  const bool landed = nfx::tma_wait(mb, 0u);
+  if (!__syncthreads_and(landed) && threadIdx.x == 0) atomicOr(status, NFX_STATUS_TMA_TIMEOUT);
+}
+
+int nfx_selftest_bounded_wait(int* status) {
+  using namespace nfx;
+  if (status == nullptr) {
+    set_error("status is NULL");
+    return NFX_ERR_INVALID;
+  }
+  int* w = device_status_word();
+  if (w == nullptr) {
+    set_error("device status word unavailable");
+    return NFX_ERR_CUDA;
+  }
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaMemset(w, 0, sizeof(int));
+  if (e == cudaSuccess) {
+    k_bounded_wait_selftest<<<1, 32>>>(w);
+    e = cudaGetLastError();
+  }
+  if (e != cudaSuccess) {
+    set_error(std::string("nfx_selftest_bounded_wait: ") + cudaGetErrorString(e));
+    return NFX_ERR_CUDA;
+  }
+  return nfx_device_status(status);
+}
+
 int nfx_device_status(int* status) {
   using namespace nfx;
   if (status == nullptr) {

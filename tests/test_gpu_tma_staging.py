@@ -81,3 +81,29 @@ def test_tma_staging_bit_identical(case, mode):
     got = tma.cpu().numpy()[..., sel]
     tol = 1e-5 if dt == np.float32 else 1e-11
     assert rel_l2(got.reshape(ref.shape), ref) <= tol
+
+
+def test_bounded_wait_gives_up_and_reports():
+    """The tile-copy wait is bounded: a barrier armed for a copy that is never
+    issued (nfx_selftest_bounded_wait) makes the kernel give up, record
+    NFX_STATUS_TMA_TIMEOUT and return; the context stays usable and the status
+    reads clean again afterwards."""
+    import ctypes
+
+    lib = _lib.load()
+    assert _lib.device_status() == 0
+    st = ctypes.c_int(0)
+    _lib.check(lib.nfx_selftest_bounded_wait(ctypes.byref(st)), "nfx_selftest_bounded_wait")
+    assert st.value == _lib.NFX_STATUS_TMA_TIMEOUT
+    assert _lib.device_status() == 0
+    # the device still runs the path afterwards
+    dev = cuda_device()
+    rng = np.random.default_rng(7)
+    X = [rng.uniform(-np.pi, np.pi, 3000).astype(np.float32) for _ in range(2)]
+    kp = compute_kernel_params(1e-6, 2.0)
+    fw_np = (rng.standard_normal((1, 96, 128)) + 1j * rng.standard_normal((1, 96, 128))).astype(np.complex64)
+    ps = PointSort([torch.from_numpy(x).to(dev) for x in X], (128, 96), kp, prenorm=True)
+    got = ps.interp(torch.from_numpy(fw_np).to(dev)).cpu().numpy()
+    ref = O.interp(X, fw_np, kp)
+    assert rel_l2(got.reshape(ref.shape), ref) <= 1e-5
+    assert _lib.device_status() == 0
