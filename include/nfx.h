@@ -93,6 +93,11 @@ int nfx_device_status(int* status);
  * bound works. */
 int nfx_selftest_bounded_wait(int* status);
 
+/* Id of the CUDA graph capture the stream takes part in (cudaStreamGetCaptureInfo),
+ * 0 when it is not capturing.  Lets a host layer reuse work captured earlier in the
+ * same capture (a point sort shared by a type 1 and a type 2). */
+int nfx_capture_id(void* stream, unsigned long long* id);
+
 /* Polynomial form of the ES weights used by the float kernels (no counterpart
  * in the reference, which evaluates exp/sqrt): coefficients a[q][d] of
  * phi(q - (v + ns - 1) / 2) as a degree-`degree` polynomial in v in [-1, 1],

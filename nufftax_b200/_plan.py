@@ -9,6 +9,7 @@ from __future__ import annotations
 
 import collections
 import threading
+import ctypes
 from ctypes import byref, c_int, c_size_t, c_void_p
 from typing import Sequence
 
@@ -258,21 +259,44 @@ class _SortCache:
 
     A cached sort may be used from another stream than the one that made it;
     its workspace is then recorded on that stream, so an eviction cannot hand
-    the memory to new work while the other stream's kernels still read it."""
+    the memory to new work while the other stream's kernels still read it.
+
+    During a CUDA graph capture a sort has only been captured, not run: it
+    belongs to the graph and never enters this cache.  It is reused only by
+    later transforms of the same capture on the same stream (so every replay
+    runs the sort before its users), e.g. a type 2 after a type 1 on the same
+    points; those entries are keyed by the capture's id."""
 
     def __init__(self, size: int = 4):
         self.size = size
         self.enabled = True
         self._d: "collections.OrderedDict[tuple, PointSort]" = collections.OrderedDict()
+        self._cap: "collections.OrderedDict[tuple, PointSort]" = collections.OrderedDict()
         self._lock = threading.Lock()
+
+    def _get_captured(self, coords, nf, kp, prenorm, key) -> PointSort:
+        dev = coords[0].device
+        s = stream_of(dev)
+        cid = ctypes.c_ulonglong(0)
+        _lib.check(_lib.load().nfx_capture_id(c_void_p(s), byref(cid)), "nfx_capture_id")
+        ckey = (int(cid.value), s) + key
+        with self._lock:
+            hit = self._cap.get(ckey)
+        if hit is not None and all(a is b for a, b in zip(hit._src, coords)):
+            return hit
+        ps = PointSort(coords, nf, kp, prenorm)
+        ps._src = list(coords)
+        with self._lock:
+            self._cap[ckey] = ps
+            while len(self._cap) > 2 * self.size:
+                self._cap.popitem(last=False)
+        return ps
 
     def get(self, coords, nf, kp, prenorm) -> PointSort:
         key = tuple((id(c), c.data_ptr(), c._version, c.dtype, c.shape[0]) for c in coords) + (
             tuple(nf), kp.nspread, float(kp.beta), float(kp.c), bool(prenorm))
         if torch.cuda.is_current_stream_capturing():
-            # a sort made during capture has only been captured, not run: it
-            # belongs to the graph and never enters the cache
-            return PointSort(coords, nf, kp, prenorm)
+            return self._get_captured(coords, nf, kp, prenorm, key)
         if self.enabled:
             with self._lock:
                 hit = self._d.get(key)
@@ -307,6 +331,7 @@ class _SortCache:
     def clear(self):
         with self._lock:
             self._d.clear()
+            self._cap.clear()
 
 
 sort_cache = _SortCache()

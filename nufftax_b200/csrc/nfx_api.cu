@@ -950,6 +950,24 @@ int nfx_selftest_bounded_wait(int* status) {
   return nfx_device_status(status);
 }
 
+int nfx_capture_id(void* stream, unsigned long long* id) {
+  using namespace nfx;
+  if (id == nullptr) {
+    set_error("id is NULL");
+    return NFX_ERR_INVALID;
+  }
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  unsigned long long cid = 0;
+  cudaError_t e = cudaStreamGetCaptureInfo((cudaStream_t)stream, &cap, &cid);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    set_error(std::string("nfx_capture_id: ") + cudaGetErrorString(e));
+    return NFX_ERR_CUDA;
+  }
+  *id = cap == cudaStreamCaptureStatusActive ? cid : 0ull;
+  return NFX_OK;
+}
+
 int nfx_device_status(int* status) {
   using namespace nfx;
   if (status == nullptr) {

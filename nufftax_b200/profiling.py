@@ -58,7 +58,7 @@ class span:
     the common case costs a thread-local read).  `launches` (kernels the call
     launches) may be a callable, evaluated only when recording."""
 
-    __slots__ = ("rec", "name", "stream", "launches", "a")
+    __slots__ = ("rec", "name", "stream", "launches", "a", "ext")
 
     def __init__(self, name: str, device, launches: int | None = None):
         self.rec = getattr(_state, "rec", None)
@@ -73,13 +73,16 @@ class span:
 
     def __enter__(self):
         if self.rec is not None:
-            self.a = torch.cuda.Event(enable_timing=True)
+            # under CUDA graph capture the events become event-record nodes of
+            # the graph (re-recorded by every replay)
+            self.ext = torch.cuda.is_current_stream_capturing()
+            self.a = torch.cuda.Event(enable_timing=True, external=self.ext)
             self.a.record(self.stream)
         return self
 
     def __exit__(self, *exc):
         if self.rec is not None:
-            b = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True, external=self.ext)
             b.record(self.stream)
             self.rec.events.append((self.name, self.a, b, self.launches))
         return False

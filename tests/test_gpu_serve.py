@@ -7,6 +7,7 @@ import pytest
 import torch
 
 import nufftax_b200 as nb
+from nufftax_b200 import profiling
 from nufftax_b200.serve import NufftServer, Request
 from tests.conftest import cuda_device, rel_l2
 
@@ -212,8 +213,9 @@ def test_fft_caller_work_area_and_capture():
 
 def test_public_api_under_graph_capture():
     """nufft2d1 / nufft2d2 captured in a CUDA graph (the FFT takes its work area
-    from the graph's pool, the sort made during capture stays out of the sort
-    cache) replay to the eager results; an eager call after capture is unaffected."""
+    from the graph's pool; the sort made during capture stays out of the sort
+    cache and is shared by the two transforms of the capture) replay to the
+    eager results; an eager call after capture is unaffected."""
     dev = cuda_device()
     rng = np.random.default_rng(31)
     M, nm = 5000, (48, 40)
@@ -229,9 +231,12 @@ def test_public_api_under_graph_capture():
     xg, yg = x.clone(), y.clone()  # fresh tensors: no cached sort to reuse
     torch.cuda.synchronize()
     g = torch.cuda.CUDAGraph()
-    with torch.cuda.graph(g):
-        out1 = nb.nufft2d1(xg, yg, c, nm)
-        out2 = nb.nufft2d2(xg, yg, f)
+    with profiling.record() as rec:
+        with torch.cuda.graph(g):
+            out1 = nb.nufft2d1(xg, yg, c, nm)
+            out2 = nb.nufft2d2(xg, yg, f)
+    # the type 2 reuses the sort captured for the type 1 (same capture, same stream)
+    assert sum(1 for e in rec.events if e[0] == "nfx_sort_points") == 1
     for _ in range(2):
         g.replay()
         torch.cuda.synchronize()
