@@ -121,6 +121,9 @@ int nfx_default_tiles(nfx_opts* opts);
 int nfx_sort_workspace_bytes(const nfx_opts* opts, int64_t M, size_t* bytes);
 int nfx_sort_points(const nfx_opts* opts, const void* x, const void* y, const void* z, int64_t M, void* workspace,
                     size_t workspace_bytes, void* stream);
+/* Kernels one nfx_sort_points call launches for these options and M (type3 != 0:
+ * a type-3 source or target sort inside nfx_nufft3); host-only query. */
+int nfx_sort_kernel_count(const nfx_opts* opts, int64_t M, int type3, int* n);
 /* Copy the sort results out of a workspace (device pointers, any may be NULL):
  * keys[M] (bin of each point, input order), perm[M] (int32) and
  * bin_start[nbins + 1]. */
@@ -301,7 +304,7 @@ int nfx_batch_deconv(int precision, int pad, const void* dev_table, int nprob, i
  * of all type-2 problems, the type-1 FFTs and one crop launch for all of them.
  * fac[d]: the problem's deconvolution factors (as nfx_deconv_*); fw: its fine
  * grid buffer; workspace: its sort workspace (nfx_sort_workspace_bytes with
- * its nf).  The problem table is built in `host_staging` (pinned host memory of
+ * its nf and default tiles, max_subproblem 0).  The problem table is built in `host_staging` (pinned host memory of
  * nfx_wave_table_bytes) and copied to `dev_table` asynchronously: both must stay
  * untouched until the wave's work on the stream is done.  The FFTs use the
  * stream's cuFFT work area (as nfx_fft), so a capturing stream is refused. */

@@ -114,6 +114,7 @@ _SIGNATURES = {
     "nfx_device_status": ([POINTER(c_int)], c_int),
     "nfx_selftest_bounded_wait": ([POINTER(c_int)], c_int),
     "nfx_capture_id": ([c_void_p, POINTER(ctypes.c_ulonglong)], c_int),
+    "nfx_sort_kernel_count": ([POINTER(NfxOpts), c_int64, c_int, POINTER(c_int)], c_int),
     "nfx_es_poly": ([c_int, c_double, c_double, POINTER(ctypes.c_float), POINTER(c_int), POINTER(c_double)], c_int),
     "nfx_default_tiles": ([POINTER(NfxOpts)], c_int),
     "nfx_sort_workspace_bytes": ([POINTER(NfxOpts), c_int64, POINTER(c_size_t)], c_int),

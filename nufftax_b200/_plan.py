@@ -101,27 +101,15 @@ def _make_opts(precision: int, nf: Sequence[int], kp: KernelParams, prenorm: boo
 
 
 def sort_launches(opts, M: int, type3: bool = False) -> int:
-    """Kernels one nfx_sort_points call launches: keys (with the first digit's
-    counts), per radix pass a column scan and a scatter (plus a count for the
-    passes after the first), the sorted-coordinates gather (double precision
-    and type-3 points only: float coordinates ride through the passes), bin
-    bounds (unless the last pass's digit is the bin: that pass writes them) and
-    subproblems.  The composite key is bin << cell_bits | cell; digits have at
-    most 11 bits."""
-    if M == 0:
-        return 2
-    nbins = ncell = 1
-    for d in range(int(opts.dim)):
-        t = int(opts.tile[d])
-        nbins *= -(-int(opts.nf[d]) // t)
-        ncell *= t
-    cbits = (ncell - 1).bit_length()
-    bits = max(1, cbits + (nbins - 1).bit_length())
-    npass = 1 if bits <= 11 else (2 if bits <= 22 else 3)
-    dbits = -(-bits // npass)
-    gather = type3 or int(opts.precision) != _lib.NFX_F32
-    bounds = (npass - 1) * dbits != cbits
-    return 3 * npass + 1 + int(gather) + int(bounds)
+    """Kernels one nfx_sort_points call launches (the library's own count for
+    these options, M and point kind): keys with the first digit's counts, per
+    radix pass a column scan and a scatter (plus a count for the passes after
+    the first), the sorted-coordinates gather (double and type-3 points only),
+    bin bounds (unless the last pass writes them) and subproblems."""
+    n = c_int(0)
+    _lib.check(_lib.load().nfx_sort_kernel_count(byref(opts), int(M), int(bool(type3)), byref(n)),
+               "nfx_sort_kernel_count")
+    return int(n.value)
 
 
 class PointSort:

@@ -798,8 +798,14 @@ static int wave_layout(const nfx_opts* common, const nfx_wave_item* items, int n
       set_error("nfx_wave: kind must be 1 or 2");
       return NFX_ERR_INVALID;
     }
+    // the item's own grid with the library's default tiles and subproblem size
+    // for it (those of `common` belong to whichever grid they were chosen for)
     nfx_opts o = *common;
-    for (int d = 0; d < 3; ++d) o.nf[d] = it.nf[d];
+    for (int d = 0; d < 3; ++d) {
+      o.nf[d] = it.nf[d];
+      o.tile[d] = 0;
+    }
+    o.max_subproblem = 0;
     Prepared P;
     int st = prepare(&o, it.M, it.x, it.y, it.z, it.workspace, it.workspace_bytes, P);
     if (st != NFX_OK) return st;
@@ -948,6 +954,26 @@ int nfx_selftest_bounded_wait(int* status) {
     return NFX_ERR_CUDA;
   }
   return nfx_device_status(status);
+}
+
+int nfx_sort_kernel_count(const nfx_opts* opts, int64_t M, int type3, int* n) {
+  using namespace nfx;
+  if (n == nullptr || M < 0) {
+    set_error("n is NULL or M < 0");
+    return NFX_ERR_INVALID;
+  }
+  nfx_opts o;
+  int st = resolve_opts(opts, o);
+  if (st != NFX_OK) return st;
+  Geom g;
+  fill_geom(&o, g);
+  g.t3_mode = type3 ? 1 : 0;
+  SortLayout L;
+  make_layout(o, g, M, L);
+  const bool carry = L.off_coord_tmp[0] != 0;
+  const bool fused_bounds = M > 0 && (int64_t)(L.npass - 1) * L.dbits == L.cbits;
+  *n = M == 0 ? 2 : 1 + 2 * L.npass + (L.npass - 1) + (carry ? 0 : 1) + (fused_bounds ? 0 : 1) + 1;
+  return NFX_OK;
 }
 
 int nfx_capture_id(void* stream, unsigned long long* id) {

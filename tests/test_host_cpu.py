@@ -292,3 +292,22 @@ def test_batch_info_host_side():
     b = info_for([(1000, (64, 64)), (50_000, (256, 192))])
     assert a.table_bytes > 0 and a.smem_bytes > 0 and a.max_subs >= 1
     assert b.table_bytes > a.table_bytes and b.max_subs > a.max_subs
+
+
+def test_sort_kernel_count():
+    """The library's count of the kernels one sort launches: 2D 1024^2 with 32^2
+    tiles is two 10-bit passes (keys, 2 x (scan, scatter), count, subproblems;
+    the coordinates ride through the passes and the last pass writes the bin
+    starts); a 3D 320^3 sort three 8-bit passes plus bin bounds; type-3 and
+    double points add the coordinate gather; an empty sort runs bin bounds and
+    subproblems only."""
+    from nufftax_b200._plan import make_opts, sort_launches
+
+    kp = nb.compute_kernel_params(1e-6)
+    o2 = make_opts(_lib.NFX_F32, (1024, 1024), kp, True)
+    assert sort_launches(o2, 4_000_000) == 7
+    assert sort_launches(o2, 4_000_000, type3=True) == 8
+    assert sort_launches(make_opts(_lib.NFX_F64, (1024, 1024), kp, True), 4_000_000) == 8
+    o3 = make_opts(_lib.NFX_F32, (320, 320, 320), kp, True)
+    assert sort_launches(o3, 10_000) == 11
+    assert sort_launches(o2, 0) == 2
