@@ -42,12 +42,14 @@
 namespace nfx {
 
 // Lanes of the warp holding the same key as this lane: one ballot per key bit.
-// Keys are in [-1, nkeys); the +1 shift keeps the inactive lanes (-1) apart
-// from every real key within `nbits` = bit length of nkeys.
-__device__ __forceinline__ unsigned peer_mask(int key, int nbits) {
+// Keys are in [-1, 2^NB - 1); the +1 shift keeps the inactive lanes (-1) apart
+// from every real key within NB bits (a compile-time count: fully unrolled).
+template <int NB>
+__device__ __forceinline__ unsigned peer_mask(int key) {
   const unsigned k = (unsigned)(key + 1);
   unsigned m = 0xffffffffu;
-  for (int b = 0; b < nbits; ++b) {
+#pragma unroll
+  for (int b = 0; b < NB; ++b) {
     const unsigned bit = (k >> b) & 1u;
     const unsigned bal = __ballot_sync(0xffffffffu, bit);
     m &= bit ? bal : ~bal;
@@ -269,8 +271,9 @@ struct RadixPayload {
 // chunks before this one; totals[d]: digit-d elements overall.  PD payload
 // arrays move with the elements (pay).  bstart (not nullptr only in a last
 // pass whose digit is the bin): CTA 0 writes the bin starts (the exclusive
-// scan of the digit totals), bstart[0..nbins].
-template <int DPT, int PD>
+// scan of the digit totals), bstart[0..nbins].  DB = dbits (compile time, so
+// the ranking's ballots unroll); DPT = digits per thread, max(1, 2^DB / 256).
+template <int DB, int PD, int DPT = (((1 << DB) + kRadixThreads - 1) / kRadixThreads)>
 __global__ void __launch_bounds__(kRadixThreads, 3) k_radix_scatter(const int* __restrict__ kin,
                                                                 const int* __restrict__ vin, int M, int shift,
                                                                 int dbits, const int* __restrict__ prefix,
@@ -281,8 +284,8 @@ __global__ void __launch_bounds__(kRadixThreads, 3) k_radix_scatter(const int* _
   extern __shared__ int smem[];
   __shared__ int s_warp[32];
   constexpr int W = kRadixThreads / 32;
-  const int B = 1 << dbits;
-  const int mask = B - 1;
+  constexpr int B = 1 << DB;
+  constexpr int mask = B - 1;
   int* s_hw = smem;                                 // [W][B] per-warp digit counts
   int* s_key = smem;                                // [kRadixChunk] staged keys (after ranking)
   int* s_val = smem + kRadixChunk;                  // [kRadixChunk] staged values
@@ -294,13 +297,13 @@ __global__ void __launch_bounds__(kRadixThreads, 3) k_radix_scatter(const int* _
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int c0 = ch * kRadixChunk;
   const int wbase = c0 + w * (kRadixItems * 32);
-  int key[kRadixItems], val[kRadixItems], rk[kRadixItems];
+  // keys now; values (and payload) only when the chunk is staged, so that the
+  // unrolled ranking does not hold them in registers
+  int key[kRadixItems], rk[kRadixItems];
 #pragma unroll
   for (int r = 0; r < kRadixItems; ++r) {
     const int p = wbase + r * 32 + lane;
-    const bool valid = p < M;
-    key[r] = valid ? kin[p] : -1;
-    val[r] = valid ? (vin != nullptr ? vin[p] : p) : 0;
+    key[r] = p < M ? kin[p] : -1;
   }
   // this thread's digits (a contiguous range): their totals and the counts of
   // the chunks before this one, fetched now so the loads overlap the ranking
@@ -322,11 +325,11 @@ __global__ void __launch_bounds__(kRadixThreads, 3) k_radix_scatter(const int* _
   // group reads the old count from that lane
   const unsigned lt = (1u << lane) - 1u;
   int* hw = s_hw + w * B;
-  const int dbits1 = dbits + 1;  // digits shifted by one so the invalid lanes (-1) stay apart
 #pragma unroll
   for (int r = 0; r < kRadixItems; ++r) {
     const int d = key[r] >= 0 ? (key[r] >> shift) & mask : -1;
-    const unsigned peers = peer_mask(d, dbits1);
+    // DB + 1 bits: digits shifted by one so the invalid lanes (-1) stay apart
+    const unsigned peers = peer_mask<DB + 1>(d);
     const int rank = __popc(peers & lt);
     int pos = 0;
     if (d >= 0 && rank == 0) pos = atomicAdd(&hw[d], __popc(peers));
@@ -379,11 +382,19 @@ __global__ void __launch_bounds__(kRadixThreads, 3) k_radix_scatter(const int* _
     }
   }
   __syncthreads();  // the per-warp counts are dead: the region now holds the staged chunk
+  {
+    int val[kRadixItems];
 #pragma unroll
-  for (int r = 0; r < kRadixItems; ++r) {
-    if (key[r] >= 0) {
-      s_key[rk[r]] = key[r];
-      s_val[rk[r]] = val[r];
+    for (int r = 0; r < kRadixItems; ++r) {
+      const int p = wbase + r * 32 + lane;
+      val[r] = key[r] >= 0 ? (vin != nullptr ? vin[p] : p) : 0;
+    }
+#pragma unroll
+    for (int r = 0; r < kRadixItems; ++r) {
+      if (key[r] >= 0) {
+        s_key[rk[r]] = key[r];
+        s_val[rk[r]] = val[r];
+      }
     }
   }
 #pragma unroll
@@ -412,19 +423,29 @@ __global__ void __launch_bounds__(kRadixThreads, 3) k_radix_scatter(const int* _
   }
 }
 
-// The scatter instantiation for 2^dbits digits and PD payload arrays.
+// The scatter instantiation for dbits-bit digits (1..11) and PD payload arrays.
 using ScatterFn = void (*)(const int*, const int*, int, int, int, const int*, const int*, int*, int*, RadixPayload,
                            int*, int);
 template <int PD>
-static ScatterFn scatter_for_digits(int B) {
-  return B <= kRadixThreads ? k_radix_scatter<1, PD>
-                            : (B <= 2 * kRadixThreads ? k_radix_scatter<2, PD>
-                                                      : (B <= 4 * kRadixThreads ? k_radix_scatter<4, PD>
-                                                                                : k_radix_scatter<8, PD>));
+static ScatterFn scatter_for_digits(int dbits) {
+  switch (dbits) {
+    case 1: return k_radix_scatter<1, PD>;
+    case 2: return k_radix_scatter<2, PD>;
+    case 3: return k_radix_scatter<3, PD>;
+    case 4: return k_radix_scatter<4, PD>;
+    case 5: return k_radix_scatter<5, PD>;
+    case 6: return k_radix_scatter<6, PD>;
+    case 7: return k_radix_scatter<7, PD>;
+    case 8: return k_radix_scatter<8, PD>;
+    case 9: return k_radix_scatter<9, PD>;
+    case 10: return k_radix_scatter<10, PD>;
+    default: return k_radix_scatter<11, PD>;
+  }
 }
-static ScatterFn scatter_for(int B, int PD) {
-  return PD == 0 ? scatter_for_digits<0>(B)
-                 : (PD == 1 ? scatter_for_digits<1>(B) : (PD == 2 ? scatter_for_digits<2>(B) : scatter_for_digits<3>(B)));
+static ScatterFn scatter_for(int dbits, int PD) {
+  return PD == 0 ? scatter_for_digits<0>(dbits)
+                 : (PD == 1 ? scatter_for_digits<1>(dbits)
+                            : (PD == 2 ? scatter_for_digits<2>(dbits) : scatter_for_digits<3>(dbits)));
 }
 
 // ---- (3) bin starts and subproblems ----------------------------------------
@@ -672,7 +693,7 @@ cudaError_t launch_sort(const SortLayout& L, const Geom& g, int ns, const void* 
   if (M > 0) {
     const size_t hist_smem = (size_t)B * sizeof(int);
     // digits per thread of the scatter: 2^dbits / 256, at least 1
-    const ScatterFn scatter = scatter_for(B, PD);
+    const ScatterFn scatter = scatter_for(L.dbits, PD);
     e = ensure_smem(reinterpret_cast<const void*>(scatter), radix_smem_bytes(B, PD));
     if (e == cudaSuccess) e = prefer_max_smem(reinterpret_cast<const void*>(scatter));
     if (e != cudaSuccess) return e;
