@@ -143,6 +143,10 @@ class PointSort:
         with torch.cuda.device(self.device), span("nfx_sort_points", self.device, launches):
             _lib.check(lib.nfx_sort_points(byref(self.opts), *self._xyz(), self.M, ptr(self.ws), self.ws_bytes,
                                            c_void_p(stream_of(self.device))), "nfx_sort_points")
+            # marks the sort's completion on its stream: a user on another stream
+            # waits for it (sort_cache does that)
+            self.ready = torch.cuda.Event()
+            self.ready.record(torch.cuda.current_stream(self.device))
 
     # -- helpers -----------------------------------------------------------
     def _xyz(self):
@@ -245,15 +249,16 @@ class _SortCache:
     transform on those coordinates reuses the old sort and drops every point
     that left its tile.
 
-    A cached sort may be used from another stream than the one that made it;
-    its workspace is then recorded on that stream, so an eviction cannot hand
-    the memory to new work while the other stream's kernels still read it.
+    A cached sort may be used from another stream than the one that made it:
+    that stream first waits for the sort's completion event, and the workspace
+    is recorded on it, so an eviction cannot hand the memory to new work while
+    the other stream's kernels still read it.
 
     During a CUDA graph capture a sort has only been captured, not run: it
     belongs to the graph and never enters this cache.  It is reused only by
-    later transforms of the same capture on the same stream (so every replay
-    runs the sort before its users), e.g. a type 2 after a type 1 on the same
-    points; those entries are keyed by the capture's id."""
+    later transforms of the same capture (keyed by the capture's id), e.g. a
+    type 2 after a type 1 on the same points, on another stream of the capture
+    through the same event wait (a dependency inside the graph)."""
 
     def __init__(self, size: int = 4):
         self.size = size
@@ -267,10 +272,12 @@ class _SortCache:
         s = stream_of(dev)
         cid = ctypes.c_ulonglong(0)
         _lib.check(_lib.load().nfx_capture_id(c_void_p(s), byref(cid)), "nfx_capture_id")
-        ckey = (int(cid.value), s) + key
+        ckey = (int(cid.value),) + key
         with self._lock:
             hit = self._cap.get(ckey)
         if hit is not None and all(a is b for a, b in zip(hit._src, coords)):
+            if hit.stream != s:
+                torch.cuda.current_stream(dev).wait_event(hit.ready)
             return hit
         ps = PointSort(coords, nf, kp, prenorm)
         ps._src = list(coords)
@@ -295,7 +302,9 @@ class _SortCache:
             if hit is not None:
                 s = stream_of(hit.device)
                 if s != hit.stream:
-                    hit.ws.record_stream(torch.cuda.ExternalStream(s, device=hit.device))
+                    cur = torch.cuda.ExternalStream(s, device=hit.device)
+                    cur.wait_event(hit.ready)
+                    hit.ws.record_stream(cur)
                 return hit
         ps = PointSort(coords, nf, kp, prenorm)
         ps._src = list(coords)

@@ -247,6 +247,60 @@ def test_public_api_under_graph_capture():
     del g
 
 
+def test_sort_shared_across_streams():
+    """A type 1 on one stream and a type 2 on another on the same points share
+    one sort: the second stream waits for the sort's completion event (eager),
+    or joins it inside the graph (capture); both match the one-stream results."""
+    dev = cuda_device()
+    rng = np.random.default_rng(32)
+    M, nm = 200_000, (96, 80)
+    x = torch.from_numpy(rng.uniform(-np.pi, np.pi, M).astype(np.float32)).to(dev)
+    y = torch.from_numpy(rng.uniform(-np.pi, np.pi, M).astype(np.float32)).to(dev)
+    c = torch.from_numpy((rng.standard_normal(M) + 1j * rng.standard_normal(M)).astype(np.complex64)).to(dev)
+    f = torch.from_numpy((rng.standard_normal(nm[::-1]) + 1j * rng.standard_normal(nm[::-1])).astype(
+        np.complex64)).to(dev)
+    nb.sort_cache.clear()
+    ref1 = nb.nufft2d1(x, y, c, nm).cpu().numpy()
+    ref2 = nb.nufft2d2(x, y, f).cpu().numpy()
+    sa, sb = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+
+    def two_streams(xs, ys):
+        cur = torch.cuda.current_stream(dev)
+        sa.wait_stream(cur)
+        sb.wait_stream(cur)
+        with torch.cuda.stream(sa):
+            o1 = nb.nufft2d1(xs, ys, c, nm)
+        with torch.cuda.stream(sb):
+            o2 = nb.nufft2d2(xs, ys, f)
+        cur.wait_stream(sa)
+        cur.wait_stream(sb)
+        return o1, o2
+
+    for rep in range(3):
+        nb.sort_cache.clear()
+        xs, ys = x.clone(), y.clone()
+        with profiling.record() as rec:
+            o1, o2 = two_streams(xs, ys)
+        torch.cuda.synchronize()
+        assert sum(1 for e in rec.events if e[0] == "nfx_sort_points") == 1
+        assert rel_l2(o1.cpu().numpy(), ref1) <= 1e-6
+        assert rel_l2(o2.cpu().numpy(), ref2) <= 1e-6
+    nb.sort_cache.clear()
+    xs, ys = x.clone(), y.clone()
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with profiling.record() as rec:
+        with torch.cuda.graph(g):
+            o1, o2 = two_streams(xs, ys)
+    assert sum(1 for e in rec.events if e[0] == "nfx_sort_points") == 1
+    for _ in range(2):
+        g.replay()
+        torch.cuda.synchronize()
+        assert rel_l2(o1.cpu().numpy(), ref1) <= 1e-6
+        assert rel_l2(o2.cpu().numpy(), ref2) <= 1e-6
+    del g
+
+
 def test_malformed_request_fails_alone():
     """A request whose inputs do not match its description gets `error` set and no
     result; the requests around it complete correctly and the budget is released."""
