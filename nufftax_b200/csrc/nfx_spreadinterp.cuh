@@ -627,6 +627,51 @@ struct Vec16<double> {
   using type = double2;
 };
 
+// The tile of the plane-owner spread holds interleaved complex cells (one
+// 8- or 16-byte load and store per cell update).  Flushed like flush_tile.
+template <typename T>
+__device__ __forceinline__ void flush_tile_c(const Geom& g, const int o[3], const cplx_t<T>* s_tile,
+                                             cplx_t<T>* __restrict__ out) {
+  const int row = g.pitch;
+  const int plane = g.pitch * g.pad[1];
+  const int nrows = g.pad[1] * g.pad[2];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int r = warp; r < nrows; r += nw) {
+    const int ly = r % g.pad[1];
+    const int lz = r / g.pad[1];
+    const int gy = wrap_up(o[1] + ly, g.nf[1]);
+    const int gz = wrap_up(o[2] + lz, g.nf[2]);
+    cplx_t<T>* dst = out + ((int64_t)gz * g.nf[1] + gy) * g.nf[0];
+    const cplx_t<T>* src = s_tile + lz * plane + ly * row;
+    for (int lx = lane; lx < g.pad[0]; lx += 32) {
+      const cplx_t<T> v = src[lx];
+      if (v.x != (T)0 || v.y != (T)0) red_add(dst + wrap_up(o[0] + lx, g.nf[0]), v);
+    }
+  }
+}
+
+// A non-negative int carried in a real's bits (read back as the low int of the
+// real's bytes).
+template <typename T>
+__device__ __forceinline__ T int_bits(int v) {
+  if constexpr (sizeof(T) == 4)
+    return __int_as_float(v);
+  else
+    return __longlong_as_double((long long)v);
+}
+
+// Row pitch (cells) of the plane-owner tile: at ns = 8 (complex64) lanes
+// 0-15 of an update touch two rows 1 apart, so a pitch of 8 mod 16 cells puts
+// their 64-byte segments in opposite halves of the banks; at ns = 4 the four
+// rows of a half-warp need a pitch of 4 mod 8.  Other widths and complex128
+// keep the tile's own pitch.
+__host__ __device__ inline int owner_pitch(int pitch, int pad0, int ns, int real_bytes) {
+  if (real_bytes != 4) return pitch;
+  if (ns == 8) return pad0 + ((8 - pad0 % 16) + 16) % 16;
+  if (ns == 4) return pad0 + ((4 - pad0 % 8) + 8) % 8;
+  return pitch;
+}
+
 template <typename T, int NS, int NW>
 __device__ __forceinline__ void spread_subproblem_owner(const PointArgs<T>& a, const cplx_t<T>* __restrict__ c,
                                                         cplx_t<T>* __restrict__ fw, int sidx,
@@ -638,13 +683,20 @@ __device__ __forceinline__ void spread_subproblem_owner(const PointArgs<T>& a, c
   constexpr int SLOT = owner_slot_reals((int)sizeof(T), NS);
   constexpr int YO = 2 * NS;                 // y weights
   constexpr int ZO = YO + owner_pad(NS, R);  // z weights
-  constexpr int OO = ZO + owner_pad(NS, R);  // origin (offset, z)
+  constexpr int OO = ZO + owner_pad(NS, R);  // origin (offset, z) as raw int bits
   constexpr int NT = NW * 32;
+  // cells of one footprint plane handled by this lane: column kx = lane % NS
+  // and rows ky0 + i * LPR (i < IT): at NS = 8 one update touches rows
+  // 0-3 (lanes 0-31), the next rows 4-7
+  constexpr int LPR = 32 / NS;             // row blocks (lanes per column)
+  constexpr int IT = (NS + LPR - 1) / LPR;  // rows per lane per plane
+  // y weights in pair order (w_y[ky0], w_y[ky0 + LPR]) when a lane's two rows
+  // are LPR apart and cover the NS rows exactly (NS = 8): one 8-byte load
+  constexpr bool PAIRS = IT == 2 && 2 * LPR == NS;
   const Geom& g = a.g;
   const int tile_cells = g.pad[2] * g.pad[1] * g.pitch;
-  T* s_re = reinterpret_cast<T*>(smem_raw);
-  T* s_im = s_re + tile_cells;
-  T* s_st = s_re + owner_pad(2 * tile_cells, R);  // [NT][SLOT], 16-byte aligned
+  CT* s_tile = reinterpret_cast<CT*>(smem_raw);
+  T* s_st = reinterpret_cast<T*>(smem_raw) + owner_pad(2 * tile_cells, R);  // [NT][SLOT], 16-byte aligned
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   const int row = g.pitch;
@@ -654,16 +706,11 @@ __device__ __forceinline__ void spread_subproblem_owner(const PointArgs<T>& a, c
   const int k1 = min(k0 + a.s.maxsub, a.s.bin_start[b + 1]);
   int o[3];
   bin_origin(g, b, o[0], o[1], o[2]);
-  // cells of one footprint plane handled by this lane: column kx = lane % NS,
-  // rows ky0 * IT .. ky0 * IT + IT - 1 with ky0 = lane / NS (LPR row blocks
-  // cover the NS rows; at NS = 8 one instruction touches rows 0, 2, 4, 6)
-  constexpr int LPR = 32 / NS;             // row blocks (lanes per column)
-  constexpr int IT = (NS + LPR - 1) / LPR;  // rows per lane per plane
   const int kx = lane % NS;
   const int ky0 = lane / NS;
   const bool lane_on = ky0 < LPR;
   for (int t = 0; t < a.n_trans; ++t) {
-    for (int i = threadIdx.x; i < 2 * tile_cells; i += blockDim.x) s_re[i] = (T)0;
+    for (int i = threadIdx.x; i < tile_cells; i += blockDim.x) s_tile[i] = CT{(T)0, (T)0};
     for (int kb = k0; kb < k1; kb += NT) {
       const int k = kb + threadIdx.x;
       if (k < k1) {
@@ -685,11 +732,17 @@ __device__ __forceinline__ void spread_subproblem_owner(const PointArgs<T>& a, c
         for (int q = 0; q < NS; ++q) {
           v[2 * q] = cv.x * w[0][q];
           v[2 * q + 1] = cv.y * w[0][q];
-          v[YO + q] = w[1][q];
           v[ZO + q] = w[2][q];
         }
-        v[OO] = (T)off;
-        v[OO + 1] = (T)(off / plane);  // z of the footprint origin in the tile
+#pragma unroll
+        for (int q = 0; q < NS; ++q) {
+          if constexpr (PAIRS)
+            v[YO + 2 * (q % LPR) + q / LPR] = w[1][q];
+          else
+            v[YO + q] = w[1][q];
+        }
+        v[OO] = int_bits<T>(off);
+        v[OO + 1] = int_bits<T>(off / plane);  // z of the footprint origin in the tile
         V16* sp = reinterpret_cast<V16*>(s_st + threadIdx.x * SLOT);
 #pragma unroll
         for (int i = 0; i < SLOT / R; ++i) {
@@ -710,9 +763,9 @@ __device__ __forceinline__ void spread_subproblem_owner(const PointArgs<T>& a, c
       const int cnt = min(NT, k1 - kb);
       for (int j = 0; j < cnt; ++j) {
         const T* sp = s_st + j * SLOT;
-        const CT org = *reinterpret_cast<const CT*>(sp + OO);  // (offset, z)
-        const int off = (int)org.x;
-        const int oz = (int)org.y;
+        const int* so = reinterpret_cast<const int*>(sp + OO);
+        const int off = so[0];
+        const int oz = so[sizeof(T) / sizeof(int)];
         // this warp's planes inside [oz, oz + NS)
         for (int dz = ((warp - oz) % NW + NW) % NW; dz < NS; dz += NW) {
           const T wz = sp[ZO + dz];
@@ -720,22 +773,24 @@ __device__ __forceinline__ void spread_subproblem_owner(const PointArgs<T>& a, c
           const CT cx = *reinterpret_cast<const CT*>(sp + 2 * kx);  // c * w_x[kx]
           if (lane_on) {
             T wyr[IT];
-            if constexpr (IT == 2) {
+            if constexpr (PAIRS) {
               const CT pr = *reinterpret_cast<const CT*>(sp + YO + 2 * ky0);
               wyr[0] = pr.x;
               wyr[1] = pr.y;
             } else {
 #pragma unroll
-              for (int i = 0; i < IT; ++i) wyr[i] = sp[YO + ky0 * IT + i];
+              for (int i = 0; i < IT; ++i) wyr[i] = ky0 + i * LPR < NS ? sp[YO + ky0 + i * LPR] : (T)0;
             }
 #pragma unroll
             for (int i = 0; i < IT; ++i) {
-              const int ky = ky0 * IT + i;
+              const int ky = ky0 + i * LPR;
               if (ky < NS) {
                 const T wy = wz * wyr[i];
-                const int addr = base + ky * row;
-                s_re[addr] += wy * cx.x;
-                s_im[addr] += wy * cx.y;
+                CT* cell = s_tile + base + ky * row;
+                CT u = *cell;
+                u.x += wy * cx.x;
+                u.y += wy * cx.y;
+                *cell = u;
               }
             }
           }
@@ -743,7 +798,7 @@ __device__ __forceinline__ void spread_subproblem_owner(const PointArgs<T>& a, c
       }
       __syncthreads();
     }
-    flush_tile<T>(g, o, s_re, s_im, fw + (int64_t)t * a.grid_stride);
+    flush_tile_c<T>(g, o, s_tile, fw + (int64_t)t * a.grid_stride);
     __syncthreads();
   }
 }
@@ -1456,10 +1511,13 @@ struct Launch {
       // shared-memory atomics) or one warp (lanes own footprint columns)
       const bool sparse = a.M < (int64_t)a.g.nf[0] * a.g.nf[1] * a.g.nf[2];
       if (a.g.spread_mode == NFX_PER_POINT_CTA || (a.g.spread_mode == NFX_PER_POINT_AUTO && sparse)) {
-        const size_t smem = owner_smem_bytes(sizeof(T), NS, NW, a.g);
-        cudaError_t e = prep(k_spread_owner<T, NS, NW>, smem, grid, a.s.max_subs);
+        // the tile's row pitch is this kernel's own (footprint offsets follow it)
+        PointArgs<T> ao = a;
+        ao.g.pitch = owner_pitch(a.g.pitch, a.g.pad[0], NS, (int)sizeof(T));
+        const size_t smem = owner_smem_bytes(sizeof(T), NS, NW, ao.g);
+        cudaError_t e = prep(k_spread_owner<T, NS, NW>, smem, grid, ao.s.max_subs);
         if (e != cudaSuccess) return e;
-        k_spread_owner<T, NS, NW><<<grid, NW * 32, smem, st>>>(a, c, fw);
+        k_spread_owner<T, NS, NW><<<grid, NW * 32, smem, st>>>(ao, c, fw);
         return cudaGetLastError();
       }
     }
