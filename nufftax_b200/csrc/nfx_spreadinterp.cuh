@@ -761,13 +761,27 @@ __device__ __forceinline__ void spread_subproblem_owner(const PointArgs<T>& a, c
       }
       __syncthreads();  // also orders the tile zeroing before the first adds
       const int cnt = min(NT, k1 - kb);
+      static_assert((NW & (NW - 1)) == 0, "warps per CTA a power of two");
+      // planes of each footprint this warp owns: dz0 + pl * NW < NS, at most
+      // ceil(NS / NW) (exactly NS / NW when NW divides NS)
+      constexpr int PLANES = (NS + NW - 1) / NW;
       for (int j = 0; j < cnt; ++j) {
         const T* sp = s_st + j * SLOT;
-        const int* so = reinterpret_cast<const int*>(sp + OO);
-        const int off = so[0];
-        const int oz = so[sizeof(T) / sizeof(int)];
-        // this warp's planes inside [oz, oz + NS)
-        for (int dz = ((warp - oz) % NW + NW) % NW; dz < NS; dz += NW) {
+        int off, oz;
+        if constexpr (sizeof(T) == 4) {
+          const int2 so = *reinterpret_cast<const int2*>(sp + OO);  // 8-byte aligned: OO is a multiple of 4
+          off = so.x;
+          oz = so.y;
+        } else {
+          const int* so = reinterpret_cast<const int*>(sp + OO);
+          off = so[0];
+          oz = so[2];
+        }
+        const int dz0 = (warp - oz) & (NW - 1);
+#pragma unroll
+        for (int pl = 0; pl < PLANES; ++pl) {
+          const int dz = dz0 + pl * NW;
+          if (NS % NW != 0 && dz >= NS) break;
           const T wz = sp[ZO + dz];
           const int base = off + dz * plane + kx;
           const CT cx = *reinterpret_cast<const CT*>(sp + 2 * kx);  // c * w_x[kx]
