@@ -1345,9 +1345,13 @@ __global__ void __launch_bounds__(NW * 32) k_interp_batch(const BatchItem<T>* __
 template <typename T, int DIM, int NS, int NW>
 __global__ void __launch_bounds__(NW * 32) k_grad(PointArgs<T> a, const cplx_t<T>* __restrict__ G,
                                                   const cplx_t<T>* __restrict__ V, cplx_t<T>* __restrict__ out_interp,
-                                                  T* __restrict__ dx, T* __restrict__ dy, T* __restrict__ dz) {
+                                                  T* __restrict__ dx, T* __restrict__ dy, T* __restrict__ dz,
+                                                  const __grid_constant__ CUtensorMap tmap) {
   using CT = cplx_t<T>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t mbar;
+  TmaStage ts{&tmap, smem_addr(&mbar), 0u};
+  if (a.tma) tma_init(&mbar);
   CT* s_tile = reinterpret_cast<CT*>(smem_raw);
   const Geom& g = a.g;
   const int row = g.pitch;
@@ -1362,7 +1366,7 @@ __global__ void __launch_bounds__(NW * 32) k_grad(PointArgs<T> a, const cplx_t<T
     bin_origin(g, b, o[0], o[1], o[2]);
     for (int t = 0; t < a.n_trans; ++t) {
       __syncthreads();
-      stage_tile<T>(g, o, G + (int64_t)t * a.grid_stride, s_tile);
+      if (!stage_interp_tile<T>(a, o, G, t, s_tile, ts)) return;
       __syncthreads();
       // loads pipelined across iterations: the permutation two iterations
       // ahead, folded coordinates (sorted order) and V one iteration ahead
@@ -1543,22 +1547,10 @@ struct Launch {
   }
   template <int MODE>
   static cudaError_t interp_as(const PointArgs<T>& a0, const cplx_t<T>* fw, cplx_t<T>* out, cudaStream_t st) {
+    // the interpolation only reads the tile, so its row pitch is free
     PointArgs<T> a = a0;
     CUtensorMap tmap{};
-    a.tma = 0;
-    if constexpr (DIM >= 2) {
-      // The interpolation only reads the tile, so its row pitch is free: a
-      // complex64 box needs an even one (16-byte rows).
-      Geom gt = a.g;
-      if (sizeof(T) == 4 && (gt.pitch & 1)) ++gt.pitch;
-      if (interp_tile_map(&tmap, sizeof(T), DIM, gt, a.n_trans, fw)) {
-        a.status = device_status_word();
-        if (a.status != nullptr) {
-          a.g = gt;
-          a.tma = 1;
-        }
-      }
-    }
+    tma_args(a, fw, &tmap);
     size_t smem = tile_smem(a.g);
     int grid = 0;
     cudaError_t e = prep(k_interp<T, DIM, NS, NW, MODE>, smem, grid, a.s.max_subs);
@@ -1572,13 +1564,33 @@ struct Launch {
     }
     return interp_as<NFX_PER_POINT_THREAD>(a, fw, out, st);
   }
-  static cudaError_t grad(const PointArgs<T>& a, const cplx_t<T>* G, const cplx_t<T>* V, cplx_t<T>* oi, T* dx, T* dy,
-                          T* dz, cudaStream_t st) {
+  // The tile staging of the interpolation and gradient passes: a tensor map of
+  // the grid for TMA box loads of interior tiles when the rules allow (else
+  // a.tma = 0 and plain loads); a complex64 tile gets an even row pitch.
+  static void tma_args(PointArgs<T>& a, const cplx_t<T>* grid, CUtensorMap* tmap) {
+    a.tma = 0;
+    if constexpr (DIM >= 2) {
+      Geom gt = a.g;
+      if (sizeof(T) == 4 && (gt.pitch & 1)) ++gt.pitch;
+      if (interp_tile_map(tmap, sizeof(T), DIM, gt, a.n_trans, grid)) {
+        a.status = device_status_word();
+        if (a.status != nullptr) {
+          a.g = gt;
+          a.tma = 1;
+        }
+      }
+    }
+  }
+  static cudaError_t grad(const PointArgs<T>& a0, const cplx_t<T>* G, const cplx_t<T>* V, cplx_t<T>* oi, T* dx,
+                          T* dy, T* dz, cudaStream_t st) {
+    PointArgs<T> a = a0;
+    CUtensorMap tmap{};
+    tma_args(a, G, &tmap);
     size_t smem = tile_smem(a.g);
     int grid = 0;
     cudaError_t e = prep(k_grad<T, DIM, NS, NW>, smem, grid, a.s.max_subs);
     if (e != cudaSuccess) return e;
-    k_grad<T, DIM, NS, NW><<<grid, NW * 32, smem, st>>>(a, G, V, oi, dx, dy, dz);
+    k_grad<T, DIM, NS, NW><<<grid, NW * 32, smem, st>>>(a, G, V, oi, dx, dy, dz, tmap);
     return cudaGetLastError();
   }
 };

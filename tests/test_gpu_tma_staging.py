@@ -107,3 +107,38 @@ def test_bounded_wait_gives_up_and_reports():
     ref = O.interp(X, fw_np, kp)
     assert rel_l2(got.reshape(ref.shape), ref) <= 1e-5
     assert _lib.device_status() == 0
+
+
+@pytest.mark.parametrize("case", [0, 2, 4, 5, 6, 7])
+def test_tma_staging_gradient_pass_bit_identical(case):
+    """The fused gradient pass (value + coordinate gradients, both adjoints)
+    stages its tile the same way: TMA and plain staging give identical outputs."""
+    dim, nf, tile, M, ntr, dt, clustered = CASES[case]
+    dev = cuda_device()
+    rng = np.random.default_rng(200 + case)
+    X = [rng.uniform(-np.pi, np.pi, M).astype(dt) for _ in range(dim)]
+    kp = compute_kernel_params(1e-6 if dt == np.float32 else 1e-10, 2.0)
+    cdt = np.complex64 if dt == np.float32 else np.complex128
+    shape = (ntr,) + tuple(reversed(nf))
+    G = torch.from_numpy((rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(cdt)).to(dev)
+    c = torch.from_numpy((rng.standard_normal((ntr, M)) + 1j * rng.standard_normal((ntr, M))).astype(cdt)).to(dev)
+    ps = PointSort([torch.from_numpy(x).to(dev) for x in X], nf, kp, prenorm=True, tile=tile)
+    need = [True] * dim
+
+    def both():
+        dc, dxs = ps.spread_grad(c, G, True, need)
+        ixs = ps.interp_grad(G, c, need)
+        return [dc.clone()] + [d.clone() for d in dxs] + [d.clone() for d in ixs]
+
+    old = os.environ.get("NFX_INTERP_STAGING")
+    try:
+        os.environ["NFX_INTERP_STAGING"] = "plain"
+        plain = both()
+        os.environ.pop("NFX_INTERP_STAGING")
+        tma = both()
+    finally:
+        if old is not None:
+            os.environ["NFX_INTERP_STAGING"] = old
+    assert _lib.device_status() == 0
+    for p_, t_ in zip(plain, tma):
+        assert torch.equal(p_, t_)
