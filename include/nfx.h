@@ -101,10 +101,12 @@ int nfx_capture_id(void* stream, unsigned long long* id);
 /* Polynomial form of the ES weights used by the float kernels (no counterpart
  * in the reference, which evaluates exp/sqrt): coefficients a[q][d] of
  * phi(q - (v + ns - 1) / 2) as a degree-`degree` polynomial in v in [-1, 1],
- * written to coeffs[q * 16 + d]; max_abs_err is the worst float Horner error
- * against the exp/sqrt form.  A fit is used when that error stays within
- * 3e-8 + 2.4e-7 |phi| (two float ulps); degree 0 means none was found and the
- * kernels evaluate exp/sqrt. */
+ * written to coeffs[q * 16 + d] (the polynomial of ns - 1 - q is that of q at
+ * -v); max_abs_err is the worst float error of the kernels' evaluation forms
+ * (Horner in v, and the even / odd split E(v^2) +- v O(v^2)) against the
+ * exp/sqrt form.  A fit is used when that error stays within
+ * 3e-8 + 2.6e-7 |phi| (about two float ulps); degree 0 means none was found and
+ * the kernels evaluate exp/sqrt. */
 int nfx_es_poly(int nspread, double beta, double kc, float* coeffs, int* degree, double* max_abs_err);
 
 /* Fill tile[] with the defaults the library would use (max_subproblem = 0 is

@@ -509,16 +509,19 @@ static int prepare(const nfx_opts* in, int64_t M, const void* x, const void* y, 
 }
 
 // ---------------------------------------------------------------------------
-// Polynomial ES weights (float path): for each q, Chebyshev interpolation of
-// v -> phi(q - (v + ns - 1) / 2) on [-1, 1] at D + 1 nodes, converted to
-// monomials in v; the degree is raised (up to the kernels' evaluation degree)
-// until Horner's rule in float (fmaf, as on the device) is within
-// kPolyAbs + kPolyRel * |phi| of the double exp/sqrt value
-// on a fine grid: two float ulps of the weight plus a small absolute floor (the
+// Polynomial ES weights (float path): for each q < ns / 2, Chebyshev
+// interpolation of v -> phi(q - (v + ns - 1) / 2) on [-1, 1] at D + 1 nodes,
+// converted to monomials in v; weight ns - 1 - q is the same polynomial at -v
+// (phi is even), stored with the odd coefficients negated.  The degree is
+// raised (up to the kernels' evaluation degree) until both forms the kernels
+// evaluate in float (fmaf, as on the device) are within kPolyAbs + kPolyRel *
+// |phi| of the double exp/sqrt value on a fine grid: Horner in v for every q,
+// and the even/odd split E(v^2) +- v O(v^2) that gives weights q and ns - 1 - q
+// together; two float ulps of the weight plus a small absolute floor (the
 // exp/sqrt form in float carries errors of the same size).
 // ---------------------------------------------------------------------------
 constexpr double kPolyAbs = 3e-8;
-constexpr double kPolyRel = 2.4e-7;
+constexpr double kPolyRel = 2.6e-7;
 
 static double es_phi(double z, double beta, double kc) {
   const double arg = 1.0 - kc * z * z;
@@ -530,7 +533,7 @@ static bool fit_es_poly_uncached(int ns, double beta, double kc, EsPoly& out, do
     double worst = 0.0, worst_ratio = 0.0;
     EsPoly P = {};  // coefficients above D stay zero (the kernels run degree kPolyEvalDeg)
     P.deg = D;
-    for (int q = 0; q < ns; ++q) {
+    for (int q = 0; q < ns / 2; ++q) {
       const int n = D + 1;
       double cheb[kPolyMaxDeg + 1] = {0};
       for (int j = 0; j < n; ++j) {
@@ -551,16 +554,34 @@ static bool fit_es_poly_uncached(int ns, double beta, double kc, EsPoly& out, do
       double mono[kPolyMaxDeg + 1] = {0};
       for (int j = 0; j <= D; ++j)
         for (int i = 0; i <= j; ++i) mono[i] += cheb[j] * Tm[j][i];
-      for (int i = 0; i <= D; ++i) P.a[q][i] = (float)mono[i];
-      for (int t = 0; t <= 2000; ++t) {
-        const double v = -1.0 + 2.0 * t / 2000.0;
-        float h = P.a[q][D];
-        for (int d = D - 1; d >= 0; --d) h = std::fmaf(h, (float)v, P.a[q][d]);
-        const double ref = es_phi(q - (v + ns - 1) / 2.0, beta, kc);
-        const double e = std::fabs((double)h - ref);
-        const double ratio = e / (kPolyAbs + kPolyRel * std::fabs(ref));
-        worst = e > worst ? e : worst;
-        worst_ratio = ratio > worst_ratio ? ratio : worst_ratio;
+      for (int i = 0; i <= D; ++i) {
+        P.a[q][i] = (float)mono[i];
+        P.a[ns - 1 - q][i] = (i % 2 == 0) ? P.a[q][i] : -P.a[q][i];
+      }
+    }
+    auto account = [&](float h, double ref) {
+      const double e = std::fabs((double)h - ref);
+      const double ratio = e / (kPolyAbs + kPolyRel * std::fabs(ref));
+      worst = e > worst ? e : worst;
+      worst_ratio = ratio > worst_ratio ? ratio : worst_ratio;
+    };
+    for (int t = 0; t <= 2000; ++t) {
+      const double v = -1.0 + 2.0 * t / 2000.0;
+      const float fv = (float)v;
+      for (int q = 0; q < ns; ++q) {  // Horner in v
+        float h = P.a[q][kPolyEvalDeg];
+        for (int d = kPolyEvalDeg - 1; d >= 0; --d) h = std::fmaf(h, fv, P.a[q][d]);
+        account(h, es_phi(q - (v + ns - 1) / 2.0, beta, kc));
+      }
+      const float u = fv * fv;
+      for (int q = 0; q < ns / 2; ++q) {  // even / odd split, weights q and ns - 1 - q
+        float e = P.a[q][kPolyEvalDeg - 1], o = P.a[q][kPolyEvalDeg];
+        for (int d = kPolyEvalDeg - 3; d >= 0; d -= 2) {
+          e = std::fmaf(e, u, P.a[q][d]);
+          o = std::fmaf(o, u, P.a[q][d + 1]);
+        }
+        account(std::fmaf(fv, o, e), es_phi(q - (v + ns - 1) / 2.0, beta, kc));
+        account(std::fmaf(-fv, o, e), es_phi(ns - 1 - q - (v + ns - 1) / 2.0, beta, kc));
       }
     }
     if (worst_ratio <= 1.0) {

@@ -153,10 +153,13 @@ __device__ __forceinline__ double2 splat2(double s) { return make_double2(s, s);
 // at scaled coordinate xs with left cell i0, every weight phi(i0 + q - xs),
 // q = 0..ns-1, is a smooth function of v = 2 (xs - i0) - (ns - 1) in (-1, 1];
 // a[q][d] are monomial coefficients in v fitted on the host (nfx_es_poly) to
-// within two float ulps of the exp/sqrt form, evaluated by Horner's rule.  The
-// kernels evaluate degree kPolyEvalDeg (coefficients above the fitted degree
-// are zero, which leaves Horner's result unchanged); widths whose weights need
-// a higher degree keep the exp/sqrt form.
+// within about two float ulps of the exp/sqrt form; a[ns - 1 - q] is a[q] at
+// -v (phi is even: odd coefficients negated).  The kernels evaluate degree
+// kPolyEvalDeg (coefficients above the fitted degree are zero, which leaves
+// the result unchanged), a whole footprint's weights as even / odd splits
+// E(v^2) +- v O(v^2) of the first ns / 2 polynomials, single weights by
+// Horner's rule; widths whose weights need a higher degree keep the exp/sqrt
+// form.
 constexpr int kPolyMaxDeg = 15;
 constexpr int kPolyEvalDeg = 7;
 struct EsPoly {

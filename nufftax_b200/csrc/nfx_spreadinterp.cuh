@@ -63,17 +63,30 @@ struct PointArgs {
 template <typename T, int NS>
 __device__ __forceinline__ void axis_weights(const PointArgs<T>& a, int i0, T xs, T* w) {
   if (std::is_same<T, float>::value && a.poly.deg > 0) {
+    // weights q and NS - 1 - q from one even / odd split of polynomial q:
+    // P(+-v) = E(v^2) +- v O(v^2)  (phi is even)
+    static_assert(kPolyEvalDeg % 2 == 1, "odd evaluation degree: E and O of equal length");
     const float v = 2.0f * (float)(xs - (T)i0) - (float)(NS - 1);
-    float h[NS];
+    const float u = v * v;
+    float e[NS / 2], o[NS / 2];
 #pragma unroll
-    for (int q = 0; q < NS; ++q) h[q] = a.poly.a[q][kPolyEvalDeg];
-#pragma unroll
-    for (int d = kPolyEvalDeg - 1; d >= 0; --d) {
-#pragma unroll
-      for (int q = 0; q < NS; ++q) h[q] = fmaf(h[q], v, a.poly.a[q][d]);
+    for (int q = 0; q < NS / 2; ++q) {
+      e[q] = a.poly.a[q][kPolyEvalDeg - 1];
+      o[q] = a.poly.a[q][kPolyEvalDeg];
     }
 #pragma unroll
-    for (int q = 0; q < NS; ++q) w[q] = (T)h[q];
+    for (int d = kPolyEvalDeg - 3; d >= 0; d -= 2) {
+#pragma unroll
+      for (int q = 0; q < NS / 2; ++q) {
+        e[q] = fmaf(e[q], u, a.poly.a[q][d]);
+        o[q] = fmaf(o[q], u, a.poly.a[q][d + 1]);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < NS / 2; ++q) {
+      w[q] = (T)fmaf(v, o[q], e[q]);
+      w[NS - 1 - q] = (T)fmaf(-v, o[q], e[q]);
+    }
   } else {
 #pragma unroll
     for (int q = 0; q < NS; ++q) w[q] = es_weight(rn_sub((T)(i0 + q), xs), a.beta, a.kc);

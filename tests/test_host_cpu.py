@@ -153,7 +153,10 @@ def test_product_does_not_import_oracle():
 @pytest.mark.parametrize("eps", [1e-6, 1e-9, 1e-12])
 def test_es_polynomial_matches_exp_sqrt(eps):
     """The float kernels' polynomial ES weights (nfx_es_poly, host-side fit) stay
-    within two float ulps (+3e-8) of exp(beta (sqrt(1 - c z^2) - 1))."""
+    within about two float ulps (2.6e-7 relative, +3e-8) of
+    exp(beta (sqrt(1 - c z^2) - 1)), by Horner's rule and by the even / odd
+    split the kernels use for whole footprints; weight ns - 1 - q is weight q
+    at -v."""
     lib = _lib.load()
     kp = nb.compute_kernel_params(eps)
     co = (ctypes.c_float * 256)()
@@ -169,7 +172,20 @@ def test_es_polynomial_matches_exp_sqrt(eps):
             h = (h.astype(np.float64) * v + a[q, d]).astype(np.float32)
         z = q - (v.astype(np.float64) + kp.nspread - 1) / 2
         ref = O.es_kernel(z, kp.beta, kp.c)
-        assert np.all(np.abs(h - ref) <= 3e-8 + 2.4e-7 * np.abs(ref) + 1e-7)
+        assert np.all(np.abs(h - ref) <= 3e-8 + 2.6e-7 * np.abs(ref) + 1e-7)
+    ns = kp.nspread
+    sign = np.array([(-1) ** d for d in range(16)], dtype=np.float32)
+    for q in range(ns // 2):
+        assert np.array_equal(a[ns - 1 - q], a[q] * sign)
+        u = (v.astype(np.float64) * v).astype(np.float32)
+        e, o = np.full_like(v, a[q, 6]), np.full_like(v, a[q, 7])
+        for d in (4, 2, 0):
+            e = (e.astype(np.float64) * u + a[q, d]).astype(np.float32)
+            o = (o.astype(np.float64) * u + a[q, d + 1]).astype(np.float32)
+        for s_, qq in ((1.0, q), (-1.0, ns - 1 - q)):
+            w = (np.float64(s_) * v * o + e).astype(np.float32)
+            ref = O.es_kernel(qq - (v.astype(np.float64) + ns - 1) / 2, kp.beta, kp.c)
+            assert np.all(np.abs(w - ref) <= 3e-8 + 2.6e-7 * np.abs(ref) + 1e-7)
 
 
 def test_es_polynomial_refused_for_narrow_kernel():
