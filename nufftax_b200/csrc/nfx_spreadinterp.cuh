@@ -380,15 +380,22 @@ __device__ __forceinline__ void spread_subproblem_runs(const PointArgs<T>& a, co
     const int per = ((k1 - k0 + NW - 1) / NW + 31) / 32 * 32;
     const int w0 = min(k0 + warp * per, k1);
     const int w1 = min(w0 + per, k1);
-    CT acc[RPL];
+    // two accumulator sets (alternate points of a run) halve the FMA
+    // dependency chains; flush_run adds them
+    CT acc[RPL], acc2[RPL];
 #pragma unroll
-    for (int r = 0; r < RPL; ++r) acc[r].x = acc[r].y = (T)0;
+    for (int r = 0; r < RPL; ++r) acc[r].x = acc[r].y = acc2[r].x = acc2[r].y = (T)0;
     int run_off = -1;
     // this lane's first cell (row grp * rpl, column kx) relative to a
     // footprint's origin; -1 for lanes past the groups
     const int rho0 = grp * RPL;
     const int lane_cell = lane_on ? (DIM == 3 ? (rho0 / NS) * plane + (rho0 % NS) * row : rho0 * row) + kx : -1;
     auto flush_run = [&]() {
+#pragma unroll
+      for (int r = 0; r < RPL; ++r) {
+        acc[r].x += acc2[r].x;
+        acc[r].y += acc2[r].y;
+      }
       if (lane_cell >= 0) {
         T* pr = s_re + run_off + lane_cell;
         T* pi = s_im + run_off + lane_cell;
@@ -411,7 +418,7 @@ __device__ __forceinline__ void spread_subproblem_runs(const PointArgs<T>& a, co
         }
       }
 #pragma unroll
-      for (int r = 0; r < RPL; ++r) acc[r].x = acc[r].y = (T)0;
+      for (int r = 0; r < RPL; ++r) acc[r].x = acc[r].y = acc2[r].x = acc2[r].y = (T)0;
     };
     // software pipeline: folded coordinates and strength of this lane's point
     // in the current batch (xn, cn) and the point index of the next batch (pn)
@@ -477,9 +484,9 @@ __device__ __forceinline__ void spread_subproblem_runs(const PointArgs<T>& a, co
         const int je = later != 0u ? min(j + __ffs(later), cnt) : cnt;
         for (; j + 4 <= je; j += 4, sp += 4 * SLOT) {
           add_slot<T, DIM, NS>(sp, kx, grp, acc);
-          add_slot<T, DIM, NS>(sp + SLOT, kx, grp, acc);
+          add_slot<T, DIM, NS>(sp + SLOT, kx, grp, acc2);
           add_slot<T, DIM, NS>(sp + 2 * SLOT, kx, grp, acc);
-          add_slot<T, DIM, NS>(sp + 3 * SLOT, kx, grp, acc);
+          add_slot<T, DIM, NS>(sp + 3 * SLOT, kx, grp, acc2);
         }
         for (; j < je; ++j, sp += SLOT) add_slot<T, DIM, NS>(sp, kx, grp, acc);
       }
