@@ -557,7 +557,7 @@ def run_gpu(args):
         # its own clock record): 1D, the 64-problem batched mix, the
         # differentiated 3D step and a served mixed stream
         line["configs"] = {"plain_1d": measure_1d(dev, 50, 5),
-                           "batched": measure_batched(dev, 10, 3),
+                           "batched": measure_batched(dev, 10, 3, autotune=True),
                            "grad3d": measure_grad3d(dev, 5, 3),
                            "served": measure_serve(dev, args.served_requests, 300, [1.0, 4.0])}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -1149,11 +1149,27 @@ def measure_1d(dev, steps: int, warmup: int) -> dict:
             step()
         b.record()
         torch.cuda.synchronize()
-    ms = a.elapsed_time(b) / steps
+        eager_ms = a.elapsed_time(b) / steps
+        # the same step captured once through the public API and replayed
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            step()
+        for _ in range(max(3, warmup)):
+            graph.replay()
+        torch.cuda.synchronize()
+        a.record()
+        for _ in range(steps):
+            graph.replay()
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / steps
+        del graph
     return {"metric": "1D type-1 + type-2 NU points/s (M=200000, N=8192, eps 1e-6, complex64)", "value": 2 * M / (ms / 1e3),
             "unit": "NU points/s", "ms_per_step": ms, "steps": steps, "warmup": n_warm, "clocks": ck.summary,
-            "note": "inputs resident, back-to-back steps (launch-bound at this size); warm-up runs 1 s under the "
-                    "clock sampler"}
+            "eager_value": 2 * M / (eager_ms / 1e3), "eager_ms_per_step": eager_ms,
+            "note": "inputs resident, back-to-back steps; value: the step replayed from a CUDA graph captured "
+                    "through the public API (sort included); eager: launched from Python, launch-bound at this "
+                    "size; warm-up runs 1 s under the clock sampler"}
 
 
 def _plain(nb, r, dev):
