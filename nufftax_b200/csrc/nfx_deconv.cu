@@ -8,41 +8,55 @@
 // Type 2 (deconvolve.py:114-166, 227-304, 369-468): one pass writes every
 //   cell of the fine grid: the deconvolved mode where the cell is a kept mode,
 //   zero elsewhere (no separate memset of the grid).
+#include <algorithm>
 #include <type_traits>
 
 #include "nfx_internal.h"
 
 namespace nfx {
 
+// Both passes go row by row (a row = one (transform, z, y) line along x, cut
+// into segments of kSeg elements so that long 1D rows still spread over many
+// warps; one warp per segment): the row's indices come from one division chain
+// per segment, the x loop is plain strided adds, so no thread divides per
+// element.
+constexpr int kSeg = 1024;
 template <typename T>
 __global__ void k_deconv_shuffle(int nf1, int nf2, int nf3, int n1, int n2, int n3, const T* __restrict__ f1,
                                  const T* __restrict__ f2, const T* __restrict__ f3,
                                  const cplx_t<T>* __restrict__ in, cplx_t<T>* __restrict__ out, int n_trans) {
   using CT = cplx_t<T>;
-  const int64_t per = (int64_t)n1 * n2 * n3;
-  const int64_t total = per * n_trans;
   const int64_t grid = (int64_t)nf1 * nf2 * nf3;
+  const int nseg = (n1 + kSeg - 1) / kSeg;
+  const int64_t nitems = (int64_t)n2 * n3 * n_trans * nseg;
   const int k1min = -(n1 / 2), k2min = -(n2 / 2), k3min = -(n3 / 2);
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t t = i / per;
-    int64_t r = i - t * per;
-    const int p1 = (int)(r % n1);
-    r /= n1;
-    const int p2 = (int)(r % n2);
-    const int p3 = (int)(r / n2);
-    int i1 = p1 + k1min;
-    int i2 = p2 + k2min;
-    int i3 = p3 + k3min;
-    if (i1 < 0) i1 += nf1;
+  const int nw = blockDim.x >> 5, lane = threadIdx.x & 31;
+  for (int64_t item = (int64_t)blockIdx.x * nw + (threadIdx.x >> 5); item < nitems; item += (int64_t)gridDim.x * nw) {
+    const int64_t row = item / nseg;
+    const int x0 = (int)(item - row * nseg) * kSeg;
+    const int x1 = min(x0 + kSeg, n1);
+    const int64_t t = row / ((int64_t)n2 * n3);
+    const int rr = (int)(row - t * n2 * n3);
+    const int p2 = rr % n2;
+    const int p3 = rr / n2;
+    int i2 = p2 + k2min, i3 = p3 + k3min;
     if (i2 < 0) i2 += nf2;
     if (i3 < 0) i3 += nf3;
-    const CT v = in[t * grid + ((int64_t)i3 * nf2 + i2) * nf1 + i1];
-    T fac = f1[p1];
-    if (f2 != nullptr) fac = (f3 != nullptr ? f3[p3] * f2[p2] : f2[p2]) * f1[p1];
-    CT o;
-    o.x = v.x * fac;
-    o.y = v.y * fac;
-    out[i] = o;
+    T fac23 = (T)1;
+    if (f2 != nullptr) fac23 = f3 != nullptr ? f3[p3] * f2[p2] : f2[p2];
+    const CT* src = in + t * grid + ((int64_t)i3 * nf2 + i2) * nf1;
+    CT* dst = out + row * n1;
+    for (int p1 = x0 + lane; p1 < x1; p1 += 32) {
+      int i1 = p1 + k1min;
+      if (i1 < 0) i1 += nf1;
+      const CT v = src[i1];
+      // (fac3 * fac2) * fac1, the reference's order
+      const T fac = f2 != nullptr ? fac23 * f1[p1] : f1[p1];
+      CT o;
+      o.x = v.x * fac;
+      o.y = v.y * fac;
+      dst[p1] = o;
+    }
   }
 }
 
@@ -51,34 +65,43 @@ __global__ void k_deconv_pad(int nf1, int nf2, int nf3, int n1, int n2, int n3, 
                              const T* __restrict__ f2, const T* __restrict__ f3, const cplx_t<T>* __restrict__ in,
                              cplx_t<T>* __restrict__ out, int n_trans) {
   using CT = cplx_t<T>;
-  const int64_t grid = (int64_t)nf1 * nf2 * nf3;
-  const int64_t total = grid * n_trans;
   const int64_t per = (int64_t)n1 * n2 * n3;
+  const int nseg = (nf1 + kSeg - 1) / kSeg;
+  const int64_t nitems = (int64_t)nf2 * nf3 * n_trans * nseg;
   const int k1max = (n1 - 1) / 2, k2max = (n2 - 1) / 2, k3max = (n3 - 1) / 2;
   const int k1min = -(n1 / 2), k2min = -(n2 / 2), k3min = -(n3 / 2);
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t t = i / grid;
-    int64_t r = i - t * grid;
-    const int c1 = (int)(r % nf1);
-    r /= nf1;
-    const int c2 = (int)(r % nf2);
-    const int c3 = (int)(r / nf2);
-    // mode of this cell per axis, or none
-    const int k1 = c1 <= k1max ? c1 : (c1 >= nf1 + k1min ? c1 - nf1 : INT32_MIN);
+  const int nw = blockDim.x >> 5, lane = threadIdx.x & 31;
+  for (int64_t item = (int64_t)blockIdx.x * nw + (threadIdx.x >> 5); item < nitems; item += (int64_t)gridDim.x * nw) {
+    const int64_t row = item / nseg;
+    const int x0 = (int)(item - row * nseg) * kSeg;
+    const int x1 = min(x0 + kSeg, nf1);
+    const int64_t t = row / ((int64_t)nf2 * nf3);
+    const int rr = (int)(row - t * nf2 * nf3);
+    const int c2 = rr % nf2;
+    const int c3 = rr / nf2;
+    // mode of this row per axis, or none
     const int k2 = c2 <= k2max ? c2 : (c2 >= nf2 + k2min ? c2 - nf2 : INT32_MIN);
     const int k3 = c3 <= k3max ? c3 : (c3 >= nf3 + k3min ? c3 - nf3 : INT32_MIN);
-    CT o;
-    o.x = (T)0;
-    o.y = (T)0;
-    if (k1 != INT32_MIN && k2 != INT32_MIN && k3 != INT32_MIN) {
-      const int p1 = k1 - k1min, p2 = k2 - k2min, p3 = k3 - k3min;
-      const CT v = in[t * per + ((int64_t)p3 * n2 + p2) * n1 + p1];
-      T fac = f1[p1];
-      if (f2 != nullptr) fac = (f3 != nullptr ? f3[p3] * f2[p2] : f2[p2]) * f1[p1];
-      o.x = v.x * fac;
-      o.y = v.y * fac;
+    CT* dst = out + row * nf1;
+    const bool has = k2 != INT32_MIN && k3 != INT32_MIN;
+    const int p2 = has ? k2 - k2min : 0, p3 = has ? k3 - k3min : 0;
+    T fac23 = (T)1;
+    if (has && f2 != nullptr) fac23 = f3 != nullptr ? f3[p3] * f2[p2] : f2[p2];
+    const CT* src = in + t * per + ((int64_t)p3 * n2 + p2) * n1;
+    for (int c1 = x0 + lane; c1 < x1; c1 += 32) {
+      CT o;
+      o.x = (T)0;
+      o.y = (T)0;
+      const int k1 = c1 <= k1max ? c1 : (c1 >= nf1 + k1min ? c1 - nf1 : INT32_MIN);
+      if (has && k1 != INT32_MIN) {
+        const int p1 = k1 - k1min;
+        const CT v = src[p1];
+        const T fac = f2 != nullptr ? fac23 * f1[p1] : f1[p1];
+        o.x = v.x * fac;
+        o.y = v.y * fac;
+      }
+      dst[c1] = o;
     }
-    out[i] = o;
   }
 }
 
@@ -169,12 +192,18 @@ static unsigned elementwise_grid(int64_t n) {
   return (unsigned)(want < cap ? (want > 0 ? want : 1) : cap);
 }
 
+// CTAs for a pass of one warp per row segment over nrows segments (8 warps a
+// CTA), at most 8 CTAs per SM.
+static int row_grid(int64_t nrows) {
+  return (int)std::max<int64_t>(1, std::min<int64_t>((nrows + 7) / 8, (int64_t)num_sms() * 8));
+}
+
 template <typename T>
 cudaError_t launch_deconv_shuffle(int dim, const int nf[3], const int nm[3], const T* f1, const T* f2, const T* f3,
                                   const void* fw_hat, void* out, int n_trans, cudaStream_t st) {
   const int64_t total = (int64_t)nm[0] * nm[1] * nm[2] * n_trans;
   if (total == 0) return cudaSuccess;
-  k_deconv_shuffle<T><<<elementwise_grid(total), 256, 0, st>>>(
+  k_deconv_shuffle<T><<<row_grid((int64_t)nm[1] * nm[2] * n_trans * ((nm[0] + kSeg - 1) / kSeg)), 256, 0, st>>>(
       nf[0], nf[1], nf[2], nm[0], nm[1], nm[2], f1, dim >= 2 ? f2 : nullptr, dim >= 3 ? f3 : nullptr,
       (const cplx_t<T>*)fw_hat, (cplx_t<T>*)out, n_trans);
   return cudaGetLastError();
@@ -185,7 +214,8 @@ cudaError_t launch_deconv_pad(int dim, const int nf[3], const int nm[3], const T
                               const void* f_in, void* fw_hat, int n_trans, cudaStream_t st) {
   const int64_t total = (int64_t)nf[0] * nf[1] * nf[2] * n_trans;
   if (total == 0) return cudaSuccess;
-  k_deconv_pad<T><<<elementwise_grid(total), 256, 0, st>>>(nf[0], nf[1], nf[2], nm[0], nm[1], nm[2], f1,
+  k_deconv_pad<T><<<row_grid((int64_t)nf[1] * nf[2] * n_trans * ((nf[0] + kSeg - 1) / kSeg)), 256, 0, st>>>(
+      nf[0], nf[1], nf[2], nm[0], nm[1], nm[2], f1,
                                                            dim >= 2 ? f2 : nullptr, dim >= 3 ? f3 : nullptr,
                                                            (const cplx_t<T>*)f_in, (cplx_t<T>*)fw_hat, n_trans);
   return cudaGetLastError();
