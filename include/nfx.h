@@ -246,7 +246,8 @@ int nfx_nufft2(const nfx_opts* opts, const int n_modes[3], const void* x, const 
  * captured in a CUDA graph and replayed.  nfx_batch_deconv_* do the same for
  * the deconvolution passes (pad = 0: shuffle/crop after a type-1 FFT; pad = 1:
  * zero-pad before a type-2 FFT); nf / n_modes are 3 ints per problem and fac 3
- * pointers per problem. */
+ * pointers per problem; *total (work units: row segments of the problems'
+ * outputs) is what nfx_batch_deconv takes. */
 typedef struct nfx_batch_problem {
   int64_t M;
   const void* x;

@@ -904,13 +904,18 @@ static void wave_items(const nfx_opts* common, const nfx_wave_item* items, int n
                       host + W.off_shuffle);
 }
 
+// Work units of the batched deconvolution pass over the wave's problems of
+// one kind (the count fill_deconv_items gives their table).
 static int64_t deconv_total(const nfx_wave_item* items, int n, int kind, int dim, bool pad) {
   int64_t t = 0;
   for (int i = 0; i < n; ++i) {
     if (items[i].kind != kind) continue;
-    int64_t c = 1;
-    for (int d = 0; d < dim; ++d) c *= pad ? items[i].nf[d] : items[i].n_modes[d];
-    t += c;
+    int nf[3], nm[3];
+    for (int d = 0; d < 3; ++d) {
+      nf[d] = d < dim ? items[i].nf[d] : 1;
+      nm[d] = d < dim ? items[i].n_modes[d] : 1;
+    }
+    t += deconv_units(nf, nm, pad);
   }
   return t;
 }

@@ -130,66 +130,80 @@ __device__ __forceinline__ int deconv_find(const DeconvItem<T>* __restrict__ ite
   return lo;
 }
 
+// Work unit of the batched passes: one row segment (kSeg elements along x)
+// of one problem, a warp each; `start` counts units.
 template <typename T>
 __global__ void k_deconv_shuffle_batch(const DeconvItem<T>* __restrict__ items, int n, int64_t total) {
   using CT = cplx_t<T>;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
-    const DeconvItem<T>& it = items[deconv_find(items, n, i)];
-    int64_t r = i - it.start;
-    const int n1 = it.nm[0], n2 = it.nm[1];
-    const int p1 = (int)(r % n1);
-    r /= n1;
-    const int p2 = (int)(r % n2);
-    const int p3 = (int)(r / n2);
-    int i1 = p1 - n1 / 2, i2 = p2 - n2 / 2, i3 = p3 - it.nm[2] / 2;
-    if (i1 < 0) i1 += it.nf[0];
+  const int nw = blockDim.x >> 5, lane = threadIdx.x & 31;
+  for (int64_t u = (int64_t)blockIdx.x * nw + (threadIdx.x >> 5); u < total; u += (int64_t)gridDim.x * nw) {
+    const DeconvItem<T>& it = items[deconv_find(items, n, u)];
+    const int n1 = it.nm[0], n2 = it.nm[1], n3 = it.nm[2];
+    const int nseg = (n1 + kSeg - 1) / kSeg;
+    const int64_t local = u - it.start;
+    const int row = (int)(local / nseg);
+    if (row >= n2 * n3) continue;  // a total past the table's units (never, with deconv_units)
+    const int x0 = (int)(local - (int64_t)row * nseg) * kSeg;
+    const int x1 = min(x0 + kSeg, n1);
+    const int p2 = row % n2, p3 = row / n2;
+    int i2 = p2 - n2 / 2, i3 = p3 - n3 / 2;
     if (i2 < 0) i2 += it.nf[1];
     if (i3 < 0) i3 += it.nf[2];
-    const CT v = ((const CT*)it.src)[((int64_t)i3 * it.nf[1] + i2) * it.nf[0] + i1];
-    T fac = it.fac[0][p1];
-    if (it.fac[1] != nullptr) fac = (it.fac[2] != nullptr ? it.fac[2][p3] * it.fac[1][p2] : it.fac[1][p2]) * it.fac[0][p1];
-    CT o;
-    o.x = v.x * fac;
-    o.y = v.y * fac;
-    ((CT*)it.dst)[i - it.start] = o;
+    T fac23 = (T)1;
+    if (it.fac[1] != nullptr) fac23 = it.fac[2] != nullptr ? it.fac[2][p3] * it.fac[1][p2] : it.fac[1][p2];
+    const CT* src = (const CT*)it.src + ((int64_t)i3 * it.nf[1] + i2) * it.nf[0];
+    CT* dst = (CT*)it.dst + (int64_t)row * n1;
+    for (int p1 = x0 + lane; p1 < x1; p1 += 32) {
+      int i1 = p1 - n1 / 2;
+      if (i1 < 0) i1 += it.nf[0];
+      const CT v = src[i1];
+      const T fac = it.fac[1] != nullptr ? fac23 * it.fac[0][p1] : it.fac[0][p1];
+      CT o;
+      o.x = v.x * fac;
+      o.y = v.y * fac;
+      dst[p1] = o;
+    }
   }
 }
 
 template <typename T>
 __global__ void k_deconv_pad_batch(const DeconvItem<T>* __restrict__ items, int n, int64_t total) {
   using CT = cplx_t<T>;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
-    const DeconvItem<T>& it = items[deconv_find(items, n, i)];
-    int64_t r = i - it.start;
+  const int nw = blockDim.x >> 5, lane = threadIdx.x & 31;
+  for (int64_t u = (int64_t)blockIdx.x * nw + (threadIdx.x >> 5); u < total; u += (int64_t)gridDim.x * nw) {
+    const DeconvItem<T>& it = items[deconv_find(items, n, u)];
     const int nf1 = it.nf[0], nf2 = it.nf[1], nf3 = it.nf[2];
-    const int c1 = (int)(r % nf1);
-    r /= nf1;
-    const int c2 = (int)(r % nf2);
-    const int c3 = (int)(r / nf2);
     const int n1 = it.nm[0], n2 = it.nm[1], n3 = it.nm[2];
-    const int k1 = c1 <= (n1 - 1) / 2 ? c1 : (c1 >= nf1 - n1 / 2 ? c1 - nf1 : INT32_MIN);
+    const int nseg = (nf1 + kSeg - 1) / kSeg;
+    const int64_t local = u - it.start;
+    const int row = (int)(local / nseg);
+    if (row >= nf2 * nf3) continue;  // a total past the table's units (never, with deconv_units)
+    const int x0 = (int)(local - (int64_t)row * nseg) * kSeg;
+    const int x1 = min(x0 + kSeg, nf1);
+    const int c2 = row % nf2, c3 = row / nf2;
     const int k2 = c2 <= (n2 - 1) / 2 ? c2 : (c2 >= nf2 - n2 / 2 ? c2 - nf2 : INT32_MIN);
     const int k3 = c3 <= (n3 - 1) / 2 ? c3 : (c3 >= nf3 - n3 / 2 ? c3 - nf3 : INT32_MIN);
-    CT o;
-    o.x = (T)0;
-    o.y = (T)0;
-    if (k1 != INT32_MIN && k2 != INT32_MIN && k3 != INT32_MIN) {
-      const int p1 = k1 + n1 / 2, p2 = k2 + n2 / 2, p3 = k3 + n3 / 2;
-      const CT v = ((const CT*)it.src)[((int64_t)p3 * n2 + p2) * n1 + p1];
-      T fac = it.fac[0][p1];
-      if (it.fac[1] != nullptr)
-        fac = (it.fac[2] != nullptr ? it.fac[2][p3] * it.fac[1][p2] : it.fac[1][p2]) * it.fac[0][p1];
-      o.x = v.x * fac;
-      o.y = v.y * fac;
+    const bool has = k2 != INT32_MIN && k3 != INT32_MIN;
+    const int p2 = has ? k2 + n2 / 2 : 0, p3 = has ? k3 + n3 / 2 : 0;
+    T fac23 = (T)1;
+    if (has && it.fac[1] != nullptr) fac23 = it.fac[2] != nullptr ? it.fac[2][p3] * it.fac[1][p2] : it.fac[1][p2];
+    const CT* src = (const CT*)it.src + ((int64_t)p3 * n2 + p2) * n1;
+    CT* dst = (CT*)it.dst + (int64_t)row * nf1;
+    for (int c1 = x0 + lane; c1 < x1; c1 += 32) {
+      CT o;
+      o.x = (T)0;
+      o.y = (T)0;
+      const int k1 = c1 <= (n1 - 1) / 2 ? c1 : (c1 >= nf1 - n1 / 2 ? c1 - nf1 : INT32_MIN);
+      if (has && k1 != INT32_MIN) {
+        const int p1 = k1 + n1 / 2;
+        const CT v = src[p1];
+        const T fac = it.fac[1] != nullptr ? fac23 * it.fac[0][p1] : it.fac[0][p1];
+        o.x = v.x * fac;
+        o.y = v.y * fac;
+      }
+      dst[c1] = o;
     }
-    ((CT*)it.dst)[i - it.start] = o;
   }
-}
-
-static unsigned elementwise_grid(int64_t n) {
-  int64_t want = (n + 255) / 256;
-  int64_t cap = (int64_t)num_sms() * 16;
-  return (unsigned)(want < cap ? (want > 0 ? want : 1) : cap);
 }
 
 // CTAs for a pass of one warp per row segment over nrows segments (8 warps a
@@ -225,14 +239,19 @@ template <typename T>
 cudaError_t launch_deconv_batch(bool pad, const void* items, int n, int64_t total, cudaStream_t st) {
   if (total <= 0) return cudaSuccess;
   if (pad)
-    k_deconv_pad_batch<T><<<elementwise_grid(total), 256, 0, st>>>((const DeconvItem<T>*)items, n, total);
+    k_deconv_pad_batch<T><<<row_grid(total), 256, 0, st>>>((const DeconvItem<T>*)items, n, total);
   else
-    k_deconv_shuffle_batch<T><<<elementwise_grid(total), 256, 0, st>>>((const DeconvItem<T>*)items, n, total);
+    k_deconv_shuffle_batch<T><<<row_grid(total), 256, 0, st>>>((const DeconvItem<T>*)items, n, total);
   return cudaGetLastError();
 }
 
 size_t deconv_item_bytes(int precision) {
   return precision == 0 ? sizeof(DeconvItem<float>) : sizeof(DeconvItem<double>);
+}
+
+int64_t deconv_units(const int nf[3], const int nm[3], bool pad) {
+  const int* e = pad ? nf : nm;  // the output's extent
+  return (int64_t)e[1] * e[2] * ((e[0] + kSeg - 1) / kSeg);
 }
 
 int64_t fill_deconv_items(int precision, int dim, bool pad, const int* nf, const int* nm, const void* const* fac,
@@ -250,8 +269,8 @@ int64_t fill_deconv_items(int precision, int dim, bool pad, const int* nf, const
       }
       it->src = src[p];
       it->dst = dst[p];
-      it->start = start;
-      start += pad ? (int64_t)it->nf[0] * it->nf[1] * it->nf[2] : (int64_t)it->nm[0] * it->nm[1] * it->nm[2];
+      it->start = start;  // in work units: row segments of kSeg elements
+      start += deconv_units(it->nf, it->nm, pad);
     };
     if (precision == 0)
       fill((DeconvItem<float>*)host_items + p);

@@ -113,7 +113,10 @@ cudaError_t launch_deconv_pad(int dim, const int nf[3], const int nm[3], const T
 template <typename T>
 cudaError_t launch_deconv_batch(bool pad, const void* items, int n, int64_t total, cudaStream_t st);
 size_t deconv_item_bytes(int precision);
-// Fill a host table of batched deconvolution items; returns the total element count.
+// Work units (row segments of the output) of one problem of a batched
+// deconvolution pass (pad: the fine grid nf; else the modes nm).
+int64_t deconv_units(const int nf[3], const int nm[3], bool pad);
+// Fill a host table of batched deconvolution items; returns the total work units.
 int64_t fill_deconv_items(int precision, int dim, bool pad, const int* nf, const int* nm, const void* const* fac,
                           const void* const* src, void* const* dst, int n, void* host_items);
 
