@@ -312,10 +312,15 @@ def run_gpu(args):
     kp = nb.compute_kernel_params(EPS)
     nf = tuple(nb.compute_grid_size(n, 2.0, kp.nspread) for n in N_MODES)
 
-    # Each point set runs on its own stream, so one set's work overlaps the
-    # other's; the step is the union (forked from and joined to the main stream).
+    # Each transform runs on its own stream: the type 1 of a point set (sort,
+    # spread, FFT, deconvolution) on one, its type 2 on another, where the
+    # deconvolve-pad and FFT run while the points sort and the interpolation
+    # waits for the sort the type 1 made (the library's sort cache: an event
+    # dependency).  The step is the union of the four, forked from and joined
+    # to the main stream.
     main = torch.cuda.current_stream(dev)
     set_streams = [torch.cuda.Stream(dev) for _ in sets]
+    t2_streams = [torch.cuda.Stream(dev) for _ in sets]
 
     def step(ds):
         # forked from and joined to the current stream (the capture stream while
@@ -323,13 +328,15 @@ def run_gpu(args):
         cur = torch.cuda.current_stream(dev)
         nb.sort_cache.clear()
         outs = []
-        for s, st in zip(ds, set_streams):
+        for s, st, st2 in zip(ds, set_streams, t2_streams):
             st.wait_stream(cur)
+            st2.wait_stream(cur)
             with torch.cuda.stream(st):
                 f1 = nb.nufft2d1(s["x"], s["y"], s["c"], N_MODES, eps=EPS)
+            with torch.cuda.stream(st2):
                 c2 = nb.nufft2d2(s["x"], s["y"], s["f"], eps=EPS)
             outs.append((f1, c2))
-        for st in set_streams:
+        for st in set_streams + t2_streams:
             cur.wait_stream(st)
         return outs
 

@@ -4,12 +4,13 @@ A `BatchPlan` holds P problems (own points, mode counts and tiling; shared eps,
 precision and dimension).  One `run()` performs, for every problem, a type-1
 transform of its strengths and a type-2 transform of its modes, as
 
-    per-problem bin sorts (concurrent, on side streams) -> ONE persistent
-    spread launch over the work queue of
-    all problems' bin tiles -> one batched cuFFT per grid-size class -> ONE
-    deconvolve/crop launch -> ONE deconvolve/pad launch -> batched cuFFT -> ONE
-    persistent interp launch,
+    type 1: per-problem bin sorts (concurrent, on side streams) -> ONE
+    persistent spread launch over the work queue of all problems' bin tiles ->
+    one batched cuFFT per grid-size class -> ONE deconvolve/crop launch;
+    type 2: ONE deconvolve/pad launch -> batched cuFFT (both while the points
+    sort) -> ONE persistent interp launch once the sorts are done,
 
+the two chains on their own streams and fine grids, so that they overlap,
 captured once in a CUDA graph and replayed (`graph=True`).  The plan owns its
 input and output buffers (`c_in`, `f_in`, `f_out`, `c_out`); callers write
 inputs in place (or pass them to `run`) and read outputs after it.  Coordinates
@@ -72,25 +73,33 @@ class BatchPlan:
         self.f_in = [torch.zeros(tuple(reversed(nm)), dtype=self.cdt, device=dev) for nm in self.n_modes]
         self.f_out = [torch.empty(tuple(reversed(nm)), dtype=self.cdt, device=dev) for nm in self.n_modes]
         self.c_out = [torch.empty(m, dtype=self.cdt, device=dev) for m in self.M]
-        # fine grids grouped by shape (contiguous per group -> one batched FFT each)
+        # fine grids grouped by shape (contiguous per group -> one batched FFT
+        # each): one set for the type 1 (fw), one for the type 2 (fw2), so the
+        # two chains do not wait for each other
         groups: dict[tuple, list[int]] = {}
         for p, nf in enumerate(self.nf):
             groups.setdefault(nf, []).append(p)
-        self.groups = []
-        self.fw = [None] * self.P
-        for nf, members in groups.items():
-            buf = torch.empty((len(members),) + tuple(reversed(nf)), dtype=self.cdt, device=dev)
-            self.groups.append((nf, buf))
-            for i, p in enumerate(members):
-                self.fw[p] = buf[i]
-        # cuFFT work areas owned by the plan (the captured graph keeps their addresses)
-        self.fft_work = []
-        for nf, buf in self.groups:
-            nbytes = c_size_t(0)
-            with torch.cuda.device(dev):
-                _lib.check(self.lib.nfx_fft_work_bytes(self.precision, self.dim, _lib.int3(nf), int(buf.shape[0]),
-                                                       byref(nbytes)), "nfx_fft_work_bytes")
-            self.fft_work.append(torch.empty(max(int(nbytes.value), 1), dtype=torch.uint8, device=dev))
+
+        def grid_set():
+            gs, views = [], [None] * self.P
+            for nf, members in groups.items():
+                buf = torch.empty((len(members),) + tuple(reversed(nf)), dtype=self.cdt, device=dev)
+                gs.append((nf, buf))
+                for i, p in enumerate(members):
+                    views[p] = buf[i]
+            # cuFFT work areas owned by the plan (the captured graph keeps their
+            # addresses), one per group: the groups' FFTs run concurrently
+            work = []
+            for nf, buf in gs:
+                nbytes = c_size_t(0)
+                with torch.cuda.device(dev):
+                    _lib.check(self.lib.nfx_fft_work_bytes(self.precision, self.dim, _lib.int3(nf),
+                                                           int(buf.shape[0]), byref(nbytes)), "nfx_fft_work_bytes")
+                work.append(torch.empty(max(int(nbytes.value), 1), dtype=torch.uint8, device=dev))
+            return gs, views, work
+
+        self.groups, self.fw, self.fft_work = grid_set()
+        self.groups2, self.fw2, self.fft_work2 = grid_set()
 
         # sort workspaces and batch problem tables
         self.opts = _lib.NfxOpts()
@@ -115,7 +124,7 @@ class BatchPlan:
             _lib.check(self.lib.nfx_sort_workspace_bytes(byref(o), self.M[p], byref(nbytes)), "workspace")
             ws = torch.empty(max(int(nbytes.value), 1), dtype=torch.uint8, device=dev)
             self.ws.append(ws)
-            for tab, src, dst in ((probs_s, self.c_in[p], self.fw[p]), (probs_i, self.fw[p], self.c_out[p])):
+            for tab, src, dst in ((probs_s, self.c_in[p], self.fw[p]), (probs_i, self.fw2[p], self.c_out[p])):
                 pb = tab[p]
                 pb.M = self.M[p]
                 cs = [t.data_ptr() for t in self.points[p]] + [None] * (3 - self.dim)
@@ -137,9 +146,12 @@ class BatchPlan:
             o.max_subproblem = probs_s[p].max_subproblem
             self._sort_opts.append(o)
         # independent per-problem sorts and per-class FFTs run on side streams
-        # (fork / join), so the captured graph executes them concurrently
+        # (fork / join), so the captured graph executes them concurrently; the
+        # type-2 chain has its own stream and side streams for its FFTs
         self.n_side = min(8, self.P)
         self.side = [torch.cuda.Stream(device=self.device) for _ in range(self.n_side)]
+        self.side2 = [torch.cuda.Stream(device=self.device) for _ in range(min(self.n_side, len(self.groups2)))]
+        self.t2 = torch.cuda.Stream(device=self.device)
         self.info_s, self.table_s = self._upload(probs_s, spread=True)
         self.info_i, self.table_i = self._upload(probs_i, spread=False)
         # deconvolution tables
@@ -147,7 +159,7 @@ class BatchPlan:
                 for p in range(self.P)]
         self._facs = facs
         self.dtab_shuffle, self.dtotal_shuffle = self._deconv_table(pad=0, src=self.fw, dst=self.f_out)
-        self.dtab_pad, self.dtotal_pad = self._deconv_table(pad=1, src=self.f_in, dst=self.fw)
+        self.dtab_pad, self.dtotal_pad = self._deconv_table(pad=1, src=self.f_in, dst=self.fw2)
         self.graph = None
         self.use_graph = graph
 
@@ -187,14 +199,15 @@ class BatchPlan:
         return table, int(total.value)
 
     # -- execution ------------------------------------------------------------
-    def _fork(self, main, work):
-        """Run work(i, stream) for i over side streams after `main`, then join."""
+    @staticmethod
+    def _fork(main, side, work):
+        """Run work() on the `side` streams after `main`, then join them into `main`."""
         start = torch.cuda.Event()
         start.record(main)
-        for sd in self.side:
+        for sd in side:
             sd.wait_event(start)
         work()
-        for sd in self.side:
+        for sd in side:
             done = torch.cuda.Event()
             done.record(sd)
             main.wait_event(done)
@@ -208,11 +221,11 @@ class BatchPlan:
                                            c_void_p(cs[2]), self.M[p], ptr(self.ws[p]), self.ws[p].numel(),
                                            c_void_p(sd.cuda_stream)), "nfx_sort_points")
 
-    def _ffts(self, sign):
+    def _ffts(self, sign, groups, works, side):
         lib = self.lib
-        for i, (nf, buf) in enumerate(self.groups):
-            sd = self.side[i % self.n_side]
-            work = self.fft_work[i]
+        for i, (nf, buf) in enumerate(groups):
+            sd = side[i % len(side)]
+            work = works[i]
             _lib.check(lib.nfx_fft_ws(self.precision, self.dim, _lib.int3(nf), int(buf.shape[0]), ptr(buf), sign,
                                       ptr(work), work.numel(), c_void_p(sd.cuda_stream)), "nfx_fft_ws")
 
@@ -220,19 +233,43 @@ class BatchPlan:
         lib = self.lib
         main = torch.cuda.current_stream(self.device)
         st = c_void_p(main.cuda_stream)
+        t2 = self.t2
+        st2 = c_void_p(t2.cuda_stream)
+        start = torch.cuda.Event()
+        start.record(main)
+        # sorts on the side streams, while the type-1 grids are zeroed on main
+        for sd in self.side:
+            sd.wait_event(start)
+        self._sorts()
         for _, buf in self.groups:
             buf.zero_()
-        self._fork(main, self._sorts)
+        sorted_ev = []
+        for sd in self.side:
+            ev = torch.cuda.Event()
+            ev.record(sd)
+            sorted_ev.append(ev)
+            main.wait_event(ev)
+        # type 2, on its own stream: deconvolve/pad and FFT run while the points
+        # sort; the interpolation waits for the sorts
+        t2.wait_event(start)
+        _lib.check(lib.nfx_batch_deconv(self.precision, 1, ptr(self.dtab_pad), self.P, self.dtotal_pad, st2),
+                   "nfx_batch_deconv(pad)")
+        self._fork(t2, self.side2,
+                   lambda: self._ffts(_fft_sign_type2(self.isign2), self.groups2, self.fft_work2, self.side2))
+        for ev in sorted_ev:
+            t2.wait_event(ev)
+        _lib.check(lib.nfx_batch_launch(byref(self.opts), 0, ptr(self.table_i), self.P, byref(self.info_i), st2),
+                   "nfx_batch_launch(interp)")
+        # type 1 on the current stream
         _lib.check(lib.nfx_batch_launch(byref(self.opts), 1, ptr(self.table_s), self.P, byref(self.info_s), st),
                    "nfx_batch_launch(spread)")
-        self._fork(main, lambda: self._ffts(_fft_sign_type1(self.isign1)))
+        self._fork(main, self.side,
+                   lambda: self._ffts(_fft_sign_type1(self.isign1), self.groups, self.fft_work, self.side))
         _lib.check(lib.nfx_batch_deconv(self.precision, 0, ptr(self.dtab_shuffle), self.P, self.dtotal_shuffle, st),
                    "nfx_batch_deconv(shuffle)")
-        _lib.check(lib.nfx_batch_deconv(self.precision, 1, ptr(self.dtab_pad), self.P, self.dtotal_pad, st),
-                   "nfx_batch_deconv(pad)")
-        self._fork(main, lambda: self._ffts(_fft_sign_type2(self.isign2)))
-        _lib.check(lib.nfx_batch_launch(byref(self.opts), 0, ptr(self.table_i), self.P, byref(self.info_i), st),
-                   "nfx_batch_launch(interp)")
+        done2 = torch.cuda.Event()
+        done2.record(t2)
+        main.wait_event(done2)
 
     def run(self, c: Sequence[torch.Tensor] | None = None, f: Sequence[torch.Tensor] | None = None):
         """Type 1 of every problem's strengths and type 2 of its modes.
