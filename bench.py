@@ -9,8 +9,9 @@ Workload (one step = one type-1 and one type-2 transform of each point set):
 Metric: NU points per second, counting M once per transform (2 * (Ma + Mb) per step).
 
 `value` times the steps with inputs resident in HBM (CUDA events, L2 flushed
-between steps by writing a 256 MB buffer outside the timed events); the two
-point sets of a step run on two CUDA streams, so their work overlaps.  `e2e` times
+between steps by writing a 256 MB buffer outside the timed events); the four
+transforms of a step run on four CUDA streams (a type 2's deconvolve-pad and FFT
+overlap the sort of its points), so their work overlaps.  `e2e` times
 the same steps through the public API with pinned host buffers: host->device
 copies of x, y, c, f and device->host copies of the results are inside the
 timed region; uploads, compute and downloads run on separate streams so they
