@@ -249,8 +249,8 @@ ALG_BYTES = {
 
 
 # Per-launch counters of the spread / interp kernels on each point set, from
-# single-step ncu --set full captures of `bench.py --case radial|clustered --reps 1`
-# (profiles/kernels_2d_bench_sets.md): DRAM bytes (dram__bytes_read.sum +
+# single-step ncu --metrics captures of `bench.py --case radial|clustered --reps 1`
+# (profiles/k_spread_interp_2d_counters.md): DRAM bytes (dram__bytes_read.sum +
 # dram__bytes_write.sum, caches flushed before the launch), warp instructions
 # (smsp__inst_executed.sum) and shared-memory wavefronts
 # (l1tex__data_pipe_lsu_wavefronts_mem_shared.sum).  The counts do not depend on
@@ -258,10 +258,10 @@ ALG_BYTES = {
 # fractions of the issue and shared-memory roofs, the ones that bind these
 # kernels (HBM runs at a few percent of peak).
 MEASURED_COUNTERS = {
-    "nfx_spread_sorted": {"radial": {"dram": 17.3e6, "inst": 36.3e6, "smem_wf": 9.40e6},
-                          "clustered": {"dram": 85.6e6, "inst": 87.1e6, "smem_wf": 18.1e6}},
-    "nfx_interp_sorted": {"radial": {"dram": 13.5e6, "inst": 8.19e6, "smem_wf": 3.71e6},
-                          "clustered": {"dram": 102.8e6, "inst": 51.1e6, "smem_wf": 10.1e6}},
+    "nfx_spread_sorted": {"radial": {"dram": 17.26e6, "inst": 40.75e6, "smem_wf": 6.39e6},
+                          "clustered": {"dram": 84.82e6, "inst": 78.85e6, "smem_wf": 17.55e6}},
+    "nfx_interp_sorted": {"radial": {"dram": 13.53e6, "inst": 7.31e6, "smem_wf": 3.71e6},
+                          "clustered": {"dram": 102.01e6, "inst": 43.48e6, "smem_wf": 10.11e6}},
 }
 N_SMS = 148
 ISSUE_PER_SM_CLK = 4      # one warp instruction per scheduler per clock, 4 schedulers per SM
@@ -288,7 +288,7 @@ def secondary_roofs(kernel: str, avg_launch_ms: float, sm_mhz) -> dict | None:
         "shared": {"achieved": wf * 128 / t / 1e9, "peak": smem_peak, "unit": "GB/s",
                    "frac": wf * 128 / t / 1e9 / smem_peak, "wavefronts_per_launch": wf},
         "clock_mhz": float(sm_mhz),
-        "counts_from": "ncu --set full, one launch per point set (profiles/kernels_2d_bench_sets.md)",
+        "counts_from": "ncu --metrics, one launch per point set (profiles/k_spread_interp_2d_counters.md)",
     }
 
 

@@ -276,6 +276,71 @@ __device__ __forceinline__ void add_slot(const T* sp, int kx, int grp, cplx_t<T>
   }
 }
 
+// Adds one staged point straight to the shared tile at footprint origin `off`.
+// lane_cell: tile offset of this lane's first cell (row grp * rpl, column kx)
+// from the origin, -1 when the lane owns no cell; rows r after the first are
+// r rows further (2D), or r / ns planes and r % ns rows further (3D with rpl a
+// multiple of ns: compile-time in r).
+template <typename T, int DIM, int NS>
+__device__ __forceinline__ void add_slot_direct(const T* sp, int kx, int grp, int off, T* s_re, T* s_im,
+                                                int lane_cell, int row, int plane) {
+  using CT = cplx_t<T>;
+  constexpr int RPL = run_rows_per_lane(DIM, NS);
+  constexpr int NR = run_rows(DIM, NS);
+  constexpr int WY = run_wy(DIM, NS);
+  constexpr int YOFF = round4(2 * NS);
+  constexpr int ZOFF = YOFF + WY;
+  if (lane_cell < 0) return;
+  const CT cw = reinterpret_cast<const CT*>(sp)[kx];
+  T* pr = s_re + off + lane_cell;
+  T* pi = s_im + off + lane_cell;
+  auto add = [&](int o, T w) {
+    atomicAdd(pr + o, w * cw.x);
+    atomicAdd(pi + o, w * cw.y);
+  };
+  if constexpr (DIM == 2) {
+    const T* wy = sp + YOFF + grp * RPL;
+#pragma unroll
+    for (int r = 0; r < RPL; ++r)
+      if (grp * RPL + r < NR) add(r * row, wy[r]);
+  } else if constexpr (RPL % NS == 0) {
+    const T* wz = sp + ZOFF + grp * (RPL / NS);
+    T wy[NS];
+#pragma unroll
+    for (int q = 0; q < NS; ++q) wy[q] = sp[YOFF + q];
+#pragma unroll
+    for (int zz = 0; zz < RPL / NS; ++zz) {
+      const T z = wz[zz];
+#pragma unroll
+      for (int q = 0; q < NS; ++q) add(zz * plane + q * row, z * wy[q]);
+    }
+  } else {
+#pragma unroll
+    for (int r = 0; r < RPL; ++r) {
+      const int rho = grp * RPL + r;
+      if (rho < NR) {
+        const int rz = rho / NS, ry = rho - rz * NS;
+        add((rz - (grp * RPL) / NS) * plane + (ry - (grp * RPL) % NS) * row, sp[ZOFF + rz] * sp[YOFF + ry]);
+      }
+    }
+  }
+}
+
+// 3D batches of 32 points with at least this many run starts (mean run of 4
+// or less) skip the register accumulation and add each point directly: a
+// lane's rpl = 16 rows make a run's walk and flush cost more than the direct
+// adds of a few points.  2D batches always take the walk: a float atomicAdd on
+// shared memory is a compare-and-swap loop (no native float add), so a run's
+// flush of rpl = 2 complex cells per lane costs about as much as adding one
+// point's cells directly, and the walk measured faster than the direct path
+// for batches of mean run 1 to 4 (2D ns = 8: 4M clustered points 167 -> 158
+// us, 0.5M radial points unchanged).
+constexpr int kSparseRuns = 8;
+template <int DIM>
+__device__ __forceinline__ bool direct_batch(unsigned starts) {
+  return DIM == 3 && __popc(starts) >= kSparseRuns;
+}
+
 // Run-merging spread (2D/3D, footprints of at least 32 cells).  Each warp walks
 // a contiguous, cell-ordered slice of the subproblem 32 points at a time: every
 // lane stages one point in a shared slot (stage_slot), then the warp takes the
@@ -285,12 +350,7 @@ __device__ __forceinline__ void add_slot(const T* sp, int kx, int grp, cplx_t<T>
 // footprint, so the registers reach shared memory (atomics, distinct addresses
 // within an instruction) only when the cell changes.  One ballot per batch
 // marks where runs start; the walk goes run by run, each run an unrolled loop
-// with no branch per point.  Batches of short runs take the same walk: a float
-// atomicAdd on shared memory is a compare-and-swap loop (no native float add),
-// so a run's flush of rpl complex cells per lane costs about as much as adding
-// one point's cells directly, and the walk measured faster than a direct-add
-// path for batches of mean run 1 to 4 (2D ns = 8: 4M clustered points 167 ->
-// 158 us, 0.5M radial points unchanged).  The next batch's point indices, coordinates and
+// with no branch per point.  The next batch's point indices, coordinates and
 // strengths are fetched while the current batch is walked.
 template <typename T, int DIM, int NS, int NW>
 __device__ __forceinline__ void spread_subproblem_runs(const PointArgs<T>& a, const cplx_t<T>* __restrict__ c,
@@ -414,6 +474,18 @@ __device__ __forceinline__ void spread_subproblem_runs(const PointArgs<T>& a, co
       const int cnt = min(32, w1 - kb);
       int j = 0;
       const T* sp = warp_slots;
+      if (direct_batch<DIM>(starts)) {
+        // short runs: points before the first run start finish the pending
+        // run; every later point is added to shared memory directly
+        const int first = __ffs(starts) - 1;
+        for (; j < first; ++j, sp += SLOT) add_slot<T, DIM, NS>(sp, kx, grp, acc);
+        if (run_off >= 0) flush_run();
+        for (; j < cnt; ++j, sp += SLOT)
+          add_slot_direct<T, DIM, NS>(sp, kx, grp, __shfl_sync(0xffffffffu, off, j), s_re, s_im, lane_cell, row,
+                                      plane);
+        run_off = __shfl_sync(0xffffffffu, off, cnt - 1);  // accumulators are empty
+        j = cnt;
+      }
       while (j < cnt) {  // one run (or the rest of one) per trip
         if ((starts >> j) & 1u) {
           if (run_off >= 0) flush_run();
