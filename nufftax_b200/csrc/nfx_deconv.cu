@@ -16,11 +16,14 @@
 namespace nfx {
 
 // Both passes go row by row (a row = one (transform, z, y) line along x, cut
-// into segments of kSeg elements so that long 1D rows still spread over many
-// warps; one warp per segment): the row's indices come from one division chain
-// per segment, the x loop is plain strided adds, so no thread divides per
-// element.
-constexpr int kSeg = 1024;
+// into segments of kSeg elements, one warp per segment): the row's indices
+// come from one division chain per segment, so no thread divides per element.
+// A lane takes kSeg / 32 elements of its segment, all loads issued before any
+// store (unrolled), so every lane has that many reads in flight; segments are
+// short enough that a 2D grid of 512 or 1024 rows still gives thousands of
+// warps.
+constexpr int kSeg = 128;
+constexpr int kSegPerLane = kSeg / 32;
 template <typename T>
 __global__ void k_deconv_shuffle(int nf1, int nf2, int nf3, int n1, int n2, int n3, const T* __restrict__ f1,
                                  const T* __restrict__ f2, const T* __restrict__ f3,
@@ -46,16 +49,29 @@ __global__ void k_deconv_shuffle(int nf1, int nf2, int nf3, int n1, int n2, int 
     if (f2 != nullptr) fac23 = f3 != nullptr ? f3[p3] * f2[p2] : f2[p2];
     const CT* src = in + t * grid + ((int64_t)i3 * nf2 + i2) * nf1;
     CT* dst = out + row * n1;
-    for (int p1 = x0 + lane; p1 < x1; p1 += 32) {
-      int i1 = p1 + k1min;
-      if (i1 < 0) i1 += nf1;
-      const CT v = src[i1];
-      // (fac3 * fac2) * fac1, the reference's order
-      const T fac = f2 != nullptr ? fac23 * f1[p1] : f1[p1];
-      CT o;
-      o.x = v.x * fac;
-      o.y = v.y * fac;
-      dst[p1] = o;
+    CT v[kSegPerLane];
+    T f[kSegPerLane];
+#pragma unroll
+    for (int j = 0; j < kSegPerLane; ++j) {
+      const int p1 = x0 + lane + 32 * j;
+      if (p1 < x1) {
+        int i1 = p1 + k1min;
+        if (i1 < 0) i1 += nf1;
+        v[j] = src[i1];
+        f[j] = f1[p1];
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < kSegPerLane; ++j) {
+      const int p1 = x0 + lane + 32 * j;
+      if (p1 < x1) {
+        // (fac3 * fac2) * fac1, the reference's order
+        const T fac = f2 != nullptr ? fac23 * f[j] : f[j];
+        CT o;
+        o.x = v[j].x * fac;
+        o.y = v[j].y * fac;
+        dst[p1] = o;
+      }
     }
   }
 }
@@ -88,19 +104,36 @@ __global__ void k_deconv_pad(int nf1, int nf2, int nf3, int n1, int n2, int n3, 
     T fac23 = (T)1;
     if (has && f2 != nullptr) fac23 = f3 != nullptr ? f3[p3] * f2[p2] : f2[p2];
     const CT* src = in + t * per + ((int64_t)p3 * n2 + p2) * n1;
-    for (int c1 = x0 + lane; c1 < x1; c1 += 32) {
-      CT o;
-      o.x = (T)0;
-      o.y = (T)0;
+    CT v[kSegPerLane];
+    T f[kSegPerLane];
+    bool m[kSegPerLane];  // the cell holds a kept mode
+#pragma unroll
+    for (int j = 0; j < kSegPerLane; ++j) {
+      const int c1 = x0 + lane + 32 * j;
       const int k1 = c1 <= k1max ? c1 : (c1 >= nf1 + k1min ? c1 - nf1 : INT32_MIN);
-      if (has && k1 != INT32_MIN) {
+      v[j].x = v[j].y = (T)0;
+      f[j] = (T)0;
+      m[j] = c1 < x1 && has && k1 != INT32_MIN;
+      if (m[j]) {
         const int p1 = k1 - k1min;
-        const CT v = src[p1];
-        const T fac = f2 != nullptr ? fac23 * f1[p1] : f1[p1];
-        o.x = v.x * fac;
-        o.y = v.y * fac;
+        v[j] = src[p1];
+        f[j] = f1[p1];
       }
-      dst[c1] = o;
+    }
+#pragma unroll
+    for (int j = 0; j < kSegPerLane; ++j) {
+      const int c1 = x0 + lane + 32 * j;
+      if (c1 < x1) {
+        CT o;
+        o.x = (T)0;
+        o.y = (T)0;
+        if (m[j]) {
+          const T fac = f2 != nullptr ? fac23 * f[j] : f[j];
+          o.x = v[j].x * fac;
+          o.y = v[j].y * fac;
+        }
+        dst[c1] = o;
+      }
     }
   }
 }
@@ -153,15 +186,28 @@ __global__ void k_deconv_shuffle_batch(const DeconvItem<T>* __restrict__ items, 
     if (it.fac[1] != nullptr) fac23 = it.fac[2] != nullptr ? it.fac[2][p3] * it.fac[1][p2] : it.fac[1][p2];
     const CT* src = (const CT*)it.src + ((int64_t)i3 * it.nf[1] + i2) * it.nf[0];
     CT* dst = (CT*)it.dst + (int64_t)row * n1;
-    for (int p1 = x0 + lane; p1 < x1; p1 += 32) {
-      int i1 = p1 - n1 / 2;
-      if (i1 < 0) i1 += it.nf[0];
-      const CT v = src[i1];
-      const T fac = it.fac[1] != nullptr ? fac23 * it.fac[0][p1] : it.fac[0][p1];
-      CT o;
-      o.x = v.x * fac;
-      o.y = v.y * fac;
-      dst[p1] = o;
+    CT v[kSegPerLane];
+    T f[kSegPerLane];
+#pragma unroll
+    for (int j = 0; j < kSegPerLane; ++j) {
+      const int p1 = x0 + lane + 32 * j;
+      if (p1 < x1) {
+        int i1 = p1 - n1 / 2;
+        if (i1 < 0) i1 += it.nf[0];
+        v[j] = src[i1];
+        f[j] = it.fac[0][p1];
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < kSegPerLane; ++j) {
+      const int p1 = x0 + lane + 32 * j;
+      if (p1 < x1) {
+        const T fac = it.fac[1] != nullptr ? fac23 * f[j] : f[j];
+        CT o;
+        o.x = v[j].x * fac;
+        o.y = v[j].y * fac;
+        dst[p1] = o;
+      }
     }
   }
 }
@@ -189,19 +235,36 @@ __global__ void k_deconv_pad_batch(const DeconvItem<T>* __restrict__ items, int 
     if (has && it.fac[1] != nullptr) fac23 = it.fac[2] != nullptr ? it.fac[2][p3] * it.fac[1][p2] : it.fac[1][p2];
     const CT* src = (const CT*)it.src + ((int64_t)p3 * n2 + p2) * n1;
     CT* dst = (CT*)it.dst + (int64_t)row * nf1;
-    for (int c1 = x0 + lane; c1 < x1; c1 += 32) {
-      CT o;
-      o.x = (T)0;
-      o.y = (T)0;
+    CT v[kSegPerLane];
+    T f[kSegPerLane];
+    bool m[kSegPerLane];  // the cell holds a kept mode
+#pragma unroll
+    for (int j = 0; j < kSegPerLane; ++j) {
+      const int c1 = x0 + lane + 32 * j;
       const int k1 = c1 <= (n1 - 1) / 2 ? c1 : (c1 >= nf1 - n1 / 2 ? c1 - nf1 : INT32_MIN);
-      if (has && k1 != INT32_MIN) {
+      v[j].x = v[j].y = (T)0;
+      f[j] = (T)0;
+      m[j] = c1 < x1 && has && k1 != INT32_MIN;
+      if (m[j]) {
         const int p1 = k1 + n1 / 2;
-        const CT v = src[p1];
-        const T fac = it.fac[1] != nullptr ? fac23 * it.fac[0][p1] : it.fac[0][p1];
-        o.x = v.x * fac;
-        o.y = v.y * fac;
+        v[j] = src[p1];
+        f[j] = it.fac[0][p1];
       }
-      dst[c1] = o;
+    }
+#pragma unroll
+    for (int j = 0; j < kSegPerLane; ++j) {
+      const int c1 = x0 + lane + 32 * j;
+      if (c1 < x1) {
+        CT o;
+        o.x = (T)0;
+        o.y = (T)0;
+        if (m[j]) {
+          const T fac = it.fac[1] != nullptr ? fac23 * f[j] : f[j];
+          o.x = v[j].x * fac;
+          o.y = v[j].y * fac;
+        }
+        dst[c1] = o;
+      }
     }
   }
 }
